@@ -1,0 +1,138 @@
+// Internal state of the AdaptaHOP engine (one per process, like the Fortran
+// module neiKDtree).  All particle arrays live in HBM in Morton-sorted order
+// ("s" index); orig[s] maps back to the caller's 0-based particle index.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "ahop_b200.h"
+
+namespace ahop {
+
+// Growable device buffer; never shrinks until close().
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t need) {
+    if (need <= bytes) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, need ? need : 16);
+    if (e == cudaSuccess) bytes = need ? need : 16;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct Params {
+  int64_t npart = 0;
+  int32_t nusedpart = 0;
+  int32_t nvoisins = 32, nhop = 16, nlevelmax = 30, nmembthresh = 20, nMembers = 20, nbPes = 1;
+  double rho_threshold = 80.0, fudge = 4.0, alphap = 1.0, epsilon = 0.0, fudgepsilon = 1e-5;
+  double massp = 0, boxsize = 1, boxsize2 = 1, Lf = 1;
+  double xlong = 1, ylong = 1, zlong = 1, xlongs2 = 0.5, ylongs2 = 0.5, zlongs2 = 0.5, xyzlong = 1;
+  bool verbose = false, megaverbose = false, optimize_nodes = false;
+  std::string method = "MSM";
+  AhopInit init{};
+};
+
+// Node record on the device; same fields as the Fortran `supernode`
+// (f90:160-174).
+struct NodeRec {
+  double rho_saddle, density, densmax, radius, truemass, pos[3];
+  int32_t mass, level, mother, firstchild, nsisters, sister;
+};
+
+constexpr int kLeaf = 32;         // particles per leaf bucket
+constexpr int kFan = 32;          // children per internal node
+constexpr int kMaxLevels = 8;
+
+struct Engine {
+  Params prm;
+  int device = -1;
+  cudaStream_t stream = nullptr;  // stream of the current call
+  cudaEvent_t ev[10] = {};
+  bool events_ready = false;
+  AhopTimings timings{};
+
+  int64_t n = 0;          // particles in the current run
+  int32_t nstore = 16;    // neighbours stored per particle
+  int32_t req_store = 0;  // requested via debug API (0 = nhop)
+  bool have_result = false;
+
+  // inputs / sorted particle arrays
+  DevBuf d_pos_in, d_mass_in;            // staging for host inputs
+  DevBuf d_key, d_key2, d_idx, d_idx2;   // Morton keys + permutation
+  DevBuf d_x, d_y, d_z, d_m;             // sorted SoA
+  DevBuf d_orig;                         // orig index (0-based) per sorted slot
+  DevBuf d_rank;                         // sorted slot per orig index
+  DevBuf d_box;                          // AABBs of all levels (6 doubles each)
+  int32_t nlev = 0;
+  int64_t lev_off[kMaxLevels + 1] = {};
+  int64_t lev_cnt[kMaxLevels] = {};
+  DevBuf d_cub;                          // CUB scratch
+
+  // kNN / density
+  DevBuf d_nei;                          // [n][nstore] sorted-slot neighbour ids
+  DevBuf d_dens;                         // density in sorted order
+  // hop / groups
+  DevBuf d_hop, d_root, d_group;         // per sorted slot
+  DevBuf d_peakflag;                     // per orig index
+  int32_t ngroups = 0;
+  DevBuf d_densg;                        // [ngroups+1] peak density per group
+  DevBuf d_gpeak;                        // [ngroups+1] sorted slot of peak
+  DevBuf d_goff;                         // [ngroups+2] member CSR offsets (desc orig order)
+  DevBuf d_gmem;                         // [nactive] sorted slots
+  DevBuf d_gmem_rho;                     // [nactive] member density in desc-density order
+  DevBuf d_gmem_rho_pref;                // [nactive] prefix sums of density (desc density order)
+  int64_t nactive = 0;
+  // saddles
+  DevBuf d_sad_key, d_sad_key2, d_sad_val, d_sad_val2, d_sad_cnt, d_sad_keep, d_sad_kpos;
+  DevBuf d_flags;                        // small device error/status flags
+  DevBuf d_soff, d_sisad, d_srho;        // final CSR
+  int32_t nconn = 0;
+  // nodes
+  DevBuf d_nodes;                        // NodeRec[nnodesmax+1]
+  DevBuf d_tree_scratch;
+  int32_t nnodes = 0;
+  DevBuf d_liste;                        // [n] node id per ORIG particle (1-based), 0 none
+  DevBuf d_dens_orig;                    // [n] density in ORIG order
+  DevBuf d_rtab, d_itab;                 // exported tables
+
+  // host copies (module outputs)
+  std::vector<int32_t> h_liste, h_itab;
+  std::vector<double> h_dens, h_rtab;
+
+  // small pinned host scalars
+  int64_t* h_scalars = nullptr;
+};
+
+Engine& engine();
+void set_error(const std::string& s);
+
+// Stage entry points (return AHOP_* codes).
+int stage_sort_and_tree(Engine& E, const double* d_pos_aos, const double* d_mass);
+int stage_knn_density(Engine& E);
+int stage_hop_groups(Engine& E);
+int stage_saddles(Engine& E);
+int stage_nodes(Engine& E);
+
+}  // namespace ahop
+
+#define AHOP_CUDA_TRY(expr)                                                                      \
+  do {                                                                                            \
+    cudaError_t _e = (expr);                                                                      \
+    if (_e != cudaSuccess) {                                                                      \
+      ::ahop::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e) + " at " + __FILE__ + \
+                        ":" + std::to_string(__LINE__));                                          \
+      return (_e == cudaErrorMemoryAllocation) ? AHOP_ENOMEM : AHOP_ECUDA;                        \
+    }                                                                                             \
+  } while (0)

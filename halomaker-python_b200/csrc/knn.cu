@@ -1,0 +1,383 @@
+// Morton-bucketed tree build and warp-per-query periodic kNN fused with the
+// SPH cubic-spline density.
+//
+// Replaces create_tree_structure/create_KDtree (f90:2967-3221),
+// omp_find_nearest_parts/walk_tree2 (f90:2841-2962) and omp_compute_density
+// (f90:2816-2838) of the reference.
+//
+// Layout: particles are radix-sorted by a 63-bit Morton key; leaf j holds the
+// 32 consecutive sorted particles [32j, 32j+32); each internal level groups 32
+// consecutive nodes of the level below.  Every node stores its padded
+// axis-aligned box as centre + half-width (6 doubles).  The kNN result of a
+// query is the set of its nvoisins nearest particles under the reference's
+// periodic distance, ordered by (distance, particle index); distances and the
+// density use the reference's exact expression order in explicitly rounded
+// FP64 (no FMA), so the density matches the reference bit for bit whenever the
+// neighbour order does.
+#include <cub/cub.cuh>
+#include <cfloat>
+#include <climits>
+#include <math_constants.h>
+
+#include "engine.h"
+#include "exact.cuh"
+
+namespace ahop {
+
+// ---------------------------------------------------------------- Morton keys
+__device__ __forceinline__ unsigned long long spread21(unsigned int v) {
+  unsigned long long x = v & 0x1fffffULL;
+  x = (x | (x << 32)) & 0x1f00000000ffffULL;
+  x = (x | (x << 16)) & 0x1f0000ff0000ffULL;
+  x = (x | (x << 8)) & 0x100f00f00f00f00fULL;
+  x = (x | (x << 4)) & 0x10c30c30c30c30c3ULL;
+  x = (x | (x << 2)) & 0x1249249249249249ULL;
+  return x;
+}
+
+__device__ __forceinline__ unsigned int quant21(double v, double half, double L) {
+  double u = (v + half) / L;  // [0,1) for v in [-L/2, L/2)
+  double q = u * 2097152.0;
+  if (!(q >= 0.0)) q = 0.0;
+  if (q > 2097151.0) q = 2097151.0;
+  return (unsigned int)q;
+}
+
+__global__ void morton_kernel(const double* __restrict__ pos, int64_t n, double Lx, double Ly, double Lz,
+                              unsigned long long* __restrict__ key, int32_t* __restrict__ idx) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double x = pos[3 * i + 0], y = pos[3 * i + 1], z = pos[3 * i + 2];
+  unsigned int qx = quant21(x, 0.5 * Lx, Lx), qy = quant21(y, 0.5 * Ly, Ly), qz = quant21(z, 0.5 * Lz, Lz);
+  key[i] = (spread21(qx) << 2) | (spread21(qy) << 1) | spread21(qz);
+  idx[i] = (int32_t)i;
+}
+
+__global__ void gather_sorted_kernel(const double* __restrict__ pos, const double* __restrict__ mass,
+                                     const int32_t* __restrict__ idx, int64_t n, double* __restrict__ x,
+                                     double* __restrict__ y, double* __restrict__ z, double* __restrict__ m,
+                                     int32_t* __restrict__ orig, int32_t* __restrict__ rank) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  int32_t o = idx[s];
+  x[s] = pos[3 * (int64_t)o + 0];
+  y[s] = pos[3 * (int64_t)o + 1];
+  z[s] = pos[3 * (int64_t)o + 2];
+  m[s] = mass[o];
+  orig[s] = o;
+  rank[o] = (int32_t)s;
+}
+
+// Box storage: 6 doubles per node: cx, cy, cz, wx, wy, wz (centre, padded half-width).
+__device__ __forceinline__ void warp_minmax(double& lo, double& hi) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+}
+
+// Leaf boxes: one warp per leaf.
+__global__ void leaf_box_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                                const double* __restrict__ z, int64_t n, int64_t nleaf, double pad,
+                                double* __restrict__ box) {
+  int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (w >= nleaf) return;
+  int64_t p = w * kLeaf + lane;
+  bool v = p < n;
+  double lx = v ? x[p] : DBL_MAX, hx = v ? x[p] : -DBL_MAX;
+  double ly = v ? y[p] : DBL_MAX, hy = v ? y[p] : -DBL_MAX;
+  double lz = v ? z[p] : DBL_MAX, hz = v ? z[p] : -DBL_MAX;
+  warp_minmax(lx, hx);
+  warp_minmax(ly, hy);
+  warp_minmax(lz, hz);
+  if (lane == 0) {
+    double* b = box + 6 * w;
+    b[0] = 0.5 * (lx + hx); b[1] = 0.5 * (ly + hy); b[2] = 0.5 * (lz + hz);
+    b[3] = 0.5 * (hx - lx) + pad; b[4] = 0.5 * (hy - ly) + pad; b[5] = 0.5 * (hz - lz) + pad;
+  }
+}
+
+// Internal boxes: one warp per node over its (<= 32) child boxes.
+__global__ void node_box_kernel(const double* __restrict__ child, int64_t nchild, int64_t nnode,
+                                double* __restrict__ box) {
+  int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (w >= nnode) return;
+  int64_t c = w * kFan + lane;
+  bool v = c < nchild;
+  double lo[3], hi[3];
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = v ? child[6 * c + k] - child[6 * c + 3 + k] : DBL_MAX;
+    hi[k] = v ? child[6 * c + k] + child[6 * c + 3 + k] : -DBL_MAX;
+    warp_minmax(lo[k], hi[k]);
+  }
+  if (lane == 0) {
+    double* b = box + 6 * w;
+    for (int k = 0; k < 3; ++k) {
+      b[k] = 0.5 * (lo[k] + hi[k]);
+      b[3 + k] = 0.5 * (hi[k] - lo[k]) * (1.0 + 1e-12) + 1e-300;
+    }
+  }
+}
+
+int stage_sort_and_tree(Engine& E, const double* d_pos, const double* d_mass) {
+  const int64_t n = E.n;
+  const Params& P = E.prm;
+  cudaStream_t st = E.stream;
+  AHOP_CUDA_TRY(E.d_key.ensure(n * 8));
+  AHOP_CUDA_TRY(E.d_key2.ensure(n * 8));
+  AHOP_CUDA_TRY(E.d_idx.ensure(n * 4));
+  AHOP_CUDA_TRY(E.d_idx2.ensure(n * 4));
+  AHOP_CUDA_TRY(E.d_x.ensure(n * 8));
+  AHOP_CUDA_TRY(E.d_y.ensure(n * 8));
+  AHOP_CUDA_TRY(E.d_z.ensure(n * 8));
+  AHOP_CUDA_TRY(E.d_m.ensure(n * 8));
+  AHOP_CUDA_TRY(E.d_orig.ensure(n * 4));
+  AHOP_CUDA_TRY(E.d_rank.ensure(n * 4));
+  const int T = 256;
+  unsigned grid = (unsigned)((n + T - 1) / T);
+  morton_kernel<<<grid, T, 0, st>>>(d_pos, n, P.xlong, P.ylong, P.zlong, E.d_key.as<unsigned long long>(),
+                                    E.d_idx.as<int32_t>());
+  AHOP_CUDA_TRY(cudaGetLastError());
+  size_t tmp = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp, E.d_key.as<unsigned long long>(),
+                                  E.d_key2.as<unsigned long long>(), E.d_idx.as<int32_t>(),
+                                  E.d_idx2.as<int32_t>(), (int)n, 0, 63, st);
+  AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
+  AHOP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(E.d_cub.p, tmp, E.d_key.as<unsigned long long>(),
+                                                E.d_key2.as<unsigned long long>(), E.d_idx.as<int32_t>(),
+                                                E.d_idx2.as<int32_t>(), (int)n, 0, 63, st));
+  gather_sorted_kernel<<<grid, T, 0, st>>>(d_pos, d_mass, E.d_idx2.as<int32_t>(), n, E.d_x.as<double>(),
+                                           E.d_y.as<double>(), E.d_z.as<double>(), E.d_m.as<double>(),
+                                           E.d_orig.as<int32_t>(), E.d_rank.as<int32_t>());
+  AHOP_CUDA_TRY(cudaGetLastError());
+  // levels
+  int64_t cnt = (n + kLeaf - 1) / kLeaf;
+  int nlev = 0;
+  int64_t off = 0;
+  for (;;) {
+    if (nlev >= kMaxLevels) { set_error("too many tree levels"); return AHOP_EINVAL; }
+    E.lev_off[nlev] = off;
+    E.lev_cnt[nlev] = cnt;
+    off += cnt;
+    nlev++;
+    if (cnt == 1) break;
+    cnt = (cnt + kFan - 1) / kFan;
+  }
+  E.lev_off[nlev] = off;
+  E.nlev = nlev;
+  AHOP_CUDA_TRY(E.d_box.ensure(off * 6 * 8));
+  double* box = E.d_box.as<double>();
+  double pad = 1e-12 * fmax(P.xlong, fmax(P.ylong, P.zlong));
+  {
+    int64_t threads = E.lev_cnt[0] * 32;
+    leaf_box_kernel<<<(unsigned)((threads + T - 1) / T), T, 0, st>>>(E.d_x.as<double>(), E.d_y.as<double>(),
+                                                                     E.d_z.as<double>(), n, E.lev_cnt[0], pad,
+                                                                     box);
+    AHOP_CUDA_TRY(cudaGetLastError());
+  }
+  for (int l = 1; l < nlev; ++l) {
+    int64_t threads = E.lev_cnt[l] * 32;
+    node_box_kernel<<<(unsigned)((threads + T - 1) / T), T, 0, st>>>(
+        box + 6 * E.lev_off[l - 1], E.lev_cnt[l - 1], E.lev_cnt[l], box + 6 * E.lev_off[l]);
+    AHOP_CUDA_TRY(cudaGetLastError());
+  }
+  return AHOP_OK;
+}
+
+// ------------------------------------------------------------------ kNN kernel
+struct KnnArgs {
+  const double *x, *y, *z, *m;
+  const int32_t* orig;
+  const double* box;
+  int64_t lev_off[kMaxLevels];
+  int64_t lev_cnt[kMaxLevels];
+  int nlev;
+  int64_t n;
+  double Lx, Ly, Lz, xyzlong;
+  int nv;       // nvoisins (<= 32)
+  int nstore;   // neighbours written per particle
+  int32_t* nei; // [n][nstore] sorted-slot ids
+  double* dens; // [n]
+  int* err;     // error flag (stack overflow)
+};
+
+constexpr int kWarpsPerBlock = 8;
+constexpr int kStack = 256;
+
+__device__ __forceinline__ double box_dist2(const double* __restrict__ b, double qx, double qy, double qz,
+                                            double Lx, double Ly, double Lz) {
+  double dx = fabs(b[0] - qx); dx = fmin(dx, Lx - dx); dx = fmax(0.0, dx - b[3]);
+  double dy = fabs(b[1] - qy); dy = fmin(dy, Ly - dy); dy = fmax(0.0, dy - b[4]);
+  double dz = fabs(b[2] - qz); dz = fmin(dz, Lz - dz); dz = fmax(0.0, dz - b[5]);
+  return dx * dx + dy * dy + dz * dz;
+}
+
+// The warp's running neighbour list: lane i holds the i-th nearest (ld, ls, lo):
+// squared distance, sorted slot, original index; empty slots hold +inf.
+struct WarpList {
+  double ld;
+  int32_t ls, lo;
+  double r2;  // squared distance of the nv-th entry (acceptance bound)
+};
+
+__device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int64_t leaf, int64_t self, double qx,
+                                            double qy, double qz, int lane) {
+  int64_t p = leaf * kLeaf + lane;
+  bool v = (p < A.n) && (p != self);
+  double d = CUDART_INF;
+  int32_t o = INT_MAX;
+  if (v) {
+    d = pdist2(qx, qy, qz, A.x[p], A.y[p], A.z[p], A.Lx, A.Ly, A.Lz);
+    o = A.orig[p];
+  }
+  unsigned mask = __ballot_sync(0xffffffffu, v && d < L.r2);
+  while (mask) {
+    int src = __ffs(mask) - 1;
+    double cd = __shfl_sync(0xffffffffu, d, src);
+    int32_t co = __shfl_sync(0xffffffffu, o, src);
+    int32_t cs = (int32_t)(leaf * kLeaf + src);
+    bool prec = (lane < A.nv) && (L.ld < cd || (L.ld == cd && L.lo < co));
+    int pos = __popc(__ballot_sync(0xffffffffu, prec));
+    double ud = __shfl_up_sync(0xffffffffu, L.ld, 1);
+    int32_t us = __shfl_up_sync(0xffffffffu, L.ls, 1);
+    int32_t uo = __shfl_up_sync(0xffffffffu, L.lo, 1);
+    if (lane > pos) { L.ld = ud; L.ls = us; L.lo = uo; }
+    if (lane == pos) { L.ld = cd; L.ls = cs; L.lo = co; }
+    if (lane >= A.nv) { L.ld = CUDART_INF; L.ls = -1; L.lo = INT_MAX; }
+    L.r2 = __shfl_sync(0xffffffffu, L.ld, A.nv - 1);
+    mask &= ~(1u << src);
+    mask &= __ballot_sync(0xffffffffu, d < L.r2);
+  }
+}
+
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) knn_density_kernel(KnnArgs A) {
+  __shared__ int32_t s_node[kWarpsPerBlock][kStack];
+  __shared__ double s_bd[kWarpsPerBlock][kStack];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
+  const int top = A.nlev - 1;
+  for (int64_t s = (int64_t)blockIdx.x * kWarpsPerBlock + wib; s < A.n; s += nwarps) {
+    const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
+    WarpList L;
+    L.ld = CUDART_INF; L.ls = -1; L.lo = INT_MAX; L.r2 = CUDART_INF;
+    const int64_t j0 = s / kLeaf;
+    const int64_t j1 = j0 ^ 1;
+    leaf_insert(A, L, j0, s, qx, qy, qz, lane);
+    if (j1 < A.lev_cnt[0]) leaf_insert(A, L, j1, s, qx, qy, qz, lane);
+    // depth-first traversal, nearest child popped first
+    int sp = 0;
+    if (lane == 0) { s_node[wib][0] = (top << 27) | 0; s_bd[wib][0] = 0.0; }
+    sp = 1;
+    __syncwarp();
+    while (sp > 0) {
+      --sp;
+      const int32_t ent = s_node[wib][sp];
+      const double bd = s_bd[wib][sp];
+      __syncwarp();
+      if (!(bd < L.r2)) continue;
+      const int lvl = ent >> 27;
+      const int64_t j = ent & ((1 << 27) - 1);
+      if (lvl == 0) {
+        if (j == j0 || j == j1) continue;
+        leaf_insert(A, L, j, s, qx, qy, qz, lane);
+        continue;
+      }
+      const int64_t c = j * kFan + lane;
+      const bool valid = c < A.lev_cnt[lvl - 1];
+      double bdc = CUDART_INF;
+      if (valid) bdc = box_dist2(A.box + 6 * (A.lev_off[lvl - 1] + c), qx, qy, qz, A.Lx, A.Ly, A.Lz);
+      const bool cand = valid && bdc < L.r2;
+      const unsigned mask = __ballot_sync(0xffffffffu, cand);
+      if (!mask) continue;
+      const int cnt = __popc(mask);
+      if (sp + cnt > kStack) {  // cannot happen for <= 7 levels; guard anyway
+        if (lane == 0) atomicExch(A.err, 1);
+        break;
+      }
+      // nearest candidate goes on top of the stack
+      double best = cand ? bdc : CUDART_INF;
+      int bl = lane;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        int ol = __shfl_xor_sync(0xffffffffu, bl, o);
+        if (ob < best || (ob == best && ol < bl)) { best = ob; bl = ol; }
+      }
+      if (cand) {
+        int r = __popc(mask & ((1u << lane) - 1));
+        int slot;
+        if (lane == bl) slot = sp + cnt - 1;
+        else {
+          int rb = __popc(mask & ((1u << bl) - 1));
+          slot = sp + (r < rb ? r : r - 1);
+        }
+        s_node[wib][slot] = ((lvl - 1) << 27) | (int32_t)c;
+        s_bd[wib][slot] = bdc;
+      }
+      sp += cnt;
+      __syncwarp();
+    }
+    // ---- SPH density (f90:2816-2838), exact evaluation order
+    const int nv = A.nv;
+    const double dlast = __shfl_sync(0xffffffffu, L.ld, nv - 1);
+    const double r = xmul(xsqrt(dlast), 0.5);
+    const double r3 = xmul(xmul(r, r), r);
+    const double unsr = xdiv(1.0, r);
+    double term = 0.0;
+    if (lane < nv - 1) term = xmul(A.m[L.ls], spline(xmul(xsqrt(L.ld), unsr)));
+    double contrib = 0.0;
+    for (int i = 0; i < nv - 1; ++i) contrib = xadd(contrib, __shfl_sync(0xffffffffu, term, i));
+    if (lane == 0) {
+      const double pi_f = (double)3.141592654f;  // f90:58 single-precision literal
+      A.dens[s] = xdiv(xmul(A.xyzlong, xadd(contrib, A.m[s])), xmul(pi_f, r3));
+    }
+    if (lane < A.nstore) A.nei[s * A.nstore + lane] = L.ls;
+    __syncwarp();
+  }
+}
+
+int stage_knn_density(Engine& E) {
+  const int64_t n = E.n;
+  const Params& P = E.prm;
+  E.nstore = E.req_store > 0 ? E.req_store : P.nhop;
+  if (E.nstore < P.nhop) E.nstore = P.nhop;
+  if (E.nstore > P.nvoisins) E.nstore = P.nvoisins;
+  AHOP_CUDA_TRY(E.d_nei.ensure((size_t)n * E.nstore * 4));
+  AHOP_CUDA_TRY(E.d_dens.ensure(n * 8));
+  KnnArgs A;
+  A.x = E.d_x.as<double>(); A.y = E.d_y.as<double>(); A.z = E.d_z.as<double>(); A.m = E.d_m.as<double>();
+  A.orig = E.d_orig.as<int32_t>();
+  A.box = E.d_box.as<double>();
+  for (int l = 0; l < kMaxLevels; ++l) { A.lev_off[l] = E.lev_off[l]; A.lev_cnt[l] = E.lev_cnt[l]; }
+  A.nlev = E.nlev;
+  A.n = n;
+  A.Lx = P.xlong; A.Ly = P.ylong; A.Lz = P.zlong; A.xyzlong = P.xyzlong;
+  A.nv = P.nvoisins;
+  A.nstore = E.nstore;
+  A.nei = E.d_nei.as<int32_t>();
+  A.dens = E.d_dens.as<double>();
+  AHOP_CUDA_TRY(E.d_flags.ensure(64));
+  AHOP_CUDA_TRY(cudaMemsetAsync(E.d_flags.p, 0, 64, E.stream));
+  A.err = E.d_flags.as<int>();
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, E.device);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, knn_density_kernel, kWarpsPerBlock * 32, 0);
+  if (per_sm < 1) per_sm = 1;
+  int64_t want = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  int64_t grid = (int64_t)nsm * per_sm * 4;
+  if (grid > want) grid = want;
+  knn_density_kernel<<<(unsigned)grid, kWarpsPerBlock * 32, 0, E.stream>>>(A);
+  AHOP_CUDA_TRY(cudaGetLastError());
+  int herr = 0;
+  AHOP_CUDA_TRY(cudaMemcpyAsync(&herr, E.d_flags.p, 4, cudaMemcpyDeviceToHost, E.stream));
+  AHOP_CUDA_TRY(cudaStreamSynchronize(E.stream));
+  if (herr) { set_error("kNN traversal stack overflow"); return AHOP_ELIMIT; }
+  return AHOP_OK;
+}
+
+}  // namespace ahop

@@ -1,0 +1,913 @@
+// Structure tree of hop groups ("create nodes"); replaces create_group_tree,
+// omp_dev_create_nodes_task, dev_do_colorize_local, treat_particles and
+// reorder_nodes_deterministic (f90:885-1131, 1188-1628, 2317-2429).
+//
+// Execution model.  A task is (node, threshold rhot, contiguous range of the
+// group list GL).  Tasks run one CUDA block each, in waves: a block runs the
+// Fortran task loop for its task -- percolate the groups above rhot through
+// saddles > rhot, measure every component, test significance -- until the
+// task branches (nsisters > 1: child nodes are created and their tasks queued
+// for the next wave) or ends.  The nsisters == 1 chain, which the reference
+// runs serially level after level, stays inside the block.
+//
+// Order.  GL keeps the reference's igr order (f90:1337-1367): components are
+// contiguous, ordered by their smallest position before the level, and keep
+// their previous relative order inside.  Components are found with a
+// block-level union-find over saddle edges > rhot linking to the smaller
+// position, then reordered by a chunked stable radix sort on the root.  The
+// structure can only change when rhot crosses a saddle value or a group peak
+// density of the task, so this pass is skipped at levels below the next such
+// value.
+//
+// Sums.  The significance tests (f90:1459-1463) need, per component, the
+// number of member particles above rhot (exact integer), the maximum group
+// peak density (exact) and density/position sums that the reference
+// accumulates sequentially.  Per level they are taken from running sums over
+// each group's members sorted by decreasing density (an O(log n) lookup per
+// group instead of the reference's rescan of every member) and carry a
+// rigorous rounding bound; a test whose outcome lies within that bound, and
+// every node that is actually created, is recomputed in the reference's exact
+// order: members in decreasing particle index, groups in GL order, posref and
+// periodic unwrapping as in treat_particles (f90:2337-2386).  Node outputs
+// are therefore the reference's sums bit for bit.
+//
+// Membership.  A child task paints the members of its groups that lie above
+// its creation threshold (f90:1297-1306); later (deeper) paints win.  The
+// final node of a particle is therefore the deepest node containing its group
+// whose rho_saddle is below the particle density; it is computed per particle
+// after the waves.
+#include <cub/cub.cuh>
+#include <cfloat>
+#include <climits>
+
+#include "engine.h"
+#include "exact.cuh"
+
+namespace ahop {
+
+constexpr int kNT = 256;        // threads per task block
+constexpr int kIPT = 4;         // items per thread in the reorder sort
+constexpr int kChunk = kNT * kIPT;
+constexpr long long kMaxTaskLevels = 4000000LL;  // cap on one task's threshold levels (error, never a hang)
+
+struct Task {
+  double rhot;
+  int32_t inode, a, b, level;
+};
+
+struct TreeArgs {
+  // particles (sorted order)
+  const double *x, *y, *z, *m, *dens;
+  const int32_t* orig;
+  // groups (1-based ids)
+  int32_t ngroups;
+  const double* densg;
+  const int32_t* gpeak;
+  const int32_t* goff;    // [ng+2] member offsets
+  const int32_t* gmem;    // members, decreasing particle index
+  const double* rdesc;    // member densities, decreasing density (same offsets)
+  const double* pref;     // [nact][6] running sums in decreasing-density order:
+                          // rho, m, m*dx, m*dy, m*dz, m*|d|^2 (d relative to the group peak)
+  // saddles
+  const int32_t* soff;    // [ng+1] row g at [soff[g-1], soff[g])
+  const int32_t* sisad;
+  const double* srho;
+  // parameters
+  double Lx, Ly, Lz, hx, hy, hz;  // box and half box (xlongs2...)
+  double fudge, alphap, epsilon;
+  int32_t nmembthresh;
+  // tree state
+  int32_t* GL;            // [ng] group list
+  int32_t* GL2;           // [ng] reorder target
+  int32_t* pos_of;        // [ng+1] position of each group in GL
+  int32_t* par;           // [ng] union-find parent (absolute positions)
+  int32_t* cnt;           // [ng] component sizes by root / running ranks
+  int32_t* run;           // [ng]
+  int32_t* cstart;        // [ng] component k of a task starts at cstart[a+k]
+  int32_t* compidx;       // [ng] component index of each position
+  int32_t* gn;            // [ng] per-position member count above rhot
+  double* gs;             // [ng][8] per-position scratch sums
+  double* cs;             // [ng][12] per-component scratch
+  int32_t* deepnode;      // [ng+1]
+  NodeRec* node;          // [nnodesmax+1]
+  int32_t nnodesmax;
+  int32_t* nnodes;        // counter
+  Task* next;
+  int32_t* nnext;
+  int32_t* err;           // [0] code, [1] detail
+};
+
+__device__ __forceinline__ void set_err(const TreeArgs& A, int code, int detail) {
+  if (atomicCAS(A.err, 0, code) == 0) A.err[1] = detail;
+}
+
+__device__ __forceinline__ double wrapd(double d, double L, double h) {
+  // f90:2359-2373 / 1516-1532
+  if (d >= h) return xsub(d, L);
+  if (d < -h) return xadd(d, L);
+  return d;
+}
+
+// number of members of group g with density > rhot (members sorted by decreasing density)
+__device__ __forceinline__ int32_t count_above(const TreeArgs& A, int32_t g, double rhot) {
+  int32_t lo = A.goff[g], hi = A.goff[g + 1];  // find first index with rdesc <= rhot
+  while (lo < hi) {
+    int32_t mid = (lo + hi) >> 1;
+    if (A.rdesc[mid] > rhot) lo = mid + 1; else hi = mid;
+  }
+  return lo - A.goff[g];
+}
+
+__device__ int32_t uf_find(int32_t* par, int32_t i) {
+  // path halving; every chain ends at a self-parent
+  for (int it = 0; it < (1 << 26); ++it) {
+    int32_t p = par[i];
+    if (p == i) return i;
+    int32_t gp = par[p];
+    if (gp != p) atomicCAS(&par[i], p, gp);
+    i = gp;
+  }
+  return i;
+}
+
+__device__ void uf_union(int32_t* par, int32_t i, int32_t j) {
+  for (int it = 0; it < (1 << 26); ++it) {
+    i = uf_find(par, i);
+    j = uf_find(par, j);
+    if (i == j) return;
+    if (i < j) { int32_t t = i; i = j; j = t; }  // link the larger root under the smaller
+    if (atomicCAS(&par[i], i, j) == i) return;
+  }
+}
+
+__device__ __forceinline__ double atomic_min_pos(double* addr, double v) {
+  // non-negative doubles order like their bit patterns
+  unsigned long long* a = reinterpret_cast<unsigned long long*>(addr);
+  unsigned long long nv = __double_as_longlong(v);
+  unsigned long long old = atomicMin(a, nv);
+  return __longlong_as_double(old);
+}
+
+// -------------------------------------------------------------------------
+// Structural pass at rhot over positions [a, b): drop groups with peak
+// density <= rhot, percolate through saddles > rhot, reorder components.
+// Returns (in shared) new b, ncomp, and the next threshold at which the
+// structure can change.
+struct SharedTask {
+  double rhot;
+  double next_event;
+  int32_t inode, a, b, level, ncomp, nsurv, nsisters, done, nexact, inode1;
+  int32_t flag;
+  long long iters;
+};
+
+template <class SortT, class ScanT, class MaxScanT>
+__device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT::TempStorage& sort_tmp,
+                                typename ScanT::TempStorage& scan_tmp, typename MaxScanT::TempStorage& maxscan_tmp,
+                                int32_t* s_keys) {
+  const int tid = threadIdx.x;
+  const int32_t a = T.a, b = T.b;
+  const double rhot = T.rhot;
+  if (tid == 0) T.next_event = DBL_MAX;
+  for (int32_t i = a + tid; i < b; i += kNT) {
+    A.par[i] = i;
+    A.cnt[i] = 0;
+    A.run[i] = 0;
+  }
+  __syncthreads();
+  // union over saddle edges above rhot (rows sorted by decreasing saddle)
+  for (int32_t i = a + tid; i < b; i += kNT) {
+    int32_t g = A.GL[i];
+    double dg = A.densg[g];
+    if (!(dg > rhot)) continue;
+    atomic_min_pos(&T.next_event, dg);
+    int32_t e0 = A.soff[g - 1], e1 = A.soff[g];
+    for (int32_t e = e0; e < e1; ++e) {
+      double r = A.srho[e];
+      if (!(r > rhot)) break;
+      atomic_min_pos(&T.next_event, r);
+      int32_t j = A.pos_of[A.sisad[e]];
+      if (j < a || j >= b) { set_err(A, 11, g); continue; }  // f90:1229-1233
+      uf_union(A.par, i, j);
+    }
+  }
+  __syncthreads();
+  for (int32_t i = a + tid; i < b; i += kNT) {
+    int32_t g = A.GL[i];
+    if (A.densg[g] > rhot) {
+      int32_t r = uf_find(A.par, i);
+      A.par[i] = r;
+      atomicAdd(&A.cnt[r], 1);
+    } else {
+      A.par[i] = -1;
+    }
+  }
+  __syncthreads();
+  // exclusive scan of component sizes over root positions -> component offsets (in cnt)
+  int32_t carry = 0;
+  for (int32_t c0 = a; c0 < b; c0 += kNT) {
+    int32_t i = c0 + tid;
+    int32_t v = (i < b) ? A.cnt[i] : 0;
+    int32_t ex, tot;
+    ScanT(scan_tmp).ExclusiveSum(v, ex, tot);
+    __syncthreads();
+    if (i < b) A.cnt[i] = carry + ex;
+    carry += tot;
+    __syncthreads();
+  }
+  const int32_t nsurv = carry;
+  // stable reorder by root, chunk by chunk: inside a chunk a stable block
+  // radix sort groups equal roots; a run's rank is its offset from the run
+  // head (block max-scan of head indices); run[] carries ranks across chunks
+  for (int32_t c0 = a; c0 < b; c0 += kChunk) {
+    int32_t keys[kIPT], vals[kIPT];
+#pragma unroll
+    for (int k = 0; k < kIPT; ++k) {
+      int32_t i = c0 + tid * kIPT + k;
+      int32_t r = (i < b) ? A.par[i] : -1;
+      keys[k] = (r >= 0) ? (r - a) : INT_MAX;
+      vals[k] = i;
+    }
+    SortT(sort_tmp).Sort(keys, vals);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kIPT; ++k) s_keys[tid * kIPT + k] = keys[k];
+    __syncthreads();
+    int32_t headq[kIPT];
+#pragma unroll
+    for (int k = 0; k < kIPT; ++k) {
+      int q = tid * kIPT + k;
+      headq[k] = (q == 0 || s_keys[q - 1] != keys[k]) ? q : 0;
+    }
+    MaxScanT(maxscan_tmp).InclusiveScan(headq, headq, cub::Max());
+    bool tail[kIPT];
+#pragma unroll
+    for (int k = 0; k < kIPT; ++k) {
+      int q = tid * kIPT + k;
+      tail[k] = (q == kChunk - 1) || (s_keys[q + 1] != keys[k]);
+      if (keys[k] == INT_MAX) continue;
+      int32_t r = keys[k] + a;
+      int32_t np = a + A.cnt[r] + A.run[r] + (q - headq[k]);
+      if (np < a || np >= b) { set_err(A, 17, np); continue; }
+      A.GL2[np] = A.GL[vals[k]];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kIPT; ++k) {
+      int q = tid * kIPT + k;
+      if (tail[k] && keys[k] != INT_MAX) A.run[keys[k] + a] += q - headq[k] + 1;
+    }
+    __syncthreads();
+  }
+  // copy back, positions, component starts
+  for (int32_t i = a + tid; i < a + nsurv; i += kNT) {
+    int32_t g = A.GL2[i];
+    A.GL[i] = g;
+    A.pos_of[g] = i;
+  }
+  __syncthreads();
+  // component starts: root positions r (par[r] == r before reorder) map to start a + cnt[r]
+  // collect them in order with a scan over root flags
+  carry = 0;
+  for (int32_t c0 = a; c0 < b; c0 += kNT) {
+    int32_t i = c0 + tid;
+    int32_t isroot = (i < b && A.par[i] == i) ? 1 : 0;
+    int32_t ex, tot;
+    ScanT(scan_tmp).ExclusiveSum(isroot, ex, tot);
+    __syncthreads();
+    if (isroot) A.cstart[a + carry + ex] = a + A.cnt[i];
+    carry += tot;
+    __syncthreads();
+  }
+  if (tid == 0) {
+    T.ncomp = carry;
+    T.nsurv = nsurv;
+    T.b = a + nsurv;
+  }
+  __syncthreads();
+  for (int32_t k = tid; k < T.ncomp; k += kNT) {
+    const int32_t c1 = (k + 1 < T.ncomp) ? A.cstart[a + k + 1] : T.b;
+    for (int32_t i = A.cstart[a + k]; i < c1; ++i) A.compidx[i] = k;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ int32_t comp_end(const TreeArgs& A, const SharedTask& T, int32_t k) {
+  return (k + 1 < T.ncomp) ? A.cstart[T.a + k + 1] : T.b;
+}
+
+// -------------------------------------------------------------------------
+// Per-component quantities.  cs row (12 doubles) for component k at index a+k:
+//  0 mass_loc  1 mass_comp  2 densmax  3 sum rho  4 M  5 Sx 6 Sy 7 Sz 8 Q
+//  9 decision (0 false, 1 true, 2 unknown)  10 exact flag  11 unused
+// Exact per-component results overwrite 0..3 and set 9 to 0/1.
+
+__device__ __forceinline__ int tri_and(int p, int q) {
+  if (p == 0 || q == 0) return 0;
+  if (p == 1 && q == 1) return 1;
+  return 2;
+}
+__device__ __forceinline__ int tri_or(int p, int q) {
+  if (p == 1 || q == 1) return 1;
+  if (p == 0 && q == 0) return 0;
+  return 2;
+}
+// tri-state comparison v > t with uncertainty e on v
+__device__ __forceinline__ int tri_gt(double v, double t, double e) {
+  if (v - e > t) return 1;
+  if (v + e <= t) return 0;
+  return 2;
+}
+
+__device__ void approx_stats(const TreeArgs& A, SharedTask& T) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const double rhot = T.rhot;
+  const double u = 1.1102230246251565e-16;
+  for (int32_t k = warp; k < T.ncomp; k += kNT / 32) {
+    const int32_t c0 = A.cstart[T.a + k], c1 = comp_end(A, T, k);
+    const int32_t g0 = A.GL[c0];
+    const int32_t p0 = A.gpeak[g0];
+    const double ax = A.x[p0], ay = A.y[p0], az = A.z[p0];
+    long long nl = 0;
+    int32_t nmax = 0;
+    double dmax = -1.0, S = 0, M = 0, Sx = 0, Sy = 0, Sz = 0, Q = 0;
+    int triB = 0;  // densmoy_comp_max > rhot
+    for (int32_t i = c0 + lane; i < c1; i += 32) {
+      const int32_t g = A.GL[i];
+      const int32_t ng = count_above(A, g, rhot);
+      A.gn[i] = ng;
+      nl += ng;
+      nmax = max(nmax, ng);
+      dmax = fmax(dmax, A.densg[g]);
+      if (ng > 0) {
+        const double* P = A.pref + 6 * (size_t)(A.goff[g] + ng - 1);
+        const double sg = P[0];
+        S += sg;
+        const int32_t pg = A.gpeak[g];
+        double dx = wrapd(A.x[pg] - ax, A.Lx, A.hx), dy = wrapd(A.y[pg] - ay, A.Ly, A.hy),
+               dz = wrapd(A.z[pg] - az, A.Lz, A.hz);
+        const double mg = P[1];
+        M += mg;
+        Sx += P[2] + mg * dx;
+        Sy += P[3] + mg * dy;
+        Sz += P[4] + mg * dz;
+        Q += P[5] + 2.0 * (dx * P[2] + dy * P[3] + dz * P[4]) + mg * (dx * dx + dy * dy + dz * dz);
+        const double dn = (double)ng;
+        const double vg = (sg / dn) / (1.0 + A.fudge / sqrt(dn));
+        triB = tri_or(triB, tri_gt(vg, rhot, (2.0 * dn + 8.0) * u * fabs(vg) * 1.01));
+      }
+    }
+    // warp reductions
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      nl += __shfl_xor_sync(0xffffffffu, nl, o);
+      nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+      dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+      S += __shfl_xor_sync(0xffffffffu, S, o);
+      M += __shfl_xor_sync(0xffffffffu, M, o);
+      Sx += __shfl_xor_sync(0xffffffffu, Sx, o);
+      Sy += __shfl_xor_sync(0xffffffffu, Sy, o);
+      Sz += __shfl_xor_sync(0xffffffffu, Sz, o);
+      Q += __shfl_xor_sync(0xffffffffu, Q, o);
+      triB = tri_or(triB, __shfl_xor_sync(0xffffffffu, triB, o));
+    }
+    if (lane == 0) {
+      double* C = A.cs + 12 * (size_t)(T.a + k);
+      const double n = (double)nl;
+      C[0] = n; C[1] = (double)nmax; C[2] = dmax; C[3] = S;
+      C[4] = M; C[5] = Sx; C[6] = Sy; C[7] = Sz; C[8] = Q;
+      int dec;
+      if (nl < A.nmembthresh) {
+        dec = 0;
+      } else {
+        const double dm = S / n;
+        const double edm = (2.0 * n + 8.0) * u * dm * 1.01;
+        const double thrA = xmul(rhot, xadd(1.0, xdiv(A.fudge, xsqrt(n))));
+        const int tA = tri_gt(dm, thrA, edm);
+        // dmax >= alphap * densmoy, densmoy known to +-edm
+        const double tiny = 8.0 * u * fabs(A.alphap * dm);
+        const int tC = (dmax >= A.alphap * (dm + edm) + tiny) ? 1
+                       : (dmax < A.alphap * (dm - edm) - tiny ? 0 : 2);
+        double r2 = Q / M - (Sx * Sx + Sy * Sy + Sz * Sz) / (M * M);
+        const double r = sqrt(fabs(r2));
+        const int tD = (r >= A.epsilon * (1.0 + 1e-6) + 1e-300) ? 1 : (r < A.epsilon * (1.0 - 1e-6) ? 0 : 2);
+        dec = tri_and(tri_and(tri_or(tA, triB), tC), tD);
+      }
+      C[9] = (double)dec;
+      C[10] = 0.0;
+    }
+  }
+}
+
+// Exact sums in the reference order for components flagged in cs[..][10].
+// Per-position scratch gs row: 0 imass 1 truemass 2..4 posg 5 rsquare 6 densmoy
+__device__ void exact_stats(const TreeArgs& A, SharedTask& T) {
+  const int tid = threadIdx.x;
+  const double rhot = T.rhot;
+  // phase 1: posref per flagged component (first particle above rhot of its first group)
+  for (int32_t k = tid; k < T.ncomp; k += kNT) {
+    double* C = A.cs + 12 * (size_t)(T.a + k);
+    if (C[10] == 0.0) continue;
+    const int32_t g0 = A.GL[A.cstart[T.a + k]];
+    int32_t ref = -1;
+    for (int32_t q = A.goff[g0]; q < A.goff[g0 + 1]; ++q) {
+      int32_t s = A.gmem[q];
+      if (A.dens[s] > rhot) { ref = s; break; }
+    }
+    if (ref < 0) { set_err(A, 18, g0); ref = A.gpeak[g0]; }  // cannot happen: the peak is above rhot
+    C[11] = (double)ref;
+  }
+  __syncthreads();
+  // phase 2: per group sequential sums (members in decreasing particle index)
+  for (int32_t i = T.a + tid; i < T.b; i += kNT) {
+    const int32_t k = A.compidx[i];
+    const double* C = A.cs + 12 * (size_t)(T.a + k);
+    if (C[10] == 0.0) continue;
+    const int32_t ref = (int32_t)C[11];
+    const double rx = A.x[ref], ry = A.y[ref], rz = A.z[ref];
+    const int32_t g = A.GL[i];
+    int32_t imass = 0;
+    double tm = 0, px = 0, py = 0, pz = 0, rs = 0, dm = 0;
+    for (int32_t q = A.goff[g]; q < A.goff[g + 1]; ++q) {
+      const int32_t s = A.gmem[q];
+      const double d = A.dens[s];
+      if (!(d > rhot)) continue;
+      imass += 1;
+      const double xm = A.m[s];
+      tm = xadd(tm, xm);
+      double ux = wrapd(xsub(A.x[s], rx), A.Lx, A.hx);
+      double uy = wrapd(xsub(A.y[s], ry), A.Ly, A.hy);
+      double uz = wrapd(xsub(A.z[s], rz), A.Lz, A.hz);
+      ux = xadd(ux, rx);
+      uy = xadd(uy, ry);
+      uz = xadd(uz, rz);
+      px = xadd(px, xmul(ux, xm));
+      py = xadd(py, xmul(uy, xm));
+      pz = xadd(pz, xmul(uz, xm));
+      rs = xadd(rs, xmul(xm, xadd(xadd(xmul(ux, ux), xmul(uy, uy)), xmul(uz, uz))));
+      dm = xadd(dm, d);
+    }
+    double* G = A.gs + 8 * (size_t)i;
+    G[0] = (double)imass; G[1] = tm; G[2] = px; G[3] = py; G[4] = pz; G[5] = rs; G[6] = dm;
+  }
+  __syncthreads();
+  // phase 3: fold over groups in GL order and test (f90:1407-1466)
+  for (int32_t k = tid; k < T.ncomp; k += kNT) {
+    double* C = A.cs + 12 * (size_t)(T.a + k);
+    if (C[10] == 0.0) continue;
+    const int32_t c0 = A.cstart[T.a + k], c1 = comp_end(A, T, k);
+    double posg0 = 0, posg1 = 0, posg2 = 0, tm = 0, rsg = 0, dmg = 0, dmax = -1.0, dcm = -1.0;
+    int32_t ml = 0, mc = 0;
+    for (int32_t i = c0; i < c1; ++i) {
+      const double* G = A.gs + 8 * (size_t)i;
+      const int32_t g = A.GL[i];
+      dmax = fmax(dmax, A.densg[g]);
+      const int32_t mt = (int32_t)G[0];
+      posg0 = xadd(posg0, G[2]);
+      posg1 = xadd(posg1, G[3]);
+      posg2 = xadd(posg2, G[4]);
+      rsg = xadd(rsg, G[5]);
+      ml += mt;
+      tm = xadd(tm, G[1]);
+      dmg = xadd(dmg, G[6]);
+      mc = max(mc, mt);
+      if (mt > 0) {
+        const double dmt = xdiv(G[6], (double)mt);
+        dcm = fmax(dcm, xdiv(dmt, xadd(1.0, xdiv(A.fudge, xsqrt((double)mt)))));
+      }
+    }
+    const double p2 = xadd(xadd(xmul(posg0, posg0), xmul(posg1, posg1)), xmul(posg2, posg2));
+    const double rsq = xsqrt(fabs(xdiv(xsub(xmul(tm, rsg), p2), xmul(tm, tm))));
+    const double densmoy = xdiv(dmg, (double)ml);
+    const bool ok = ml >= A.nmembthresh &&
+                    (densmoy > xmul(rhot, xadd(1.0, xdiv(A.fudge, xsqrt((double)ml)))) || dcm > rhot) &&
+                    dmax >= xmul(A.alphap, densmoy) && rsq >= A.epsilon;
+    // exact record: 0 mass_loc 1 mass_comp 2 densmax 3 densmoy 4 truemass 5..7 posg 8 radius 9 decision
+    C[0] = (double)ml; C[1] = (double)mc; C[2] = dmax; C[3] = densmoy; C[4] = tm;
+    C[5] = posg0; C[6] = posg1; C[7] = posg2; C[8] = rsq; C[9] = ok ? 1.0 : 0.0;
+  }
+  __syncthreads();
+}
+
+template <class SortT, class ScanT, class MaxScanT>
+__global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* __restrict__ tasks) {
+  __shared__ typename SortT::TempStorage sort_tmp;
+  __shared__ typename ScanT::TempStorage scan_tmp;
+  __shared__ typename MaxScanT::TempStorage maxscan_tmp;
+  __shared__ int32_t s_keys[kChunk];
+  __shared__ SharedTask T;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    const Task t = tasks[blockIdx.x];
+    T.rhot = t.rhot; T.inode = t.inode; T.a = t.a; T.b = t.b; T.level = t.level;
+    T.next_event = -DBL_MAX;  // force a structural pass first
+    T.nsurv = 0;
+    T.ncomp = 0;
+    T.done = 0;
+    T.iters = 0;
+  }
+  __syncthreads();
+  while (true) {
+    if (T.rhot >= T.next_event) structural_pass<SortT, ScanT, MaxScanT>(A, T, sort_tmp, scan_tmp, maxscan_tmp, s_keys);
+    if (T.nsurv == 0) {  // all groups below the threshold (f90:1348-1351 prints, then ends with no colour)
+      if (tid == 0) A.node[T.inode].firstchild = 0;
+      break;
+    }
+    approx_stats(A, T);
+    __syncthreads();
+    // flag unknown decisions for exact recomputation
+    if (tid == 0) T.nexact = 0;
+    __syncthreads();
+    for (int32_t k = tid; k < T.ncomp; k += kNT) {
+      double* C = A.cs + 12 * (size_t)(T.a + k);
+      if (C[9] == 2.0) { C[10] = 1.0; atomicAdd(&T.nexact, 1); }
+    }
+    __syncthreads();
+    if (T.nexact > 0) exact_stats(A, T);
+    // count significant components
+    if (tid == 0) {
+      int32_t ns = 0;
+      for (int32_t k = 0; k < T.ncomp; ++k) ns += (A.cs[12 * (size_t)(T.a + k) + 9] == 1.0);
+      T.nsisters = ns;
+    }
+    __syncthreads();
+    const int32_t ns = T.nsisters;
+    if (ns == 0) {
+      if (tid == 0) A.node[T.inode].firstchild = 0;
+      break;
+    }
+    if (ns == 1) {
+      if (tid == 0) {
+        int32_t kk = 0;
+        for (int32_t k = 0; k < T.ncomp; ++k)
+          if (A.cs[12 * (size_t)(T.a + k) + 9] == 1.0) kk = k;
+        const double mc = A.cs[12 * (size_t)(T.a + kk) + 1];
+        const double rnew = xmul(T.rhot, xadd(1.0, xdiv(A.fudge, xsqrt(mc))));
+        if (T.nsurv > 1) {
+          T.rhot = rnew;
+          T.done = 0;
+        } else {
+          A.node[T.inode].firstchild = 0;
+          T.done = 1;
+        }
+        T.iters += 1;
+        if (T.iters > kMaxTaskLevels) { set_err(A, 12, T.inode); T.done = 1; }
+      }
+      __syncthreads();
+      if (T.done) break;
+      continue;
+    }
+    // ---- branching: exact sums for the significant components, then nodes
+    for (int32_t k = tid; k < T.ncomp; k += kNT) {
+      double* C = A.cs + 12 * (size_t)(T.a + k);
+      C[10] = (C[9] == 1.0) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    exact_stats(A, T);
+    if (tid == 0) {
+      int32_t ns2 = 0;
+      for (int32_t k = 0; k < T.ncomp; ++k) ns2 += (A.cs[12 * (size_t)(T.a + k) + 9] == 1.0);
+      // the exact pass only recomputes components already decided significant
+      if (ns2 != ns) set_err(A, 13, T.inode);
+      const int32_t first = atomicAdd(A.nnodes, ns) + 1;
+      if (first + ns - 1 > A.nnodesmax) { set_err(A, 14, first); ns2 = 0; }
+      T.inode1 = first;
+      T.nsisters = (ns2 == ns) ? ns : 0;
+    }
+    __syncthreads();
+    if (T.nsisters == 0) break;
+    if (tid == 0) {
+      int32_t is = 0;
+      for (int32_t k = 0; k < T.ncomp; ++k) {
+        const double* C = A.cs + 12 * (size_t)(T.a + k);
+        if (C[9] != 1.0) continue;
+        const int32_t io = T.inode1 + is;
+        NodeRec& nd = A.node[io];
+        nd.mother = T.inode;
+        nd.densmax = C[2];
+        nd.sister = is > 0 ? io - 1 : 0;
+        nd.nsisters = T.nsisters;
+        nd.mass = (int32_t)C[0];
+        nd.truemass = C[4];
+        double pf0 = xdiv(C[5], C[4]), pf1 = xdiv(C[6], C[4]), pf2 = xdiv(C[7], C[4]);
+        nd.radius = C[8];
+        nd.density = C[3];
+        if (pf0 >= A.hx) pf0 = xsub(pf0, A.Lx); else if (pf0 < -A.hx) pf0 = xadd(pf0, A.Lx);
+        if (pf1 >= A.hy) pf1 = xsub(pf1, A.Ly); else if (pf1 < -A.hy) pf1 = xadd(pf1, A.Ly);
+        if (pf2 >= A.hz) pf2 = xsub(pf2, A.Lz); else if (pf2 < -A.hz) pf2 = xadd(pf2, A.Lz);
+        nd.pos[0] = pf0; nd.pos[1] = pf1; nd.pos[2] = pf2;
+        nd.rho_saddle = T.rhot;
+        nd.level = T.level + 1;
+        nd.firstchild = 0;
+        if (nd.mass == 0) set_err(A, 15, io);  // f90:1506-1510
+        // child task (f90:1543-1556)
+        const double rc = xmul(T.rhot, xadd(1.0, xdiv(A.fudge, xsqrt(C[1]))));
+        const int32_t slot = atomicAdd(A.nnext, 1);
+        A.next[slot] = Task{rc, io, A.cstart[T.a + k], comp_end(A, T, k), T.level + 1};
+        ++is;
+      }
+      A.node[T.inode].firstchild = T.inode1 + T.nsisters - 1;  // f90:1540
+    }
+    __syncthreads();
+    // deepest node per group
+    {
+      int32_t is = 0;
+      for (int32_t k = 0; k < T.ncomp; ++k) {
+        const double* C = A.cs + 12 * (size_t)(T.a + k);
+        if (C[9] != 1.0) continue;
+        const int32_t io = T.inode1 + is;
+        for (int32_t i = A.cstart[T.a + k] + tid; i < comp_end(A, T, k); i += kNT) A.deepnode[A.GL[i]] = io;
+        ++is;
+      }
+    }
+    break;
+  }
+}
+
+// ------------------------------------------------------- setup / membership / order
+__global__ void init_groups_kernel(int32_t ng, int32_t* GL, int32_t* pos_of, int32_t* deepnode) {
+  int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ng) {
+    GL[i] = i + 1;
+    pos_of[i + 1] = i;
+  }
+  if (i <= ng) deepnode[i] = 0;
+}
+
+// per-group members in decreasing density: gather keys for the segmented sort
+__global__ void gather_member_rho(const int32_t* __restrict__ gmem, const double* __restrict__ dens, int64_t m,
+                                  double* __restrict__ rho) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < m) rho[i] = dens[gmem[i]];
+}
+
+// running sums per group (one warp per group) in decreasing-density order
+__global__ void prefix_moments_kernel(const int32_t* __restrict__ goff, int32_t ng,
+                                      const int32_t* __restrict__ mem_rho_order, const double* __restrict__ rdesc,
+                                      const int32_t* __restrict__ gpeak, const double* __restrict__ x,
+                                      const double* __restrict__ y, const double* __restrict__ z,
+                                      const double* __restrict__ mm, double Lx, double Ly, double Lz,
+                                      double hx, double hy, double hz, double* __restrict__ pref) {
+  const int lane = threadIdx.x & 31;
+  const int32_t g = (int32_t)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) + 1;
+  if (g > ng) return;
+  const int32_t p = gpeak[g];
+  const double ax = x[p], ay = y[p], az = z[p];
+  double c[6] = {0, 0, 0, 0, 0, 0};
+  for (int32_t base = goff[g]; base < goff[g + 1]; base += 32) {
+    const int32_t q = base + lane;
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    if (q < goff[g + 1]) {
+      const int32_t s = mem_rho_order[q];
+      const double w = mm[s];
+      double dx = wrapd(x[s] - ax, Lx, hx), dy = wrapd(y[s] - ay, Ly, hy), dz = wrapd(z[s] - az, Lz, hz);
+      v[0] = rdesc[q]; v[1] = w; v[2] = w * dx; v[3] = w * dy; v[4] = w * dz;
+      v[5] = w * (dx * dx + dy * dy + dz * dz);
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+      for (int t = 0; t < 6; ++t) {
+        double up = __shfl_up_sync(0xffffffffu, v[t], o);
+        if (lane >= o) v[t] += up;
+      }
+    }
+    if (q < goff[g + 1]) {
+#pragma unroll
+      for (int t = 0; t < 6; ++t) pref[6 * (size_t)q + t] = c[t] + v[t];
+    }
+#pragma unroll
+    for (int t = 0; t < 6; ++t) c[t] += __shfl_sync(0xffffffffu, v[t], 31);
+  }
+}
+
+__global__ void membership_kernel(const int32_t* __restrict__ group, const double* __restrict__ dens,
+                                  const int32_t* __restrict__ orig, const int32_t* __restrict__ deepnode,
+                                  const NodeRec* __restrict__ node, int64_t n, int32_t* __restrict__ liste,
+                                  int32_t* err) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  int32_t g = group[s];
+  int32_t nd = 0;
+  if (g > 0) {
+    nd = deepnode[g];
+    const double d = dens[s];
+    int guard = 0;
+    while (nd > 0 && !(d > node[nd].rho_saddle)) {
+      nd = node[nd].mother;
+      if (++guard > 100000) { atomicExch(err, 16); nd = 0; break; }
+    }
+  }
+  liste[orig[s]] = nd;
+}
+
+struct NodeLess {
+  const NodeRec* node;
+  __device__ bool operator()(int32_t ia, int32_t ib) const {
+    // node_precedes (f90:1083-1131)
+    const NodeRec& a = node[ia];
+    const NodeRec& b = node[ib];
+    if (a.level != b.level) return a.level < b.level;
+    if (a.truemass != b.truemass) return a.truemass > b.truemass;
+    if (a.mass != b.mass) return a.mass > b.mass;
+    if (a.densmax != b.densmax) return a.densmax > b.densmax;
+    if (a.density != b.density) return a.density > b.density;
+    if (a.rho_saddle != b.rho_saddle) return a.rho_saddle > b.rho_saddle;
+    for (int k = 0; k < 3; ++k)
+      if (a.pos[k] != b.pos[k]) return a.pos[k] < b.pos[k];
+    return ia < ib;
+  }
+};
+
+__global__ void iota_kernel(int32_t* v, int32_t n, int32_t base) {
+  int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = i + base;
+}
+
+__global__ void old_to_new_kernel(const int32_t* __restrict__ new_to_old, int32_t nn, int32_t* __restrict__ o2n) {
+  int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nn) o2n[new_to_old[k]] = k + 1;
+  if (k == 0) o2n[0] = 0;
+}
+
+__global__ void tables_kernel(const NodeRec* __restrict__ node, const int32_t* __restrict__ new_to_old,
+                              const int32_t* __restrict__ o2n, int32_t nn, double* __restrict__ rt,
+                              int32_t* __restrict__ it) {
+  int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nn) return;
+  const NodeRec& d = node[new_to_old[k]];
+  double* r = rt + 8 * (size_t)k;
+  r[0] = d.rho_saddle; r[1] = d.density; r[2] = d.densmax; r[3] = d.radius; r[4] = d.truemass;
+  r[5] = d.pos[0]; r[6] = d.pos[1]; r[7] = d.pos[2];
+  int32_t* t = it + 6 * (size_t)k;
+  t[0] = d.mass; t[1] = d.level;
+  t[2] = d.mother > 0 ? o2n[d.mother] : d.mother;
+  t[3] = d.firstchild > 0 ? o2n[d.firstchild] : d.firstchild;
+  t[4] = d.nsisters;
+  t[5] = d.sister > 0 ? o2n[d.sister] : d.sister;
+}
+
+__global__ void remap_liste_kernel(int32_t* __restrict__ liste, int64_t n, const int32_t* __restrict__ o2n) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int32_t v = liste[i];
+  if (v > 0) liste[i] = o2n[v];
+}
+
+int stage_nodes(Engine& E) {
+  const int64_t n = E.n;
+  const Params& P = E.prm;
+  cudaStream_t st = E.stream;
+  const int32_t ng = E.ngroups;
+  const int T = 256;
+  AHOP_CUDA_TRY(E.d_liste.ensure(n * 4));
+  E.nnodes = 0;
+  if (ng == 0) {
+    AHOP_CUDA_TRY(cudaMemsetAsync(E.d_liste.p, 0, n * 4, st));
+    return AHOP_OK;
+  }
+  const int64_t nact = E.nactive;
+  const int32_t nnodesmax = 2 * ng;  // f90:906
+  // ---- per-group members by decreasing density + running sums
+  AHOP_CUDA_TRY(E.d_gmem_rho.ensure(nact * 8 * 2 + 8));
+  AHOP_CUDA_TRY(E.d_gmem_rho_pref.ensure(nact * 8 * 6 + 8));
+  AHOP_CUDA_TRY(E.d_sad_val2.ensure((size_t)nact * 4 + 8));  // member order by density
+  double* rho_idx = E.d_gmem_rho.as<double>();        // densities in particle-index order
+  double* rdesc = E.d_gmem_rho.as<double>() + nact;   // sorted decreasing
+  int32_t* mem_rho = reinterpret_cast<int32_t*>(E.d_sad_val2.p);
+  gather_member_rho<<<(unsigned)((nact + T - 1) / T), T, 0, st>>>(E.d_gmem.as<int32_t>(), E.d_dens.as<double>(),
+                                                                  nact, rho_idx);
+  AHOP_CUDA_TRY(cudaGetLastError());
+  size_t tmp = 0;
+  cub::DeviceSegmentedSort::SortPairsDescending(nullptr, tmp, rho_idx, rdesc, E.d_gmem.as<int32_t>(), mem_rho,
+                                                (int)nact, ng, E.d_goff.as<int32_t>() + 1,
+                                                E.d_goff.as<int32_t>() + 2, st);
+  AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
+  AHOP_CUDA_TRY(cub::DeviceSegmentedSort::SortPairsDescending(E.d_cub.p, tmp, rho_idx, rdesc,
+                                                              E.d_gmem.as<int32_t>(), mem_rho, (int)nact, ng,
+                                                              E.d_goff.as<int32_t>() + 1,
+                                                              E.d_goff.as<int32_t>() + 2, st));
+  {
+    int64_t threads = (int64_t)ng * 32;
+    prefix_moments_kernel<<<(unsigned)((threads + T - 1) / T), T, 0, st>>>(
+        E.d_goff.as<int32_t>(), ng, mem_rho, rdesc, E.d_gpeak.as<int32_t>(), E.d_x.as<double>(),
+        E.d_y.as<double>(), E.d_z.as<double>(), E.d_m.as<double>(), P.xlong, P.ylong, P.zlong, P.xlongs2,
+        P.ylongs2, P.zlongs2, E.d_gmem_rho_pref.as<double>());
+    AHOP_CUDA_TRY(cudaGetLastError());
+  }
+  // ---- tree scratch
+  const size_t G = (size_t)ng + 1;
+  const size_t bytes_i = G * 4;
+  const size_t need = bytes_i * 10 + G * 8 * 8 + G * 12 * 8 + (size_t)(nnodesmax + 1) * sizeof(Task) * 2 + 256;
+  AHOP_CUDA_TRY(E.d_tree_scratch.ensure(need));
+  char* p = static_cast<char*>(E.d_tree_scratch.p);
+  auto take = [&](size_t b) { char* q = p; p += (b + 255) & ~size_t(255); return q; };
+  TreeArgs A;
+  A.GL = reinterpret_cast<int32_t*>(take(bytes_i));
+  A.GL2 = reinterpret_cast<int32_t*>(take(bytes_i));
+  A.pos_of = reinterpret_cast<int32_t*>(take(bytes_i));
+  A.par = reinterpret_cast<int32_t*>(take(bytes_i));
+  A.cnt = reinterpret_cast<int32_t*>(take(bytes_i));
+  A.run = reinterpret_cast<int32_t*>(take(bytes_i));
+  A.cstart = reinterpret_cast<int32_t*>(take(bytes_i));
+  A.compidx = reinterpret_cast<int32_t*>(take(bytes_i));
+  A.gn = reinterpret_cast<int32_t*>(take(bytes_i));
+  A.deepnode = reinterpret_cast<int32_t*>(take(bytes_i));
+  A.gs = reinterpret_cast<double*>(take(G * 8 * 8));
+  A.cs = reinterpret_cast<double*>(take(G * 12 * 8));
+  Task* tasks[2];
+  tasks[0] = reinterpret_cast<Task*>(take((size_t)(nnodesmax + 1) * sizeof(Task)));
+  tasks[1] = reinterpret_cast<Task*>(take((size_t)(nnodesmax + 1) * sizeof(Task)));
+  AHOP_CUDA_TRY(E.d_nodes.ensure((size_t)(nnodesmax + 1) * sizeof(NodeRec)));
+  AHOP_CUDA_TRY(cudaMemsetAsync(E.d_nodes.p, 0, (size_t)(nnodesmax + 1) * sizeof(NodeRec), st));
+  AHOP_CUDA_TRY(E.d_flags.ensure(64));
+  AHOP_CUDA_TRY(cudaMemsetAsync(E.d_flags.p, 0, 64, st));
+  int32_t* flags = E.d_flags.as<int32_t>();  // [0..1] err, [2] nnodes, [3] nnext
+  A.err = flags;
+  A.nnodes = flags + 2;
+  A.nnext = flags + 3;
+  A.x = E.d_x.as<double>(); A.y = E.d_y.as<double>(); A.z = E.d_z.as<double>(); A.m = E.d_m.as<double>();
+  A.dens = E.d_dens.as<double>();
+  A.orig = E.d_orig.as<int32_t>();
+  A.ngroups = ng;
+  A.densg = E.d_densg.as<double>();
+  A.gpeak = E.d_gpeak.as<int32_t>();
+  A.goff = E.d_goff.as<int32_t>();
+  A.gmem = E.d_gmem.as<int32_t>();
+  A.rdesc = rdesc - 0;  // indexed with goff (which starts group 1 at 0)
+  A.pref = E.d_gmem_rho_pref.as<double>();
+  A.soff = E.d_soff.as<int32_t>();
+  A.sisad = E.d_sisad.as<int32_t>();
+  A.srho = E.d_srho.as<double>();
+  A.Lx = P.xlong; A.Ly = P.ylong; A.Lz = P.zlong; A.hx = P.xlongs2; A.hy = P.ylongs2; A.hz = P.zlongs2;
+  A.fudge = P.fudge; A.alphap = P.alphap; A.epsilon = P.epsilon; A.nmembthresh = P.nmembthresh;
+  A.node = E.d_nodes.as<NodeRec>();
+  A.nnodesmax = nnodesmax;
+  init_groups_kernel<<<(unsigned)((ng + 1 + T - 1) / T), T, 0, st>>>(ng, A.GL, A.pos_of, A.deepnode);
+  AHOP_CUDA_TRY(cudaGetLastError());
+  // root node 0 (f90:934-943): mass and truemass stay 0, densmax = max peak density
+  {
+    Task root{P.rho_threshold, 0, 0, ng, 0};
+    AHOP_CUDA_TRY(cudaMemcpyAsync(tasks[0], &root, sizeof(Task), cudaMemcpyHostToDevice, st));
+  }
+  using SortT = cub::BlockRadixSort<int32_t, kNT, kIPT, int32_t>;
+  using ScanT = cub::BlockScan<int32_t, kNT>;
+  using MaxScanT = cub::BlockScan<int32_t, kNT>;
+  int32_t ntasks = 1;
+  int cur = 0;
+  int32_t* h = reinterpret_cast<int32_t*>(E.h_scalars);
+  for (int wave = 0; ntasks > 0; ++wave) {
+    if (wave > 100000) { set_error("structure tree: too many waves"); return AHOP_ELIMIT; }
+    A.next = tasks[cur ^ 1];
+    AHOP_CUDA_TRY(cudaMemsetAsync(A.nnext, 0, 4, st));
+    tree_wave_kernel<SortT, ScanT, MaxScanT><<<ntasks, kNT, 0, st>>>(A, tasks[cur]);
+    AHOP_CUDA_TRY(cudaGetLastError());
+    AHOP_CUDA_TRY(cudaMemcpyAsync(h, flags, 16, cudaMemcpyDeviceToHost, st));
+    AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h[0] != 0) {
+      set_error("structure tree invariant failed (code " + std::to_string(h[0]) + ", detail " +
+                std::to_string(h[1]) + ")");
+      return h[0] == 12 ? AHOP_ELIMIT : AHOP_EINVARIANT;
+    }
+    ntasks = h[3];
+    cur ^= 1;
+  }
+  const int32_t nn = h[2];
+  E.nnodes = nn;
+  // ---- membership (f90:1297-1306 paint order => deepest node above rho_saddle)
+  membership_kernel<<<(unsigned)((n + T - 1) / T), T, 0, st>>>(E.d_group.as<int32_t>(), E.d_dens.as<double>(),
+                                                              E.d_orig.as<int32_t>(), A.deepnode, A.node, n,
+                                                              E.d_liste.as<int32_t>(), flags);
+  AHOP_CUDA_TRY(cudaGetLastError());
+  // ---- deterministic renumbering (f90:987-1041)
+  AHOP_CUDA_TRY(E.d_rtab.ensure((size_t)(nn > 0 ? nn : 1) * 64));
+  AHOP_CUDA_TRY(E.d_itab.ensure((size_t)(nn > 0 ? nn : 1) * 24));
+  if (nn > 0) {
+    AHOP_CUDA_TRY(E.d_idx2.ensure((size_t)(nn + 1) * 4 * 2));
+    int32_t* new_to_old = E.d_idx2.as<int32_t>();
+    int32_t* o2n = new_to_old + nn + 1;
+    iota_kernel<<<(unsigned)((nn + T - 1) / T), T, 0, st>>>(new_to_old, nn, 1);
+    AHOP_CUDA_TRY(cudaGetLastError());
+    tmp = 0;
+    NodeLess less{A.node};
+    cub::DeviceMergeSort::SortKeys(nullptr, tmp, new_to_old, nn, less, st);
+    AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
+    AHOP_CUDA_TRY(cub::DeviceMergeSort::SortKeys(E.d_cub.p, tmp, new_to_old, nn, less, st));
+    old_to_new_kernel<<<(unsigned)((nn + T - 1) / T), T, 0, st>>>(new_to_old, nn, o2n);
+    AHOP_CUDA_TRY(cudaGetLastError());
+    tables_kernel<<<(unsigned)((nn + T - 1) / T), T, 0, st>>>(A.node, new_to_old, o2n, nn, E.d_rtab.as<double>(),
+                                                              E.d_itab.as<int32_t>());
+    AHOP_CUDA_TRY(cudaGetLastError());
+    remap_liste_kernel<<<(unsigned)((n + T - 1) / T), T, 0, st>>>(E.d_liste.as<int32_t>(), n, o2n);
+    AHOP_CUDA_TRY(cudaGetLastError());
+  }
+  AHOP_CUDA_TRY(cudaMemcpyAsync(h, flags, 8, cudaMemcpyDeviceToHost, st));
+  AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+  if (h[0] != 0) {
+    set_error("membership walk exceeded its bound");
+    return AHOP_ELIMIT;
+  }
+  return AHOP_OK;
+}
+
+}  // namespace ahop

@@ -1,0 +1,126 @@
+/* ahop_b200 — B200-native AdaptaHOP halo finder, C ABI.
+ *
+ * Drop-in for the f2py module `compute_adaptahop.neikdtree` that the reference
+ * builds from fortran/compute_adaptahop.pyf + fortran/compute_adaptahop.f90 and
+ * calls from src/compute_neiKDtree_mod.py.  Plain pointers and sizes only.
+ *
+ * Conventions
+ *  - Every entry point returns 0 on success and a nonzero AHOP_E* code on
+ *    failure; ahop_last_error() gives a one-line reason.  Nothing aborts the
+ *    process (the Fortran STOPs; this library reports instead).
+ *  - State is module-global like the Fortran module: one finder per process,
+ *    not re-entrant, one CUDA device (the current device at the first call).
+ *  - Particle positions are in [-L/2, L/2) per axis with L = xlong (=boxsize2),
+ *    laid out like the Fortran pos(3,npart): x0,y0,z0,x1,y1,z1,...
+ *  - Particle, group and node ids at this boundary are 1-based like the
+ *    Fortran; 0 means "none".
+ */
+#ifndef AHOP_B200_H
+#define AHOP_B200_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  AHOP_OK = 0,
+  AHOP_EINVAL = 1,     /* bad argument or parameter */
+  AHOP_ECUDA = 2,      /* CUDA runtime error */
+  AHOP_ENOMEM = 3,     /* device allocation failed */
+  AHOP_ESTATE = 4,     /* called out of order (e.g. outputs before compute) */
+  AHOP_EINVARIANT = 5, /* an internal consistency check failed (Fortran would STOP) */
+  AHOP_ELIMIT = 6      /* a bounded device loop hit its iteration cap */
+};
+
+/* Arguments of sync_from_init_adaptahop (fortran/compute_adaptahop.pyf:25-48,
+ * f90:591-641; called once per run from src/compute_neiKDtree_mod.py:183-197). */
+typedef struct {
+  int64_t npart;
+  int32_t nmembthresh, nMembers;
+  double omegaL, omega_lambda_f, omega0, omega_f, aexp_max, af, hubble, H_f;
+  double boxsize2, Lf, xlong, ylong, zlong, xlongs2, ylongs2, zlongs2, Hub_pt, aexp;
+  double pos_shift[3];
+} AhopInit;
+
+/* Arguments of sync_others (pyf:50-65, f90:643-678; NEI:738-747). */
+typedef struct {
+  int32_t verbose, megaverbose;
+  int32_t npart, nbPes;
+  double rho_threshold, massp, boxsize;
+  int32_t nhop, nvoisins;
+  double fudge, alphap;
+  char method[8];
+  int32_t nlevelmax, optimize_nodes;
+} AhopOthers;
+
+/* Borrowed views of the module outputs after compute (f90:485-490, node2table
+ * f90:550-573).  real_table is [nnodes][8] = rho_saddle, density, densmax,
+ * radius, truemass, x, y, z; integer_table is [nnodes][6] = mass, level,
+ * mother, firstchild, nsisters, sister.  Row k is node k+1.  Valid until the
+ * next compute or close. */
+typedef struct {
+  int64_t npart, nusedpart;
+  int32_t nnodes, ngroups;
+  const int32_t* liste_parts; /* [nusedpart] node id per particle, 0 = none */
+  const double* density;      /* [npart] */
+  const double* real_table;   /* [nnodes][8] */
+  const int32_t* integer_table; /* [nnodes][6] */
+} AhopOutputs;
+
+/* Per-stage device timings of the last compute, milliseconds (CUDA events). */
+typedef struct {
+  float upload, tree, knn_density, hop_groups, saddles, nodes, membership, download, total;
+} AhopTimings;
+
+const char* ahop_last_error(void);
+
+/* replaces sync_from_init_adaptahop (pyf:25-48, f90:591) */
+int ahop_sync_from_init_adaptahop(const AhopInit* init);
+/* replaces sync_from_change_pos (pyf:16-23, f90:576) */
+int ahop_sync_from_change_pos(int64_t npart, int32_t nusedpart, double epsilon, double fudgepsilon,
+                              double xlong, double boxsize2);
+/* replaces sync_others (pyf:50-65, f90:643) */
+int ahop_sync_others(const AhopOthers* others);
+/* replaces compute_adaptahop(pos_in, mass_in) (pyf:9-12, f90:495): host
+ * buffers pos_in[npart][3], mass_in[npart]; copies in, runs every stage on the
+ * GPU, copies the module outputs back to host memory owned by the library. */
+int ahop_compute_adaptahop(const double* pos_in, const double* mass_in, int64_t npart);
+/* The same pipeline on device-resident inputs (pos_in[npart][3] and
+ * mass_in[npart] in device memory, read on `stream`, a cudaStream_t or NULL).
+ * Outputs stay on the device; ahop_get_device_outputs exposes them. */
+int ahop_compute_adaptahop_device(const double* d_pos_in, const double* d_mass_in, int64_t npart,
+                                  void* stream);
+/* replaces the module arrays liste_parts/density/nnodes/real_table/
+ * integer_table read by src/compute_neiKDtree_mod.py:53-60 (host copies). */
+int ahop_get_outputs(AhopOutputs* out);
+/* Device-pointer view of the same outputs after either compute call. */
+int ahop_get_device_outputs(AhopOutputs* out);
+int ahop_get_timings(AhopTimings* t);
+/* replaces close (pyf:67, f90:3227): frees every module buffer. */
+int ahop_close(void);
+
+/* ---- stage views for parity tests (host copies of device intermediates) ---- */
+/* First k (<= stored count) neighbours of every particle, 1-based ids, sorted by
+ * (distance, particle id); the kNN of omp_find_nearest_parts (f90:2841). */
+int ahop_debug_neighbours(int32_t* out, int32_t k);
+/* SPH density (omp_compute_density f90:2816-2838) of every particle, caller order. */
+int ahop_debug_density(double* out);
+/* Hop target (densest of the first nhop neighbours, f90:774-795), 1-based, 0
+ * for particles at or below rho_threshold; and group id per particle after
+ * find_local_maxima (f90:819-845), 0 for none. */
+int ahop_debug_groups(int32_t* hop_target, int32_t* group_id, int32_t* ngroups);
+/* Saddle CSR (dev_compute_saddle_list f90:2433-2813) before the tree build:
+ * offsets[ngroups+1] (0-based), neighbour group ids (1-based) and saddle
+ * densities, rows in decreasing saddle density.  Pass NULLs to get nconn. */
+int ahop_debug_saddles(int32_t* nconn, int32_t* offsets, int32_t* isad, double* rho);
+/* Run the pipeline on host inputs up to stage last_stage (2 = kNN + density,
+ * 3 = hop + groups, 4 = saddles, 5 = everything) for stage-wise parity tests;
+ * the stage views above then describe that partial run. */
+int ahop_debug_compute_stages(const double* pos_in, const double* mass_in, int64_t npart, int32_t last_stage);
+/* Ask compute to keep the first k neighbours per particle (default nhop). */
+int ahop_debug_set_store_neighbours(int32_t k);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,53 @@
+"""The C-ABI library builds for sm_100a, loads and exports every declared symbol.
+
+These checks need no GPU: they load libahop_b200.so without calling into CUDA.
+"""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared(header):
+    src = open(os.path.join(REPO, "include", header)).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(ahop_\w+|halo_\w+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def libpath():
+    from ahop_b200 import build
+    return build.build()
+
+
+def test_library_exports_every_declared_symbol(libpath):
+    syms = subprocess.run(["nm", "-D", "--defined-only", libpath], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (\w+)", syms))
+    for h in os.listdir(os.path.join(REPO, "include")):
+        for name in declared(h):
+            assert name in exported, f"{name} declared in include/{h} but not exported"
+
+
+def test_library_loads_and_reports_errors(libpath):
+    lib = ctypes.CDLL(libpath)
+    lib.ahop_last_error.restype = ctypes.c_char_p
+    # argument validation happens before any CUDA call
+    assert lib.ahop_sync_others(None) == 1
+    assert b"null" in lib.ahop_last_error()
+
+
+def test_built_for_sm100a():
+    from ahop_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def test_dropin_module_surface():
+    from compute_adaptahop import neikdtree
+    for name in ("compute_adaptahop", "sync_from_change_pos", "sync_from_init_adaptahop", "sync_others", "close"):
+        assert callable(getattr(neikdtree, name))
+    for name in ("liste_parts", "density", "nnodes", "real_table", "integer_table"):
+        assert hasattr(neikdtree, name)
