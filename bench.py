@@ -1,0 +1,278 @@
+"""Benchmark: AdaptaHOP end to end on one B200 per rank (replicas), JSON line out.
+
+Workload (N=1): the 256^3 box -- 16,777,216 float64 DM particles from the
+seeded clustered generator (19,200 NFW halos with subhalos, counts 20..2e6,
+plus 40 % uniform background), nvoisins=32, nhop=16, rhot=80, fudge=4,
+fudgepsilon=1e-5, alphap=1, nmembthresh=20.
+
+  value  -- Mparticles/s of the full pipeline with pos/mass already in HBM
+            (ahop_compute_adaptahop_device), CUDA events on the compute stream;
+  e2e    -- the same metric through the public drop-in call
+            compute_adaptahop.neikdtree.compute_adaptahop(pos, mass) on host
+            buffers: host->device copies, all stages and the copy-back of the
+            module outputs inside the timed region;
+  roofline -- the fused kNN + density kernel (the dominant kernel) against the
+            measured HBM copy bandwidth;
+  cpu_baseline -- the CPU restatement of the reference finder (OpenMP, all host
+            cores) on a bounded sample: the 128^3 box from the same generator.
+
+--impl reference times that CPU restatement (the reference's own Fortran
+cannot be built: no Fortran compiler in the image) on the same sample.
+Multi-GPU: the finder does not shard (its structure tree needs a global
+merge), so --gpus N runs N independent replicas (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "halomaker-python_b200"))
+
+METRIC = "Mpart/s end-to-end vs host CPU; halo Epot pairs/s FP32-comp vs FP64 at 1e-6"
+PARAMS = dict(nvoisins=32, nhop=16, rho_threshold=80.0, fudge=4.0, fudgepsilon=1e-5, alphap=1.0, nmembthresh=20)
+WORKLOAD = dict(name="c2_256cubed", npart=16_777_216, nhalo=19_200, seed=2, nmin=20, nmax=2_000_000)
+CPU_SAMPLE = dict(name="128cubed_same_generator", npart=2_097_152, nhalo=2_400, seed=2, nmax=250_000)
+
+
+def _gen(spec):
+    from ahop_b200 import synthetic
+    return synthetic.clustered_box(spec["npart"], spec["nhalo"], seed=spec["seed"], nmax=spec["nmax"])
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample_rate(nthreads=None):
+    """Oracle (CPU restatement, OpenMP) Mparticles/s on the bounded sample."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    ps = _gen(CPU_SAMPLE)
+    prm = oracle.default_params(ps.n, nthreads=nthreads or os.cpu_count(),
+                                **{k: PARAMS[k] for k in ("nvoisins", "nhop", "rho_threshold", "fudge", "alphap",
+                                                          "nmembthresh")})
+    t = time.perf_counter()
+    r = oracle.run(ps.pos, ps.mass, prm)
+    dt = time.perf_counter() - t
+    return ps.n / dt / 1e6, dt, prm["nthreads"], r
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    rates = []
+    nth = os.cpu_count()
+    for i in range(args.warmup + args.steps):
+        rate, dt, nth, _ = cpu_sample_rate()
+        if i >= args.warmup:
+            rates.append(rate)
+    v = statistics.mean(rates)
+    sample = (f"{CPU_SAMPLE['npart']} particles ({CPU_SAMPLE['name']}, {CPU_SAMPLE['nhalo']} halos, seed "
+              f"{CPU_SAMPLE['seed']}), full finder per step")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mpart/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": CPU_SAMPLE["npart"] / v / 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD["name"], "sample": CPU_SAMPLE["name"], **PARAMS},
+            "cpu_baseline": {"value": v, "unit": "Mpart/s", "cores": nth, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "Mpart/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--npart", type=int, default=0, help="override the workload size (testing)")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from ahop_b200 import _lib as L, finder, build
+    from compute_adaptahop import neikdtree
+    build.build()
+    spec = dict(WORKLOAD)
+    if args.npart:
+        spec.update(npart=args.npart, nhalo=max(10, int(WORKLOAD["nhalo"] * args.npart / WORKLOAD["npart"])),
+                    name=f"scaled_{args.npart}")
+    ps = _gen(spec)
+    n = ps.n
+    eps = finder.configure(n, **PARAMS)
+    lib = L.lib()
+    # device-resident inputs (Fortran pos(3,n) layout == (n,3) row-major)
+    d_pos = torch.from_numpy(ps.pos).cuda()
+    d_mass = torch.from_numpy(ps.mass).cuda()
+    stream = torch.cuda.current_stream()
+
+    def dev_step():
+        L.check(lib.ahop_compute_adaptahop_device(d_pos.data_ptr(), d_mass.data_ptr(), n, C.c_void_p(stream.cuda_stream)),
+                "compute_device")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        dev_step()
+    torch.cuda.synchronize()
+    knn_ms, stage = [], []
+    with ClockSampler(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            dev_step()
+            t = L.timings()
+            knn_ms.append(t["knn_kernel"])
+            stage.append(t)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    dev_ms = e0.elapsed_time(e1)
+    if world > 1:
+        tt = torch.tensor([dev_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dev_ms = float(tt.item())
+    value = world * n * args.steps / (dev_ms / 1e3) / 1e6
+
+    # end to end through the public drop-in call on pinned host buffers
+    pos_h = torch.from_numpy(ps.pos).pin_memory().numpy()
+    mass_h = torch.from_numpy(ps.mass).pin_memory().numpy()
+    neikdtree.compute_adaptahop(pos_h.T, mass_h)  # warm
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        neikdtree.compute_adaptahop(pos_h.T, mass_h)
+        _ = int(neikdtree.nnodes)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        tt = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e = world * n * args.steps / e2e_s / 1e6
+    nnodes = int(neikdtree.nnodes)
+    d2h = n * 8 + neikdtree.liste_parts.nbytes + nnodes * (64 + 24)
+    h2d = n * 32
+
+    # roofline of the fused kNN + density kernel: 168 algorithmic bytes per particle
+    knn_avg = statistics.mean(knn_ms)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    alg = 168.0 * n
+    achieved = alg / (knn_avg / 1e3) / 1e9
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(REPO, "profiles", "knn_density_traffic.json")))
+        traffic = prof["dram_bytes_per_particle"] * n
+    except Exception:
+        pass
+    roof = {"kernel": "knn_density_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic, "alg_bytes_per_launch": alg,
+            "launch_ms": knn_avg, "peak_source": "measured" if peaks else "fallback"}
+    mean_stage = {k: statistics.mean(s[k] for s in stage) for k in
+                  ("tree", "knn_density", "hop_groups", "saddles", "nodes", "membership", "total")}
+    line = {"metric": METRIC, "value": value, "unit": "Mpart/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": spec["name"], "npart": n, "nhalo": spec["nhalo"], "seed": spec["seed"],
+                       "epsilon": eps, **PARAMS, "l2": "inputs (537 MB) larger than L2",
+                       "parallelism": f"replicas{world}"},
+            "e2e": {"value": e2e, "unit": "Mpart/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": roof, "stages_ms": mean_stage,
+            "gpu_launches": int(stage[-1]["kernel_launches"]) * args.steps,
+            "cub_calls_per_step": int(stage[-1]["cub_calls"]), "tree_waves": int(stage[-1]["tree_waves"]),
+            "nnodes": nnodes, "clocks": clk.summary()}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, dt, nth, _ = cpu_sample_rate()
+        line["cpu_baseline"] = {"value": rate, "unit": "Mpart/s", "cores": nth, "kind": "port",
+                                "sample": f"{CPU_SAMPLE['npart']} particles ({CPU_SAMPLE['name']}), full finder, "
+                                          f"{dt:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    neikdtree.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -39,7 +39,8 @@ class AhopOutputs(C.Structure):
 
 class AhopTimings(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("upload", "tree", "knn_density", "hop_groups", "saddles", "nodes",
-                                         "membership", "download", "total")]
+                                         "membership", "download", "total", "knn_kernel")] + [
+        (n, C.c_int32) for n in ("kernel_launches", "cub_calls", "tree_waves", "hop_passes")]
 
 
 class AhopError(RuntimeError):
@@ -98,4 +99,4 @@ def ptr(a: np.ndarray) -> int:
 def timings() -> dict:
     t = AhopTimings()
     check(lib().ahop_get_timings(C.byref(t)), "ahop_get_timings")
-    return {n: float(getattr(t, n)) for n, _ in AhopTimings._fields_}
+    return {n: (float(getattr(t, n)) if ty is C.c_float else int(getattr(t, n))) for n, ty in AhopTimings._fields_}

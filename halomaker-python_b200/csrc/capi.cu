@@ -71,6 +71,7 @@ static int validate(const Engine& E, int64_t n) {
 
 static int run_pipeline(Engine& E, const double* d_pos, const double* d_mass, int last_stage = 99) {
   int rc;
+  E.launches = E.cub_calls = E.waves = E.hop_passes = 0;
   cudaStream_t st = E.stream;
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[1], st));
   if ((rc = stage_sort_and_tree(E, d_pos, d_mass))) return rc;
@@ -89,6 +90,7 @@ static int run_pipeline(Engine& E, const double* d_pos, const double* d_mass, in
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[6], st));
   // density back to caller order
   AHOP_CUDA_TRY(E.d_dens_orig.ensure(E.n * 8));
+  E.launches++;
   dens_to_orig_kernel<<<(unsigned)((E.n + 255) / 256), 256, 0, st>>>(E.d_dens.as<double>(),
                                                                      E.d_orig.as<int32_t>(), E.n,
                                                                      E.d_dens_orig.as<double>());
@@ -113,6 +115,11 @@ static void fill_timings(Engine& E, bool host) {
   t.membership = el(6, 7);
   t.download = host ? el(7, 8) : 0.f;
   t.total = host ? el(0, 8) : el(1, 7);
+  t.knn_kernel = el(9, 10);
+  t.kernel_launches = E.launches;
+  t.cub_calls = E.cub_calls;
+  t.tree_waves = E.waves;
+  t.hop_passes = E.hop_passes;
 }
 
 }  // namespace ahop
@@ -322,6 +329,7 @@ int ahop_debug_neighbours(int32_t* out, int32_t k) {
   if (k < 1 || k > E.nstore) { set_error("k exceeds stored neighbours"); return AHOP_EINVAL; }
   DevBuf tmp;
   AHOP_CUDA_TRY(tmp.ensure((size_t)E.n * k * 4));
+  E.launches++;
   nei_to_orig_kernel<<<(unsigned)((E.n + 255) / 256), 256, 0, E.stream>>>(E.d_nei.as<int32_t>(), E.nstore, k,
                                                                           E.d_orig.as<int32_t>(), E.n,
                                                                           tmp.as<int32_t>());
@@ -336,6 +344,7 @@ int ahop_debug_density(double* out) {
   Engine& E = engine();
   if (E.n == 0 || !out) { set_error("no result"); return AHOP_ESTATE; }
   AHOP_CUDA_TRY(E.d_dens_orig.ensure(E.n * 8));
+  E.launches++;
   dens_to_orig_kernel<<<(unsigned)((E.n + 255) / 256), 256, 0, E.stream>>>(E.d_dens.as<double>(),
                                                                           E.d_orig.as<int32_t>(), E.n,
                                                                           E.d_dens_orig.as<double>());
@@ -364,6 +373,7 @@ int ahop_debug_groups(int32_t* hop_target, int32_t* group_id, int32_t* ngroups) 
   DevBuf tmp;
   AHOP_CUDA_TRY(tmp.ensure((size_t)E.n * 8));
   int32_t* h = tmp.as<int32_t>();
+  E.launches++;
   groups_to_orig_kernel<<<(unsigned)((E.n + 255) / 256), 256, 0, E.stream>>>(
       E.d_hop.as<int32_t>(), E.d_group.as<int32_t>(), E.d_orig.as<int32_t>(), E.n, h, h + E.n);
   AHOP_CUDA_TRY(cudaGetLastError());

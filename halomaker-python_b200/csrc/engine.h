@@ -59,7 +59,8 @@ struct Engine {
   Params prm;
   int device = -1;
   cudaStream_t stream = nullptr;  // stream of the current call
-  cudaEvent_t ev[10] = {};
+  cudaEvent_t ev[12] = {};
+  int32_t launches = 0, cub_calls = 0, waves = 0, hop_passes = 0;  // counters of the current compute
   bool events_ready = false;
   AhopTimings timings{};
 

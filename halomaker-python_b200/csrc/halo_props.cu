@@ -1,0 +1,491 @@
+// Batched per-halo properties; replaces the per-halo NumPy reductions of
+// src/compute_halo_props.py that _compute_halo_props (CHP:270-301) runs for
+// every halo in a multiprocessing pool:
+//   det_mass_17 (CHP:754-780)          m
+//   det_center_18 (CHP:901-966)        centre = densest member (cdm=False),
+//                                      bulk velocity, sigma
+//   compute_ang_mom_19 (CHP:783-824)   L about the centre, min-image
+//   r_halos_1a (CHP:828-851)           r = max |dr|
+//   det_inertial_tensor_1b20 (CHP:1932-1951) + det_main_axis_1b2 (1954-1967)
+//                                      I_ab, sha/shb/shc = sqrt(eig(I)/m)
+//   det_halo_energies_1b3 (CHP:1400-1444) E_kin with Hubble flow and the
+//                                      direct-sum E_pot for every halo size
+//   compute_spin_parameter_1c (CHP:1599-1602)
+//
+// Layout: members of halo h are rows [off[h], off[h+1]) of pos/vel (n,3),
+// mass (n) and density (n), FP64 in HBM.  One block per halo computes the
+// O(n) quantities (two passes over the members, fixed-order block
+// reductions, so results are deterministic).  The O(n^2) potential runs as
+// one persistent launch over a work list of (halo, i-tile) items sorted by
+// decreasing cost; each item sums m_j / r_ij for its 256 i-particles over all
+// j > i.  Two forms share the schedule:
+//   * FP64: relative positions and 1/sqrt in double;
+//   * FP32-compensated: positions relative to the halo centre split into
+//     hi = float(r) and lo = float(r - hi); a pair separation is
+//     (hi_j - hi_i) + (lo_j - lo_i) in FP32, 1/r from rsqrtf plus one Newton
+//     step, partial sums Kahan-compensated in FP32 and folded into FP64 per
+//     item.
+// Per-item partials are reduced per halo in item order (deterministic).
+#include <cuda_runtime.h>
+#include <cfloat>
+#include <climits>
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "ahop_halo.h"
+#include "engine.h"
+
+namespace ahop {
+
+constexpr int kPB = 256;  // threads per block (and i-tile size of the pair kernel)
+
+__device__ __forceinline__ double wrap_chp(double d, double L, double h, int periodic) {
+  // correct_for_periodicity_1d (CHP:854-863): strict comparisons
+  if (!periodic) return d;
+  if (d > h) d -= L;
+  if (d < -h) d += L;
+  return d;
+}
+
+template <class T>
+__device__ __forceinline__ T block_sum(T v, T* sh) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((tid & 31) == 0) sh[tid >> 5] = v;
+  __syncthreads();
+  T r = 0;
+  if (tid < 32) {
+    r = (tid < kPB / 32) ? sh[tid] : T(0);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+  }
+  __syncthreads();
+  if (tid == 0) sh[0] = r;
+  __syncthreads();
+  r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+// One block per halo: pass 1 (mass, momentum, densest member), pass 2
+// (L, r, inertia, E_kin, sigma) about the densest member and bulk velocity.
+__global__ void __launch_bounds__(kPB) halo_moments_kernel(HaloArgs A) {
+  __shared__ double sh[kPB / 32];
+  __shared__ double s_best_d[kPB / 32];
+  __shared__ long long s_best_i[kPB / 32];
+  __shared__ double s_c[7];
+  const int tid = threadIdx.x;
+  const int64_t h = blockIdx.x;
+  const int64_t b0 = A.off[h], b1 = A.off[h + 1];
+  // pass 1
+  double m = 0, mvx = 0, mvy = 0, mvz = 0, bd = -DBL_MAX;
+  long long bi = LLONG_MAX;
+  for (int64_t i = b0 + tid; i < b1; i += kPB) {
+    const double w = A.mass[i];
+    m += w;
+    mvx += w * A.vel[3 * i];
+    mvy += w * A.vel[3 * i + 1];
+    mvz += w * A.vel[3 * i + 2];
+    const double d = A.dens[i];
+    if (d > bd || (d == bd && i < bi)) { bd = d; bi = i; }  // np.argmax: first maximum
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    double od = __shfl_xor_sync(0xffffffffu, bd, o);
+    long long oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (od > bd || (od == bd && oi < bi)) { bd = od; bi = oi; }
+  }
+  if ((tid & 31) == 0) { s_best_d[tid >> 5] = bd; s_best_i[tid >> 5] = bi; }
+  m = block_sum(m, sh);
+  mvx = block_sum(mvx, sh);
+  mvy = block_sum(mvy, sh);
+  mvz = block_sum(mvz, sh);
+  if (tid == 0) {
+    double d = s_best_d[0];
+    long long ii = s_best_i[0];
+    for (int w = 1; w < kPB / 32; ++w)
+      if (s_best_d[w] > d || (s_best_d[w] == d && s_best_i[w] < ii)) { d = s_best_d[w]; ii = s_best_i[w]; }
+    s_c[0] = A.pos[3 * ii]; s_c[1] = A.pos[3 * ii + 1]; s_c[2] = A.pos[3 * ii + 2];
+    s_c[3] = mvx / m; s_c[4] = mvy / m; s_c[5] = mvz / m;
+    s_c[6] = (double)(ii - b0);
+  }
+  __syncthreads();
+  const double cx = s_c[0], cy = s_c[1], cz = s_c[2], vx = s_c[3], vy = s_c[4], vz = s_c[5];
+  // pass 2
+  double Lx = 0, Ly = 0, Lz = 0, r2max = 0, Ixx = 0, Ixy = 0, Ixz = 0, Iyy = 0, Iyz = 0, Izz = 0, ek = 0, sg = 0;
+  for (int64_t i = b0 + tid; i < b1; i += kPB) {
+    const double w = A.mass[i];
+    const double dx = wrap_chp(A.pos[3 * i] - cx, A.L, A.h, A.periodic);
+    const double dy = wrap_chp(A.pos[3 * i + 1] - cy, A.L, A.h, A.periodic);
+    const double dz = wrap_chp(A.pos[3 * i + 2] - cz, A.L, A.h, A.periodic);
+    const double ux = A.vel[3 * i] - vx, uy = A.vel[3 * i + 1] - vy, uz = A.vel[3 * i + 2] - vz;
+    const double px = w * ux, py = w * uy, pz = w * uz;
+    Lx += dy * pz - dz * py;
+    Ly += dz * px - dx * pz;
+    Lz += dx * py - dy * px;
+    r2max = fmax(r2max, dx * dx + dy * dy + dz * dz);
+    Ixx += w * dx * dx; Ixy += w * dx * dy; Ixz += w * dx * dz;
+    Iyy += w * dy * dy; Iyz += w * dy * dz; Izz += w * dz * dz;
+    const double tx = ux + dx * A.hub, ty = uy + dy * A.hub, tz = uz + dz * A.hub;
+    ek += w * (tx * tx + ty * ty + tz * tz);
+    sg += w * (ux * ux + uy * uy + uz * uz);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) r2max = fmax(r2max, __shfl_xor_sync(0xffffffffu, r2max, o));
+  if ((tid & 31) == 0) s_best_d[tid >> 5] = r2max;
+  Lx = block_sum(Lx, sh); Ly = block_sum(Ly, sh); Lz = block_sum(Lz, sh);
+  Ixx = block_sum(Ixx, sh); Ixy = block_sum(Ixy, sh); Ixz = block_sum(Ixz, sh);
+  Iyy = block_sum(Iyy, sh); Iyz = block_sum(Iyz, sh); Izz = block_sum(Izz, sh);
+  ek = block_sum(ek, sh);
+  sg = block_sum(sg, sh);
+  if (tid == 0) {
+    double rm = s_best_d[0];
+    for (int w = 1; w < kPB / 32; ++w) rm = fmax(rm, s_best_d[w]);
+    double* o = A.out + (size_t)kHaloFields * h;
+    o[HP_M] = m;
+    o[HP_PX] = cx; o[HP_PY] = cy; o[HP_PZ] = cz;
+    o[HP_VX] = vx; o[HP_VY] = vy; o[HP_VZ] = vz;
+    o[HP_LX] = Lx; o[HP_LY] = Ly; o[HP_LZ] = Lz;
+    o[HP_R] = sqrt(rm);
+    o[HP_IXX] = Ixx; o[HP_IXY] = Ixy; o[HP_IXZ] = Ixz; o[HP_IYY] = Iyy; o[HP_IYZ] = Iyz; o[HP_IZZ] = Izz;
+    o[HP_EK] = 0.5 * ek;
+    o[HP_SIGMA] = sqrt(sg / m);
+    o[HP_ICENTER] = s_c[6];
+  }
+}
+
+// Potential pair sums.  Work item w: halo item_h[w], i-tile start item_i[w].
+template <bool FP32C>
+__global__ void __launch_bounds__(kPB) epot_pairs_kernel(HaloArgs A, const int32_t* __restrict__ item_h,
+                                                         const int32_t* __restrict__ item_i, int32_t nitems,
+                                                         int32_t* __restrict__ counter, double* __restrict__ part) {
+  __shared__ float s_hx[kPB], s_hy[kPB], s_hz[kPB], s_lx[kPB], s_ly[kPB], s_lz[kPB], s_m[kPB];
+  __shared__ double s_dx[kPB], s_dy[kPB], s_dz[kPB], s_dm[kPB];
+  __shared__ double sh[kPB / 32];
+  __shared__ int32_t s_item;
+  const int tid = threadIdx.x;
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int32_t w = s_item;
+    __syncthreads();
+    if (w >= nitems) break;
+    const int32_t h = item_h[w];
+    const int64_t base = A.off[h];
+    const int32_t n = (int32_t)(A.off[h + 1] - base);
+    const int32_t i0 = item_i[w];
+    const double* c = A.out + (size_t)kHaloFields * h;
+    const double cx = c[HP_PX], cy = c[HP_PY], cz = c[HP_PZ];
+    const int32_t i = i0 + tid;
+    const bool vi = i < n;
+    double rxi = 0, ryi = 0, rzi = 0;
+    if (vi) {
+      rxi = wrap_chp(A.pos[3 * (base + i)] - cx, A.L, A.h, A.periodic);
+      ryi = wrap_chp(A.pos[3 * (base + i) + 1] - cy, A.L, A.h, A.periodic);
+      rzi = wrap_chp(A.pos[3 * (base + i) + 2] - cz, A.L, A.h, A.periodic);
+    }
+    const float hxi = (float)rxi, hyi = (float)ryi, hzi = (float)rzi;
+    const float lxi = (float)(rxi - (double)hxi), lyi = (float)(ryi - (double)hyi), lzi = (float)(rzi - (double)hzi);
+    float ks = 0.f, kc = 0.f;  // Kahan sum / compensation (FP32 form)
+    double ds = 0.0;           // FP64 form
+    for (int32_t j0 = i0; j0 < n; j0 += kPB) {
+      const int32_t j = j0 + tid;
+      if (j < n) {
+        const double rx = wrap_chp(A.pos[3 * (base + j)] - cx, A.L, A.h, A.periodic);
+        const double ry = wrap_chp(A.pos[3 * (base + j) + 1] - cy, A.L, A.h, A.periodic);
+        const double rz = wrap_chp(A.pos[3 * (base + j) + 2] - cz, A.L, A.h, A.periodic);
+        if (FP32C) {
+          const float hx = (float)rx, hy = (float)ry, hz = (float)rz;
+          s_hx[tid] = hx; s_hy[tid] = hy; s_hz[tid] = hz;
+          s_lx[tid] = (float)(rx - (double)hx); s_ly[tid] = (float)(ry - (double)hy);
+          s_lz[tid] = (float)(rz - (double)hz);
+          s_m[tid] = (float)A.mass[base + j];
+        } else {
+          s_dx[tid] = rx; s_dy[tid] = ry; s_dz[tid] = rz; s_dm[tid] = A.mass[base + j];
+        }
+      } else {
+        if (FP32C) { s_m[tid] = 0.f; s_hx[tid] = s_hy[tid] = s_hz[tid] = 3.0e30f; s_lx[tid] = s_ly[tid] = s_lz[tid] = 0.f; }
+        else { s_dm[tid] = 0.0; s_dx[tid] = s_dy[tid] = s_dz[tid] = 3.0e30; }
+      }
+      __syncthreads();
+      if (vi) {
+        const int jstart = (j0 == i0) ? tid + 1 : 0;  // j > i on the diagonal tile
+        const int jend = min(kPB, n - j0);
+        if (FP32C) {
+#pragma unroll 8
+          for (int jj = jstart; jj < jend; ++jj) {
+            const float dx = (s_hx[jj] - hxi) + (s_lx[jj] - lxi);
+            const float dy = (s_hy[jj] - hyi) + (s_ly[jj] - lyi);
+            const float dz = (s_hz[jj] - hzi) + (s_lz[jj] - lzi);
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            float inv = rsqrtf(r2);
+            inv = inv * (1.5f - 0.5f * r2 * inv * inv);  // one Newton step
+            const float t = (r2 > 0.f) ? s_m[jj] * inv : 0.f;
+            const float y = t - kc;
+            const float s2 = ks + y;
+            kc = (s2 - ks) - y;
+            ks = s2;
+          }
+        } else {
+#pragma unroll 4
+          for (int jj = jstart; jj < jend; ++jj) {
+            const double dx = s_dx[jj] - rxi, dy = s_dy[jj] - ryi, dz = s_dz[jj] - rzi;
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 > 0.0) ds += s_dm[jj] / sqrt(r2);
+          }
+        }
+      }
+      __syncthreads();
+    }
+    double mine = 0.0;
+    if (vi) {
+      const double mi = A.mass[base + i];
+      mine = FP32C ? mi * ((double)ks - (double)kc) : mi * ds;
+    }
+    const double tot = block_sum(mine, sh);
+    if (tid == 0) part[w] = tot;
+  }
+}
+
+// per-halo reduction of item partials (items of a halo are contiguous in the
+// halo-ordered list hitem_off), then E_pot, totals and spin
+__global__ void epot_finalize_kernel(HaloArgs A, const int64_t* __restrict__ hitem_off,
+                                     const int32_t* __restrict__ order, const double* __restrict__ part64,
+                                     const double* __restrict__ part32, int64_t nhalo) {
+  int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (h >= nhalo) return;
+  double s64 = 0, s32 = 0;
+  for (int64_t k = hitem_off[h]; k < hitem_off[h + 1]; ++k) {
+    const int32_t w = order[k];
+    if (part64) s64 += part64[w];
+    if (part32) s32 += part32[w];
+  }
+  double* o = A.out + (size_t)kHaloFields * h;
+  o[HP_EP64] = -A.G * s64;
+  o[HP_EP32C] = -A.G * s32;
+  const double m = o[HP_M];
+  const double hl = sqrt(o[HP_LX] * o[HP_LX] + o[HP_LY] * o[HP_LY] + o[HP_LZ] * o[HP_LZ]);
+  // compute_spin_parameter_1c: |L| sqrt(|E|) / m^2.5 / G with E = ek + ep
+  o[HP_SPIN64] = hl * sqrt(fabs(o[HP_EK] + o[HP_EP64])) / pow(m, 2.5) / A.G;
+  o[HP_SPIN32C] = hl * sqrt(fabs(o[HP_EK] + o[HP_EP32C])) / pow(m, 2.5) / A.G;
+  // principal axes: Jacobi eigenvalues of the symmetric inertia tensor
+  double a[3][3] = {{o[HP_IXX], o[HP_IXY], o[HP_IXZ]}, {o[HP_IXY], o[HP_IYY], o[HP_IYZ]},
+                    {o[HP_IXZ], o[HP_IYZ], o[HP_IZZ]}};
+  for (int sweep = 0; sweep < 50; ++sweep) {
+    const double off = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
+    const double dia = a[0][0] * a[0][0] + a[1][1] * a[1][1] + a[2][2] * a[2][2];
+    if (off <= 1e-34 * dia || off == 0.0) break;
+    for (int p = 0; p < 2; ++p)
+      for (int q = p + 1; q < 3; ++q) {
+        if (a[p][q] == 0.0) continue;
+        const double theta = (a[q][q] - a[p][p]) / (2.0 * a[p][q]);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        const double cs = 1.0 / sqrt(t * t + 1.0), sn = t * cs;
+        for (int k = 0; k < 3; ++k) {
+          const double akp = a[k][p], akq = a[k][q];
+          a[k][p] = cs * akp - sn * akq;
+          a[k][q] = sn * akp + cs * akq;
+        }
+        for (int k = 0; k < 3; ++k) {
+          const double apk = a[p][k], aqk = a[q][k];
+          a[p][k] = cs * apk - sn * aqk;
+          a[q][k] = sn * apk + cs * aqk;
+        }
+      }
+  }
+  double e0 = a[0][0], e1 = a[1][1], e2 = a[2][2], t;
+  if (e0 > e1) { t = e0; e0 = e1; e1 = t; }
+  if (e1 > e2) { t = e1; e1 = e2; e2 = t; }
+  if (e0 > e1) { t = e0; e0 = e1; e1 = t; }
+  o[HP_SHA] = sqrt(e0 / m);
+  o[HP_SHB] = sqrt(e1 / m);
+  o[HP_SHC] = sqrt(e2 / m);
+}
+
+}  // namespace ahop
+
+// ------------------------------------------------------------------ host side
+namespace ahop {
+
+struct HaloEngine {
+  DevBuf d_off, d_pos, d_vel, d_mass, d_dens, d_out;  // staging for host inputs
+  DevBuf d_item_h, d_item_i, d_part64, d_part32, d_counter, d_hoff, d_order;
+  cudaEvent_t ev[5] = {};
+  bool ready = false;
+  cudaStream_t own = nullptr;
+  AhopHaloTimings t{};
+  std::vector<int64_t> h_off;
+};
+
+static HaloEngine& halo_engine() {
+  static HaloEngine* e = new HaloEngine();
+  return *e;
+}
+
+static int halo_run(HaloEngine& H, const AhopHaloParams* p, const int64_t* d_off, const int64_t* h_off,
+                    int64_t nhalo, const double* d_pos, const double* d_vel, const double* d_mass,
+                    const double* d_dens, double* d_out, cudaStream_t st) {
+  if (!H.ready) {
+    for (auto& e : H.ev) AHOP_CUDA_TRY(cudaEventCreate(&e));
+    H.ready = true;
+  }
+  // work list: (halo, i-tile) items sorted by decreasing pair cost
+  std::vector<int64_t> cost;
+  std::vector<int32_t> ih, ii;
+  std::vector<int64_t> hoff(nhalo + 1, 0);
+  double pairs = 0;
+  for (int64_t h = 0; h < nhalo; ++h) {
+    const int64_t n = h_off[h + 1] - h_off[h];
+    if (n < 0 || n > INT32_MAX) { set_error("halo member count out of range"); return AHOP_EINVAL; }
+    pairs += 0.5 * (double)n * (double)(n - 1);
+    hoff[h] = (int64_t)ih.size();
+    for (int64_t i0 = 0; i0 < n; i0 += kPB) {
+      ih.push_back((int32_t)h);
+      ii.push_back((int32_t)i0);
+      cost.push_back((n - i0) * (int64_t)kPB);
+    }
+  }
+  hoff[nhalo] = (int64_t)ih.size();
+  const int32_t nitems = (int32_t)ih.size();
+  std::vector<int32_t> sorted(nitems);
+  for (int32_t k = 0; k < nitems; ++k) sorted[k] = k;
+  std::stable_sort(sorted.begin(), sorted.end(), [&](int32_t a, int32_t b) { return cost[a] > cost[b]; });
+  std::vector<int32_t> sh(nitems), si(nitems), order(nitems);
+  for (int32_t k = 0; k < nitems; ++k) {
+    sh[k] = ih[sorted[k]];
+    si[k] = ii[sorted[k]];
+    order[sorted[k]] = k;  // halo-ordered item k runs as scheduled item order[k]
+  }
+  const size_t ni = (size_t)(nitems > 0 ? nitems : 1);
+  AHOP_CUDA_TRY(H.d_item_h.ensure(ni * 4));
+  AHOP_CUDA_TRY(H.d_item_i.ensure(ni * 4));
+  AHOP_CUDA_TRY(H.d_order.ensure(ni * 4));
+  AHOP_CUDA_TRY(H.d_part64.ensure(ni * 8));
+  AHOP_CUDA_TRY(H.d_part32.ensure(ni * 8));
+  AHOP_CUDA_TRY(H.d_counter.ensure(16));
+  AHOP_CUDA_TRY(H.d_hoff.ensure((size_t)(nhalo + 1) * 8));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_item_h.p, sh.data(), nitems * 4, cudaMemcpyHostToDevice, st));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_item_i.p, si.data(), nitems * 4, cudaMemcpyHostToDevice, st));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_order.p, order.data(), nitems * 4, cudaMemcpyHostToDevice, st));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_hoff.p, hoff.data(), (nhalo + 1) * 8, cudaMemcpyHostToDevice, st));
+  HaloArgs A;
+  A.off = d_off; A.pos = d_pos; A.vel = d_vel; A.mass = d_mass; A.dens = d_dens; A.out = d_out;
+  A.L = p->Lbox; A.h = 0.5 * p->Lbox; A.hub = p->Hub_pt; A.G = p->gravconst; A.periodic = p->periodic != 0;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  int launches = 0;
+  AHOP_CUDA_TRY(cudaEventRecord(H.ev[0], st));
+  if (nhalo > 0) {
+    halo_moments_kernel<<<(unsigned)nhalo, kPB, 0, st>>>(A);
+    ++launches;
+    AHOP_CUDA_TRY(cudaGetLastError());
+  }
+  AHOP_CUDA_TRY(cudaEventRecord(H.ev[1], st));
+  if ((p->epot & 1) && nitems > 0) {
+    int per = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, epot_pairs_kernel<false>, kPB, 0);
+    AHOP_CUDA_TRY(cudaMemsetAsync(H.d_counter.p, 0, 4, st));
+    epot_pairs_kernel<false><<<nsm * (per > 0 ? per : 1), kPB, 0, st>>>(
+        A, H.d_item_h.as<int32_t>(), H.d_item_i.as<int32_t>(), nitems, H.d_counter.as<int32_t>(),
+        H.d_part64.as<double>());
+    ++launches;
+    AHOP_CUDA_TRY(cudaGetLastError());
+  }
+  AHOP_CUDA_TRY(cudaEventRecord(H.ev[2], st));
+  if ((p->epot & 2) && nitems > 0) {
+    int per = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, epot_pairs_kernel<true>, kPB, 0);
+    AHOP_CUDA_TRY(cudaMemsetAsync(H.d_counter.as<int32_t>() + 1, 0, 4, st));
+    epot_pairs_kernel<true><<<nsm * (per > 0 ? per : 1), kPB, 0, st>>>(
+        A, H.d_item_h.as<int32_t>(), H.d_item_i.as<int32_t>(), nitems, H.d_counter.as<int32_t>() + 1,
+        H.d_part32.as<double>());
+    ++launches;
+    AHOP_CUDA_TRY(cudaGetLastError());
+  }
+  AHOP_CUDA_TRY(cudaEventRecord(H.ev[3], st));
+  if (nhalo > 0) {
+    epot_finalize_kernel<<<(unsigned)((nhalo + 127) / 128), 128, 0, st>>>(
+        A, H.d_hoff.as<int64_t>(), H.d_order.as<int32_t>(), (p->epot & 1) ? H.d_part64.as<double>() : nullptr,
+        (p->epot & 2) ? H.d_part32.as<double>() : nullptr, nhalo);
+    ++launches;
+    AHOP_CUDA_TRY(cudaGetLastError());
+  }
+  AHOP_CUDA_TRY(cudaEventRecord(H.ev[4], st));
+  AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+  auto el = [&](int a, int b) { float ms = 0; cudaEventElapsedTime(&ms, H.ev[a], H.ev[b]); return ms; };
+  H.t.moments = el(0, 1);
+  H.t.epot64 = el(1, 2);
+  H.t.epot32c = el(2, 3);
+  H.t.finalize = el(3, 4);
+  H.t.total = el(0, 4);
+  H.t.pairs = pairs;
+  H.t.items = nitems;
+  H.t.kernel_launches = launches;
+  return AHOP_OK;
+}
+
+static int halo_validate(const AhopHaloParams* p, int64_t nhalo) {
+  if (!p) { set_error("null params"); return AHOP_EINVAL; }
+  if (nhalo < 0) { set_error("nhalo must be >= 0"); return AHOP_EINVAL; }
+  if (p->periodic && !(p->Lbox > 0)) { set_error("Lbox must be positive for periodic boxes"); return AHOP_EINVAL; }
+  return AHOP_OK;
+}
+
+}  // namespace ahop
+
+using namespace ahop;
+
+extern "C" {
+
+int ahop_halo_props_device(const AhopHaloParams* p, const int64_t* d_off, int64_t nhalo, const double* d_pos,
+                           const double* d_vel, const double* d_mass, const double* d_density, double* d_out,
+                           void* stream) {
+  int rc;
+  if ((rc = halo_validate(p, nhalo))) return rc;
+  HaloEngine& H = halo_engine();
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  H.h_off.resize(nhalo + 1);
+  AHOP_CUDA_TRY(cudaMemcpyAsync(H.h_off.data(), d_off, (nhalo + 1) * 8, cudaMemcpyDeviceToHost, st));
+  AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+  return halo_run(H, p, d_off, H.h_off.data(), nhalo, d_pos, d_vel, d_mass, d_density, d_out, st);
+}
+
+int ahop_halo_props(const AhopHaloParams* p, const int64_t* off, int64_t nhalo, const double* pos,
+                    const double* vel, const double* mass, const double* density, double* out) {
+  int rc;
+  if ((rc = halo_validate(p, nhalo))) return rc;
+  if (!off || (nhalo > 0 && (!pos || !vel || !mass || !density || !out))) { set_error("null input"); return AHOP_EINVAL; }
+  HaloEngine& H = halo_engine();
+  if (!H.own) AHOP_CUDA_TRY(cudaStreamCreateWithFlags(&H.own, cudaStreamNonBlocking));
+  cudaStream_t st = H.own;
+  const int64_t n = off[nhalo];
+  AHOP_CUDA_TRY(H.d_off.ensure((nhalo + 1) * 8));
+  AHOP_CUDA_TRY(H.d_pos.ensure(n * 24 + 8));
+  AHOP_CUDA_TRY(H.d_vel.ensure(n * 24 + 8));
+  AHOP_CUDA_TRY(H.d_mass.ensure(n * 8 + 8));
+  AHOP_CUDA_TRY(H.d_dens.ensure(n * 8 + 8));
+  AHOP_CUDA_TRY(H.d_out.ensure((size_t)nhalo * kHaloFields * 8 + 8));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_off.p, off, (nhalo + 1) * 8, cudaMemcpyHostToDevice, st));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_pos.p, pos, n * 24, cudaMemcpyHostToDevice, st));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_vel.p, vel, n * 24, cudaMemcpyHostToDevice, st));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_mass.p, mass, n * 8, cudaMemcpyHostToDevice, st));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_dens.p, density, n * 8, cudaMemcpyHostToDevice, st));
+  if ((rc = halo_run(H, p, H.d_off.as<int64_t>(), off, nhalo, H.d_pos.as<double>(), H.d_vel.as<double>(),
+                     H.d_mass.as<double>(), H.d_dens.as<double>(), H.d_out.as<double>(), st)))
+    return rc;
+  AHOP_CUDA_TRY(cudaMemcpyAsync(out, H.d_out.p, (size_t)nhalo * kHaloFields * 8, cudaMemcpyDeviceToHost, st));
+  AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+  return AHOP_OK;
+}
+
+int ahop_halo_get_timings(AhopHaloTimings* t) {
+  if (!t) return AHOP_EINVAL;
+  *t = halo_engine().t;
+  return AHOP_OK;
+}
+
+}  // extern "C"

@@ -110,6 +110,7 @@ int stage_hop_groups(Engine& E) {
   AHOP_CUDA_TRY(E.d_peakflag.ensure((n + 1) * 4));
   int32_t* hop = E.d_hop.as<int32_t>();
   int32_t* root = E.d_root.as<int32_t>();
+  E.launches++;
   hop_kernel<<<grid, T, 0, st>>>(E.d_dens.as<double>(), E.d_nei.as<int32_t>(), E.nstore, P.nhop,
                                  E.d_orig.as<int32_t>(), n, P.rho_threshold, hop);
   AHOP_CUDA_TRY(cudaGetLastError());
@@ -121,15 +122,18 @@ int stage_hop_groups(Engine& E) {
   bool converged = false;
   for (int it = 0; it < 64; ++it) {
     AHOP_CUDA_TRY(cudaMemsetAsync(d_changed, 0, 4, st));
+    E.launches++;
     jump_kernel<<<grid, T, 0, st>>>(root, n, d_changed);
     AHOP_CUDA_TRY(cudaGetLastError());
     AHOP_CUDA_TRY(cudaMemcpyAsync(h_changed, d_changed, 4, cudaMemcpyDeviceToHost, st));
     AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+    E.hop_passes = it + 1;
     if (*h_changed == 0) { converged = true; break; }
   }
   if (!converged) { set_error("hop pointer jumping did not converge in 64 passes"); return AHOP_ELIMIT; }
   // peaks numbered in increasing particle index
   int32_t* flag = E.d_peakflag.as<int32_t>();
+  E.launches++;
   peak_flag_kernel<<<grid, T, 0, st>>>(hop, E.d_orig.as<int32_t>(), n, flag);
   AHOP_CUDA_TRY(cudaGetLastError());
   AHOP_CUDA_TRY(cudaMemsetAsync(flag + n, 0, 4, st));
@@ -138,6 +142,7 @@ int stage_hop_groups(Engine& E) {
   size_t tmp = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp, flag, scan, (int)(n + 1), st);
   AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
+  E.cub_calls++;
   AHOP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(E.d_cub.p, tmp, flag, scan, (int)(n + 1), st));
   int32_t ng = 0;
   AHOP_CUDA_TRY(cudaMemcpyAsync(&ng, scan + n, 4, cudaMemcpyDeviceToHost, st));
@@ -149,6 +154,7 @@ int stage_hop_groups(Engine& E) {
   AHOP_CUDA_TRY(E.d_sad_cnt.ensure((size_t)(ng + 2) * 4));
   int32_t* gcount = E.d_sad_cnt.as<int32_t>();  // gcount[g], g = 1..ng; gcount[0] = gcount[ng+1] = 0
   AHOP_CUDA_TRY(cudaMemsetAsync(gcount, 0, (size_t)(ng + 2) * 4, st));
+  E.launches++;
   group_kernel<<<grid, T, 0, st>>>(root, E.d_orig.as<int32_t>(), scan, E.d_dens.as<double>(), n,
                                    E.d_group.as<int32_t>(), E.d_densg.as<double>(), E.d_gpeak.as<int32_t>(),
                                    gcount);
@@ -158,6 +164,7 @@ int stage_hop_groups(Engine& E) {
     size_t t2 = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, t2, gcount, E.d_goff.as<int32_t>(), ng + 2, st);
     AHOP_CUDA_TRY(E.d_cub.ensure(t2));
+    E.cub_calls++;
     AHOP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(E.d_cub.p, t2, gcount, E.d_goff.as<int32_t>(), ng + 2, st));
   }
   // member CSR in (group asc, particle index desc)
@@ -165,6 +172,7 @@ int stage_hop_groups(Engine& E) {
   AHOP_CUDA_TRY(E.d_key2.ensure(n * 8));
   AHOP_CUDA_TRY(E.d_idx2.ensure(n * 4));
   AHOP_CUDA_TRY(E.d_gmem.ensure(n * 4));
+  E.launches++;
   member_keys_kernel<<<grid, T, 0, st>>>(E.d_group.as<int32_t>(), E.d_orig.as<int32_t>(), n, ng,
                                          E.d_key.as<unsigned long long>(), E.d_idx2.as<int32_t>());
   AHOP_CUDA_TRY(cudaGetLastError());
@@ -175,6 +183,7 @@ int stage_hop_groups(Engine& E) {
                                   E.d_key2.as<unsigned long long>(), E.d_idx2.as<int32_t>(),
                                   E.d_gmem.as<int32_t>(), (int)n, 0, end_bit, st);
   AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
+  E.cub_calls++;
   AHOP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(E.d_cub.p, tmp, E.d_key.as<unsigned long long>(),
                                                 E.d_key2.as<unsigned long long>(), E.d_idx2.as<int32_t>(),
                                                 E.d_gmem.as<int32_t>(), (int)n, 0, end_bit, st));

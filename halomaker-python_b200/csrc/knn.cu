@@ -138,6 +138,7 @@ int stage_sort_and_tree(Engine& E, const double* d_pos, const double* d_mass) {
   AHOP_CUDA_TRY(E.d_rank.ensure(n * 4));
   const int T = 256;
   unsigned grid = (unsigned)((n + T - 1) / T);
+  E.launches++;
   morton_kernel<<<grid, T, 0, st>>>(d_pos, n, P.xlong, P.ylong, P.zlong, E.d_key.as<unsigned long long>(),
                                     E.d_idx.as<int32_t>());
   AHOP_CUDA_TRY(cudaGetLastError());
@@ -146,9 +147,11 @@ int stage_sort_and_tree(Engine& E, const double* d_pos, const double* d_mass) {
                                   E.d_key2.as<unsigned long long>(), E.d_idx.as<int32_t>(),
                                   E.d_idx2.as<int32_t>(), (int)n, 0, 63, st);
   AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
+  E.cub_calls++;
   AHOP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(E.d_cub.p, tmp, E.d_key.as<unsigned long long>(),
                                                 E.d_key2.as<unsigned long long>(), E.d_idx.as<int32_t>(),
                                                 E.d_idx2.as<int32_t>(), (int)n, 0, 63, st));
+  E.launches++;
   gather_sorted_kernel<<<grid, T, 0, st>>>(d_pos, d_mass, E.d_idx2.as<int32_t>(), n, E.d_x.as<double>(),
                                            E.d_y.as<double>(), E.d_z.as<double>(), E.d_m.as<double>(),
                                            E.d_orig.as<int32_t>(), E.d_rank.as<int32_t>());
@@ -173,6 +176,7 @@ int stage_sort_and_tree(Engine& E, const double* d_pos, const double* d_mass) {
   double pad = 1e-12 * fmax(P.xlong, fmax(P.ylong, P.zlong));
   {
     int64_t threads = E.lev_cnt[0] * 32;
+    E.launches++;
     leaf_box_kernel<<<(unsigned)((threads + T - 1) / T), T, 0, st>>>(E.d_x.as<double>(), E.d_y.as<double>(),
                                                                      E.d_z.as<double>(), n, E.lev_cnt[0], pad,
                                                                      box);
@@ -180,6 +184,7 @@ int stage_sort_and_tree(Engine& E, const double* d_pos, const double* d_mass) {
   }
   for (int l = 1; l < nlev; ++l) {
     int64_t threads = E.lev_cnt[l] * 32;
+    E.launches++;
     node_box_kernel<<<(unsigned)((threads + T - 1) / T), T, 0, st>>>(
         box + 6 * E.lev_off[l - 1], E.lev_cnt[l - 1], E.lev_cnt[l], box + 6 * E.lev_off[l]);
     AHOP_CUDA_TRY(cudaGetLastError());
@@ -371,7 +376,10 @@ int stage_knn_density(Engine& E) {
   int64_t want = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
   int64_t grid = (int64_t)nsm * per_sm * 4;
   if (grid > want) grid = want;
+  E.launches++;
+  AHOP_CUDA_TRY(cudaEventRecord(E.ev[9], E.stream));
   knn_density_kernel<<<(unsigned)grid, kWarpsPerBlock * 32, 0, E.stream>>>(A);
+  AHOP_CUDA_TRY(cudaEventRecord(E.ev[10], E.stream));
   AHOP_CUDA_TRY(cudaGetLastError());
   int herr = 0;
   AHOP_CUDA_TRY(cudaMemcpyAsync(&herr, E.d_flags.p, 4, cudaMemcpyDeviceToHost, E.stream));

@@ -508,7 +508,11 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
   }
   __syncthreads();
   while (true) {
-    if (T.rhot >= T.next_event) structural_pass<SortT, ScanT, MaxScanT>(A, T, sort_tmp, scan_tmp, maxscan_tmp, s_keys);
+    // every thread must take the same branch: snapshot the test before thread 0
+    // rewrites next_event inside the pass
+    const bool restructure = T.rhot >= T.next_event;
+    __syncthreads();
+    if (restructure) structural_pass<SortT, ScanT, MaxScanT>(A, T, sort_tmp, scan_tmp, maxscan_tmp, s_keys);
     if (T.nsurv == 0) {  // all groups below the threshold (f90:1348-1351 prints, then ends with no colour)
       if (tid == 0) A.node[T.inode].firstchild = 0;
       break;
@@ -523,7 +527,9 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
       if (C[9] == 2.0) { C[10] = 1.0; atomicAdd(&T.nexact, 1); }
     }
     __syncthreads();
-    if (T.nexact > 0) exact_stats(A, T);
+    const int32_t nexact = T.nexact;  // block-uniform after the barrier
+    __syncthreads();
+    if (nexact > 0) exact_stats(A, T);
     // count significant components
     if (tid == 0) {
       int32_t ns = 0;
@@ -775,6 +781,7 @@ int stage_nodes(Engine& E) {
   double* rho_idx = E.d_gmem_rho.as<double>();        // densities in particle-index order
   double* rdesc = E.d_gmem_rho.as<double>() + nact;   // sorted decreasing
   int32_t* mem_rho = reinterpret_cast<int32_t*>(E.d_sad_val2.p);
+  E.launches++;
   gather_member_rho<<<(unsigned)((nact + T - 1) / T), T, 0, st>>>(E.d_gmem.as<int32_t>(), E.d_dens.as<double>(),
                                                                   nact, rho_idx);
   AHOP_CUDA_TRY(cudaGetLastError());
@@ -783,12 +790,14 @@ int stage_nodes(Engine& E) {
                                                 (int)nact, ng, E.d_goff.as<int32_t>() + 1,
                                                 E.d_goff.as<int32_t>() + 2, st);
   AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
+  E.cub_calls++;
   AHOP_CUDA_TRY(cub::DeviceSegmentedSort::SortPairsDescending(E.d_cub.p, tmp, rho_idx, rdesc,
                                                               E.d_gmem.as<int32_t>(), mem_rho, (int)nact, ng,
                                                               E.d_goff.as<int32_t>() + 1,
                                                               E.d_goff.as<int32_t>() + 2, st));
   {
     int64_t threads = (int64_t)ng * 32;
+    E.launches++;
     prefix_moments_kernel<<<(unsigned)((threads + T - 1) / T), T, 0, st>>>(
         E.d_goff.as<int32_t>(), ng, mem_rho, rdesc, E.d_gpeak.as<int32_t>(), E.d_x.as<double>(),
         E.d_y.as<double>(), E.d_z.as<double>(), E.d_m.as<double>(), P.xlong, P.ylong, P.zlong, P.xlongs2,
@@ -798,7 +807,10 @@ int stage_nodes(Engine& E) {
   // ---- tree scratch
   const size_t G = (size_t)ng + 1;
   const size_t bytes_i = G * 4;
-  const size_t need = bytes_i * 10 + G * 8 * 8 + G * 12 * 8 + (size_t)(nnodesmax + 1) * sizeof(Task) * 2 + 256;
+  // every sub-array starts on a 256-byte boundary: size the buffer with the rounding
+  auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
+  const size_t need = r256(bytes_i) * 10 + r256(G * 8 * 8) + r256(G * 12 * 8) +
+                      r256((size_t)(nnodesmax + 1) * sizeof(Task)) * 2;
   AHOP_CUDA_TRY(E.d_tree_scratch.ensure(need));
   char* p = static_cast<char*>(E.d_tree_scratch.p);
   auto take = [&](size_t b) { char* q = p; p += (b + 255) & ~size_t(255); return q; };
@@ -843,6 +855,7 @@ int stage_nodes(Engine& E) {
   A.fudge = P.fudge; A.alphap = P.alphap; A.epsilon = P.epsilon; A.nmembthresh = P.nmembthresh;
   A.node = E.d_nodes.as<NodeRec>();
   A.nnodesmax = nnodesmax;
+  E.launches++;
   init_groups_kernel<<<(unsigned)((ng + 1 + T - 1) / T), T, 0, st>>>(ng, A.GL, A.pos_of, A.deepnode);
   AHOP_CUDA_TRY(cudaGetLastError());
   // root node 0 (f90:934-943): mass and truemass stay 0, densmax = max peak density
@@ -860,6 +873,7 @@ int stage_nodes(Engine& E) {
     if (wave > 100000) { set_error("structure tree: too many waves"); return AHOP_ELIMIT; }
     A.next = tasks[cur ^ 1];
     AHOP_CUDA_TRY(cudaMemsetAsync(A.nnext, 0, 4, st));
+    E.launches++;
     tree_wave_kernel<SortT, ScanT, MaxScanT><<<ntasks, kNT, 0, st>>>(A, tasks[cur]);
     AHOP_CUDA_TRY(cudaGetLastError());
     AHOP_CUDA_TRY(cudaMemcpyAsync(h, flags, 16, cudaMemcpyDeviceToHost, st));
@@ -871,10 +885,12 @@ int stage_nodes(Engine& E) {
     }
     ntasks = h[3];
     cur ^= 1;
+    E.waves = wave + 1;
   }
   const int32_t nn = h[2];
   E.nnodes = nn;
   // ---- membership (f90:1297-1306 paint order => deepest node above rho_saddle)
+  E.launches++;
   membership_kernel<<<(unsigned)((n + T - 1) / T), T, 0, st>>>(E.d_group.as<int32_t>(), E.d_dens.as<double>(),
                                                               E.d_orig.as<int32_t>(), A.deepnode, A.node, n,
                                                               E.d_liste.as<int32_t>(), flags);
@@ -886,18 +902,23 @@ int stage_nodes(Engine& E) {
     AHOP_CUDA_TRY(E.d_idx2.ensure((size_t)(nn + 1) * 4 * 2));
     int32_t* new_to_old = E.d_idx2.as<int32_t>();
     int32_t* o2n = new_to_old + nn + 1;
+    E.launches++;
     iota_kernel<<<(unsigned)((nn + T - 1) / T), T, 0, st>>>(new_to_old, nn, 1);
     AHOP_CUDA_TRY(cudaGetLastError());
     tmp = 0;
     NodeLess less{A.node};
     cub::DeviceMergeSort::SortKeys(nullptr, tmp, new_to_old, nn, less, st);
     AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
+    E.cub_calls++;
     AHOP_CUDA_TRY(cub::DeviceMergeSort::SortKeys(E.d_cub.p, tmp, new_to_old, nn, less, st));
+    E.launches++;
     old_to_new_kernel<<<(unsigned)((nn + T - 1) / T), T, 0, st>>>(new_to_old, nn, o2n);
     AHOP_CUDA_TRY(cudaGetLastError());
+    E.launches++;
     tables_kernel<<<(unsigned)((nn + T - 1) / T), T, 0, st>>>(A.node, new_to_old, o2n, nn, E.d_rtab.as<double>(),
                                                               E.d_itab.as<int32_t>());
     AHOP_CUDA_TRY(cudaGetLastError());
+    E.launches++;
     remap_liste_kernel<<<(unsigned)((n + T - 1) / T), T, 0, st>>>(E.d_liste.as<int32_t>(), n, o2n);
     AHOP_CUDA_TRY(cudaGetLastError());
   }

@@ -107,12 +107,14 @@ int stage_saddles(Engine& E) {
   AHOP_CUDA_TRY(E.d_idx.ensure((n + 1) * 4));
   int32_t* cnt = E.d_idx2.as<int32_t>();
   int32_t* off = E.d_idx.as<int32_t>();
+  E.launches++;
   link_count_kernel<<<grid, T, 0, st>>>(E.d_group.as<int32_t>(), E.d_nei.as<int32_t>(), E.nstore, P.nhop, n, cnt);
   AHOP_CUDA_TRY(cudaGetLastError());
   AHOP_CUDA_TRY(cudaMemsetAsync(cnt + n, 0, 4, st));
   size_t tmp = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp, cnt, off, (int)(n + 1), st);
   AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
+  E.cub_calls++;
   AHOP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(E.d_cub.p, tmp, cnt, off, (int)(n + 1), st));
   int32_t nlink = 0;
   AHOP_CUDA_TRY(cudaMemcpyAsync(&nlink, off + n, 4, cudaMemcpyDeviceToHost, st));
@@ -130,6 +132,7 @@ int stage_saddles(Engine& E) {
     AHOP_CUDA_TRY(E.d_srho.ensure(8));
     return AHOP_OK;
   }
+  E.launches++;
   link_emit_kernel<<<grid, T, 0, st>>>(E.d_group.as<int32_t>(), E.d_nei.as<int32_t>(), E.nstore, P.nhop,
                                        E.d_dens.as<double>(), n, off, E.d_sad_key.as<unsigned long long>(),
                                        E.d_sad_val.as<double>());
@@ -142,6 +145,7 @@ int stage_saddles(Engine& E) {
                                   E.d_sad_key2.as<unsigned long long>(), E.d_sad_val.as<double>(),
                                   E.d_sad_val2.as<double>(), nlink, 0, 32 + gb, st);
   AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
+  E.cub_calls++;
   AHOP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(E.d_cub.p, tmp, E.d_sad_key.as<unsigned long long>(),
                                                 E.d_sad_key2.as<unsigned long long>(), E.d_sad_val.as<double>(),
                                                 E.d_sad_val2.as<double>(), nlink, 0, 32 + gb, st));
@@ -154,6 +158,7 @@ int stage_saddles(Engine& E) {
                                  E.d_sad_key.as<unsigned long long>(), E.d_sad_val2.as<double>(),
                                  E.d_sad_val.as<double>(), d_nu, MaxOp(), nlink, st);
   AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
+  E.cub_calls++;
   AHOP_CUDA_TRY(cub::DeviceReduce::ReduceByKey(E.d_cub.p, tmp, E.d_sad_key2.as<unsigned long long>(),
                                                E.d_sad_key.as<unsigned long long>(), E.d_sad_val2.as<double>(),
                                                E.d_sad_val.as<double>(), d_nu, MaxOp(), nlink, st));
@@ -168,6 +173,7 @@ int stage_saddles(Engine& E) {
   int32_t* rowcnt = E.d_sad_cnt.as<int32_t>();
   AHOP_CUDA_TRY(cudaMemsetAsync(rowcnt, 0, (size_t)(ng + 2) * 4, st));
   const unsigned gu = (unsigned)((nu + T - 1) / T);
+  E.launches++;
   symmetrize_kernel<<<gu, T, 0, st>>>(E.d_sad_key.as<unsigned long long>(), E.d_sad_val.as<double>(), nu, keep,
                                       sval, rowcnt);
   AHOP_CUDA_TRY(cudaGetLastError());
@@ -175,6 +181,7 @@ int stage_saddles(Engine& E) {
   tmp = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp, keep, kpos, nu + 1, st);
   AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
+  E.cub_calls++;
   AHOP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(E.d_cub.p, tmp, keep, kpos, nu + 1, st));
   int32_t nc = 0;
   AHOP_CUDA_TRY(cudaMemcpyAsync(&nc, kpos + nu, 4, cudaMemcpyDeviceToHost, st));
@@ -187,9 +194,11 @@ int stage_saddles(Engine& E) {
   tmp = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp, rowcnt + 1, E.d_soff.as<int32_t>(), ng + 1, st);
   AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
+  E.cub_calls++;
   AHOP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(E.d_cub.p, tmp, rowcnt + 1, E.d_soff.as<int32_t>(), ng + 1, st));
   if (nc == 0) return AHOP_OK;
   // compacted (g1, g2) order == row order by g1; scatter then sort each row by decreasing saddle
+  E.launches++;
   compact_kernel<<<gu, T, 0, st>>>(E.d_sad_key.as<unsigned long long>(), sval, keep, kpos, nu,
                                    E.d_sisad.as<int32_t>(), E.d_sad_val.as<double>());
   AHOP_CUDA_TRY(cudaGetLastError());
@@ -201,6 +210,7 @@ int stage_saddles(Engine& E) {
                                                       E.d_sisad.as<int32_t>(), isad_sorted, nc, ng,
                                                       E.d_soff.as<int32_t>(), E.d_soff.as<int32_t>() + 1, st);
   AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
+  E.cub_calls++;
   AHOP_CUDA_TRY(cub::DeviceSegmentedSort::StableSortPairsDescending(
       E.d_cub.p, tmp, E.d_sad_val.as<double>(), E.d_srho.as<double>(), E.d_sisad.as<int32_t>(), isad_sorted, nc,
       ng, E.d_soff.as<int32_t>(), E.d_soff.as<int32_t>() + 1, st));

@@ -67,9 +67,13 @@ typedef struct {
   const int32_t* integer_table; /* [nnodes][6] */
 } AhopOutputs;
 
-/* Per-stage device timings of the last compute, milliseconds (CUDA events). */
+/* Per-stage device timings of the last compute, milliseconds (CUDA events on
+ * the compute stream), plus launch counts of the last compute: kernels of this
+ * library, and CUB device-wide primitives it invoked. */
 typedef struct {
   float upload, tree, knn_density, hop_groups, saddles, nodes, membership, download, total;
+  float knn_kernel; /* the fused kNN + density kernel alone */
+  int32_t kernel_launches, cub_calls, tree_waves, hop_passes;
 } AhopTimings;
 
 const char* ahop_last_error(void);
@@ -119,6 +123,44 @@ int ahop_debug_saddles(int32_t* nconn, int32_t* offsets, int32_t* isad, double* 
 int ahop_debug_compute_stages(const double* pos_in, const double* mass_in, int64_t npart, int32_t last_stage);
 /* Ask compute to keep the first k neighbours per particle (default nhop). */
 int ahop_debug_set_store_neighbours(int32_t k);
+
+/* ---- batched halo properties ------------------------------------------------
+ * Replaces the per-halo reductions of src/compute_halo_props.py run by
+ * _compute_halo_props (CHP:270-301): det_mass_17, det_center_18 (densest
+ * member as centre, cdm=False), compute_ang_mom_19, r_halos_1a,
+ * det_inertial_tensor_1b20 + det_main_axis_1b2, det_halo_energies_1b3 (E_kin
+ * with Hubble flow; E_pot as the direct pair sum for every halo size) and
+ * compute_spin_parameter_1c.  Members of halo h are rows [off[h], off[h+1]).
+ * Each halo gets AHOP_HALO_NFIELDS doubles, indexed by the HP_* constants. */
+enum {
+  HP_M = 0, HP_PX, HP_PY, HP_PZ, HP_VX, HP_VY, HP_VZ, HP_LX, HP_LY, HP_LZ, HP_R,
+  HP_IXX, HP_IXY, HP_IXZ, HP_IYY, HP_IYZ, HP_IZZ, HP_EK, HP_EP64, HP_EP32C, HP_SIGMA,
+  HP_SHA, HP_SHB, HP_SHC, HP_SPIN64, HP_SPIN32C, HP_ICENTER, AHOP_HALO_NFIELDS
+};
+
+typedef struct {
+  double Lbox;      /* period (H.Lbox_pt), same unit as positions */
+  double Hub_pt;    /* Hubble constant used for the Hubble flow in E_kin */
+  double gravconst; /* G (H.gravconst = 430.1) */
+  int32_t periodic; /* H.FlagPeriod != 0 */
+  int32_t epot;     /* bit 0: FP64 direct sum, bit 1: FP32-compensated direct sum */
+} AhopHaloParams;
+
+typedef struct {
+  float moments, epot64, epot32c, finalize, total; /* ms, CUDA events */
+  double pairs;                                    /* sum over halos of n(n-1)/2 */
+  int32_t items, kernel_launches;
+} AhopHaloTimings;
+
+/* Host buffers: off[nhalo+1], pos[n][3], vel[n][3], mass[n], density[n];
+ * out[nhalo][AHOP_HALO_NFIELDS] (host). */
+int ahop_halo_props(const AhopHaloParams* p, const int64_t* off, int64_t nhalo, const double* pos,
+                    const double* vel, const double* mass, const double* density, double* out);
+/* Same on device buffers (all pointers device memory), on `stream`. */
+int ahop_halo_props_device(const AhopHaloParams* p, const int64_t* d_off, int64_t nhalo, const double* d_pos,
+                           const double* d_vel, const double* d_mass, const double* d_density, double* d_out,
+                           void* stream);
+int ahop_halo_get_timings(AhopHaloTimings* t);
 
 #ifdef __cplusplus
 }

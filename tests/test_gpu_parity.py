@@ -52,7 +52,8 @@ def compare_neighbour_sets(pos, mine, ref):
     return len(bad)
 
 
-def run_both(pos, mass, k=32, **kw):
+def run_both(pos, mass, **kw):
+    k = kw.get("nvoisins", 32)
     f = _finder()
     n = mass.shape[0]
     f.configure(n, **kw)
