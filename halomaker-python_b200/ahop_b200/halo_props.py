@@ -1,0 +1,81 @@
+"""Batched per-halo properties through the C ABI (ahop_halo_props*).
+
+Replaces the per-halo property chain of the reference
+(_compute_halo_props, src/compute_halo_props.py:270-301) for the fields it
+lists: mass, centre (densest member), bulk velocity, sigma, angular momentum,
+r, inertia tensor and principal axes, E_kin (with Hubble flow), the direct-sum
+E_pot in FP64 and FP32-compensated forms, and spin.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+
+FIELDS = ["m", "px", "py", "pz", "vx", "vy", "vz", "Lx", "Ly", "Lz", "r", "Ixx", "Ixy", "Ixz", "Iyy", "Iyz",
+          "Izz", "ek", "ep64", "ep32c", "sigma", "sha", "shb", "shc", "spin64", "spin32c", "icenter"]
+NF = len(FIELDS)
+
+
+class AhopHaloParams(C.Structure):
+    _fields_ = [("Lbox", C.c_double), ("Hub_pt", C.c_double), ("gravconst", C.c_double),
+                ("periodic", C.c_int32), ("epot", C.c_int32)]
+
+
+class AhopHaloTimings(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("moments", "epot64", "epot32c", "finalize", "total")] + [
+        ("pairs", C.c_double), ("items", C.c_int32), ("kernel_launches", C.c_int32)]
+
+
+_bound = False
+
+
+def _lib():
+    global _bound
+    lib = L.lib()
+    if not _bound:
+        lib.ahop_halo_props.argtypes = [C.POINTER(AhopHaloParams), C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.ahop_halo_props_device.argtypes = [C.POINTER(AhopHaloParams), C.c_void_p, C.c_int64, C.c_void_p,
+                                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.ahop_halo_get_timings.argtypes = [C.POINTER(AhopHaloTimings)]
+        _bound = True
+    return lib
+
+
+def params(Lbox, Hub_pt, gravconst=430.1, periodic=True, epot=3):
+    return AhopHaloParams(float(Lbox), float(Hub_pt), float(gravconst), int(bool(periodic)), int(epot))
+
+
+def compute(off, pos, vel, mass, dens, Lbox, Hub_pt, gravconst=430.1, periodic=True, epot=3) -> dict:
+    """Host arrays in, dict of per-halo arrays out (FIELDS)."""
+    off = np.ascontiguousarray(off, np.int64)
+    nh = len(off) - 1
+    pos = np.ascontiguousarray(pos, np.float64)
+    vel = np.ascontiguousarray(vel, np.float64)
+    mass = np.ascontiguousarray(mass, np.float64)
+    dens = np.ascontiguousarray(dens, np.float64)
+    out = np.zeros((max(nh, 1), NF))
+    p = params(Lbox, Hub_pt, gravconst, periodic, epot)
+    L.check(_lib().ahop_halo_props(C.byref(p), off.ctypes.data, nh, pos.ctypes.data, vel.ctypes.data,
+                                   mass.ctypes.data, dens.ctypes.data, out.ctypes.data), "halo_props")
+    return {f: out[:nh, k].copy() for k, f in enumerate(FIELDS)}
+
+
+def compute_device(d_off, d_pos, d_vel, d_mass, d_dens, d_out, Lbox, Hub_pt, gravconst=430.1, periodic=True,
+                   epot=3, stream=None):
+    """torch CUDA tensors in; fills d_out (nhalo, NF) in place."""
+    p = params(Lbox, Hub_pt, gravconst, periodic, epot)
+    nh = d_off.numel() - 1
+    st = C.c_void_p(stream.cuda_stream if stream is not None else 0)
+    L.check(_lib().ahop_halo_props_device(C.byref(p), d_off.data_ptr(), nh, d_pos.data_ptr(), d_vel.data_ptr(),
+                                          d_mass.data_ptr(), d_dens.data_ptr(), d_out.data_ptr(), st),
+            "halo_props_device")
+
+
+def timings() -> dict:
+    t = AhopHaloTimings()
+    L.check(_lib().ahop_halo_get_timings(C.byref(t)), "halo_get_timings")
+    return {n: getattr(t, n) for n, _ in AhopHaloTimings._fields_}

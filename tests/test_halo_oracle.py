@@ -1,0 +1,33 @@
+"""Pin the halo-property oracle against fixtures from the reference's functions.
+
+tests/golden/halo_case.npz comes from src/compute_halo_props.py run on seeded
+halos (tests/golden/make_halo_golden.py).  The oracle restates the same NumPy
+formulas, so O(n) fields agree to rounding; the potential is compared where
+the reference itself sums pairs (fewer than 1000 members).
+"""
+import os
+
+import numpy as np
+
+import halo_oracle
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "halo_case.npz")
+
+
+def test_oracle_matches_reference_halo_functions():
+    g = np.load(GOLD)
+    f = list(g["fields"])
+    ref = g["out"]
+    r = halo_oracle.props(g["off"], g["pos"], g["vel"], g["mass"], g["dens"], float(g["Lbox"]), float(g["Hub_pt"]),
+                          float(g["gravconst"]), nthreads=2)
+    col = lambda n: ref[:, f.index(n)]
+    for name in ["m", "px", "py", "pz", "vx", "vy", "vz", "r", "ek", "sigma"]:
+        np.testing.assert_allclose(r[name], col(name), rtol=1e-12, atol=0, err_msg=name)
+    for name in ["Lx", "Ly", "Lz"]:
+        np.testing.assert_allclose(r[name], col(name), rtol=1e-10, atol=1e-12 * np.abs(col(name)).max(), err_msg=name)
+    for name in ["sha", "shb", "shc"]:
+        np.testing.assert_allclose(r[name], col(name), rtol=1e-10, err_msg=name)
+    n = np.diff(g["off"])
+    small = n < 1000
+    np.testing.assert_allclose(r["ep64"][small], col("ep")[small], rtol=1e-12)
+    np.testing.assert_allclose(r["spin64"][small], col("spin")[small], rtol=1e-10)
