@@ -249,6 +249,11 @@ def main():
     roof = {"kernel": "knn_density_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "alg_bytes_per_launch": alg,
             "launch_ms": knn_avg, "peak_source": "measured" if peaks else "fallback"}
+    ts = (C.c_int64 * 8)()
+    lib.ahop_debug_tree_stats(ts, 8)
+    tree_stats = {"structural_Mcycles": ts[0] / 1e6, "level_stats_Mcycles": ts[1] / 1e6,
+                  "exact_Mcycles": ts[2] / 1e6, "levels": ts[3], "undecided_exact_passes": ts[4],
+                  "max_levels_one_task": ts[5], "max_Mcycles_one_task": ts[6] / 1e6}
     mean_stage = {k: statistics.mean(s[k] for s in stage) for k in
                   ("tree", "knn_density", "hop_groups", "saddles", "nodes", "membership", "total")}
     line = {"metric": METRIC, "value": value, "unit": "Mpart/s", "n_gpus": world, "steps": args.steps,
@@ -261,7 +266,7 @@ def main():
             "roofline": roof, "stages_ms": mean_stage,
             "gpu_launches": int(stage[-1]["kernel_launches"]) * args.steps,
             "cub_calls_per_step": int(stage[-1]["cub_calls"]), "tree_waves": int(stage[-1]["tree_waves"]),
-            "nnodes": nnodes, "clocks": clk.summary()}
+            "nnodes": nnodes, "tree_stats": tree_stats, "clocks": clk.summary()}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, dt, nth, _ = cpu_sample_rate()
         line["cpu_baseline"] = {"value": rate, "unit": "Mpart/s", "cores": nth, "kind": "port",

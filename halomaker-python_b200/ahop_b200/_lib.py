@@ -60,12 +60,14 @@ _SIGS = {
     "ahop_get_device_outputs": [C.POINTER(AhopOutputs)],
     "ahop_get_timings": [C.POINTER(AhopTimings)],
     "ahop_close": [],
+    "ahop_release_device_memory": [],
     "ahop_debug_neighbours": [C.c_void_p, C.c_int32],
     "ahop_debug_density": [C.c_void_p],
     "ahop_debug_groups": [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)],
     "ahop_debug_saddles": [C.POINTER(C.c_int32), C.c_void_p, C.c_void_p, C.c_void_p],
     "ahop_debug_compute_stages": [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32],
     "ahop_debug_set_store_neighbours": [C.c_int32],
+    "ahop_debug_tree_stats": [C.c_void_p, C.c_int32],
 }
 
 

@@ -76,18 +76,21 @@ class _NeiKDtree:
         n = pos.shape[1]
         if mass.shape[0] != n:
             raise ValueError("mass_in must have npart entries")
-        self.close()
+        self.close()  # f90:501
         L.check(L.lib().ahop_compute_adaptahop(pos.ctypes.data, mass.ctypes.data, n), "compute_adaptahop")
         out = L.AhopOutputs()
         L.check(L.lib().ahop_get_outputs(C.byref(out)), "get_outputs")
         nn = int(out.nnodes)
         self.nnodes = np.int32(nn)
-        self.density = np.ctypeslib.as_array(C.cast(out.density, C.POINTER(C.c_double)), (n,)).copy()
+        # Like f2py's module arrays these are views of library-owned (pinned)
+        # memory, valid until the next compute_adaptahop; the reference copies
+        # them out before calling close() (NEI:53-64).
+        self.density = np.ctypeslib.as_array(C.cast(out.density, C.POINTER(C.c_double)), (n,))
         nused = int(out.nusedpart)
-        self.liste_parts = np.ctypeslib.as_array(C.cast(out.liste_parts, C.POINTER(C.c_int32)), (nused,)).copy()
+        self.liste_parts = np.ctypeslib.as_array(C.cast(out.liste_parts, C.POINTER(C.c_int32)), (nused,))
         if nn > 0:
-            rt = np.ctypeslib.as_array(C.cast(out.real_table, C.POINTER(C.c_double)), (nn * 8,)).copy()
-            it = np.ctypeslib.as_array(C.cast(out.integer_table, C.POINTER(C.c_int32)), (nn * 6,)).copy()
+            rt = np.ctypeslib.as_array(C.cast(out.real_table, C.POINTER(C.c_double)), (nn * 8,))
+            it = np.ctypeslib.as_array(C.cast(out.integer_table, C.POINTER(C.c_int32)), (nn * 6,))
         else:
             rt = np.empty(0, np.float64)
             it = np.empty(0, np.int32)

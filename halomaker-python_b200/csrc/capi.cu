@@ -212,18 +212,20 @@ int ahop_compute_adaptahop(const double* pos_in, const double* mass_in, int64_t 
   AHOP_CUDA_TRY(cudaMemcpyAsync(E.d_pos_in.p, pos_in, npart * 24, cudaMemcpyHostToDevice, st));
   AHOP_CUDA_TRY(cudaMemcpyAsync(E.d_mass_in.p, mass_in, npart * 8, cudaMemcpyHostToDevice, st));
   if ((rc = run_pipeline(E, E.d_pos_in.as<double>(), E.d_mass_in.as<double>()))) return rc;
-  // module outputs to host
+  // module outputs to host (pinned, reused across calls)
   const int64_t nused = E.prm.nusedpart > 0 ? std::min<int64_t>(E.prm.nusedpart, npart) : npart;
-  E.h_dens.resize(npart);
-  E.h_liste.resize(nused);
-  E.h_rtab.resize((size_t)E.nnodes * 8);
-  E.h_itab.resize((size_t)E.nnodes * 6);
-  AHOP_CUDA_TRY(cudaMemcpyAsync(E.h_dens.data(), E.d_dens_orig.p, npart * 8, cudaMemcpyDeviceToHost, st));
-  AHOP_CUDA_TRY(cudaMemcpyAsync(E.h_liste.data(), E.d_liste.p, nused * 4, cudaMemcpyDeviceToHost, st));
+  AHOP_CUDA_TRY(E.h_dens.ensure(npart * 8));
+  AHOP_CUDA_TRY(E.h_liste.ensure(nused * 4));
+  AHOP_CUDA_TRY(E.h_rtab.ensure((size_t)(E.nnodes > 0 ? E.nnodes : 1) * 64));
+  AHOP_CUDA_TRY(E.h_itab.ensure((size_t)(E.nnodes > 0 ? E.nnodes : 1) * 24));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(E.h_dens.p, E.d_dens_orig.p, npart * 8, cudaMemcpyDeviceToHost, st));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(E.h_liste.p, E.d_liste.p, nused * 4, cudaMemcpyDeviceToHost, st));
   if (E.nnodes > 0) {
-    AHOP_CUDA_TRY(cudaMemcpyAsync(E.h_rtab.data(), E.d_rtab.p, (size_t)E.nnodes * 64, cudaMemcpyDeviceToHost, st));
-    AHOP_CUDA_TRY(cudaMemcpyAsync(E.h_itab.data(), E.d_itab.p, (size_t)E.nnodes * 24, cudaMemcpyDeviceToHost, st));
+    AHOP_CUDA_TRY(cudaMemcpyAsync(E.h_rtab.p, E.d_rtab.p, (size_t)E.nnodes * 64, cudaMemcpyDeviceToHost, st));
+    AHOP_CUDA_TRY(cudaMemcpyAsync(E.h_itab.p, E.d_itab.p, (size_t)E.nnodes * 24, cudaMemcpyDeviceToHost, st));
   }
+  E.h_n = npart;
+  E.h_nused = nused;
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[8], st));
   AHOP_CUDA_TRY(cudaStreamSynchronize(st));
   fill_timings(E, true);
@@ -234,15 +236,15 @@ int ahop_compute_adaptahop(const double* pos_in, const double* mass_in, int64_t 
 int ahop_get_outputs(AhopOutputs* out) {
   Engine& E = engine();
   if (!out) { set_error("null out"); return AHOP_EINVAL; }
-  if (!E.have_result || E.h_dens.size() != (size_t)E.n) { set_error("no host outputs (call ahop_compute_adaptahop)"); return AHOP_ESTATE; }
+  if (!E.have_result || E.h_n != E.n) { set_error("no host outputs (call ahop_compute_adaptahop)"); return AHOP_ESTATE; }
   out->npart = E.n;
-  out->nusedpart = (int64_t)E.h_liste.size();
+  out->nusedpart = E.h_nused;
   out->nnodes = E.nnodes;
   out->ngroups = E.ngroups;
-  out->liste_parts = E.h_liste.data();
-  out->density = E.h_dens.data();
-  out->real_table = E.h_rtab.data();
-  out->integer_table = E.h_itab.data();
+  out->liste_parts = E.h_liste.as<int32_t>();
+  out->density = E.h_dens.as<double>();
+  out->real_table = E.h_rtab.as<double>();
+  out->integer_table = E.h_itab.as<int32_t>();
   return AHOP_OK;
 }
 
@@ -268,9 +270,7 @@ int ahop_get_timings(AhopTimings* t) {
   return AHOP_OK;
 }
 
-int ahop_close(void) {
-  if (!g_engine) return AHOP_OK;
-  Engine& E = *g_engine;
+static void release_device(Engine& E) {
   DevBuf* bufs[] = {&E.d_pos_in, &E.d_mass_in, &E.d_key, &E.d_key2, &E.d_idx, &E.d_idx2, &E.d_x, &E.d_y,
                     &E.d_z, &E.d_m, &E.d_orig, &E.d_rank, &E.d_box, &E.d_cub, &E.d_nei, &E.d_dens,
                     &E.d_hop, &E.d_root, &E.d_group, &E.d_peakflag, &E.d_densg, &E.d_gpeak, &E.d_goff,
@@ -280,13 +280,30 @@ int ahop_close(void) {
                     &E.d_rtab, &E.d_itab};
   if (E.device >= 0) cudaSetDevice(E.device);
   for (DevBuf* b : bufs) b->release();
-  E.h_liste.clear(); E.h_liste.shrink_to_fit();
-  E.h_dens.clear(); E.h_dens.shrink_to_fit();
-  E.h_rtab.clear(); E.h_itab.clear();
+  E.h_liste.release(); E.h_dens.release(); E.h_rtab.release(); E.h_itab.release();
+}
+
+// close (f90:3227-3264) deallocates the module's arrays.  Here the module
+// outputs are dropped; device buffers stay cached for the next compute (a
+// pool, like torch's caching allocator) -- the reference calls close() after
+// every snapshot (NEI:64), and re-allocating gigabytes per snapshot would
+// dominate the run.  ahop_release_device_memory() returns them.
+int ahop_close(void) {
+  if (!g_engine) return AHOP_OK;
+  Engine& E = *g_engine;
+  E.h_n = 0;
+  E.h_nused = 0;
   E.have_result = false;
   E.nnodes = 0;
   E.ngroups = 0;
   E.n = 0;
+  return AHOP_OK;
+}
+
+int ahop_release_device_memory(void) {
+  if (!g_engine) return AHOP_OK;
+  ahop_close();
+  release_device(*g_engine);
   return AHOP_OK;
 }
 
@@ -307,6 +324,12 @@ int ahop_debug_compute_stages(const double* pos_in, const double* mass_in, int64
   rc = run_pipeline(E, E.d_pos_in.as<double>(), E.d_mass_in.as<double>(), last_stage);
   if (rc) return rc;
   AHOP_CUDA_TRY(cudaStreamSynchronize(E.stream));
+  return AHOP_OK;
+}
+
+int ahop_debug_tree_stats(int64_t* out, int32_t n) {
+  Engine& E = engine();
+  for (int i = 0; i < n && i < 8; ++i) out[i] = (int64_t)E.tree_stats[i];
   return AHOP_OK;
 }
 

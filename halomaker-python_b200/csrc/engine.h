@@ -32,6 +32,27 @@ struct DevBuf {
   template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
+// Growable pinned host buffer (module outputs live here; fast D2H).
+struct HostBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t need) {
+    if (need <= bytes) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMallocHost(&p, need ? need : 16);
+    if (e == cudaSuccess) bytes = need ? need : 16;
+    return e;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
 struct Params {
   int64_t npart = 0;
   int32_t nusedpart = 0;
@@ -61,6 +82,7 @@ struct Engine {
   cudaStream_t stream = nullptr;  // stream of the current call
   cudaEvent_t ev[12] = {};
   int32_t launches = 0, cub_calls = 0, waves = 0, hop_passes = 0;  // counters of the current compute
+  unsigned long long tree_stats[8] = {};                             // structure-tree kernel counters
   bool events_ready = false;
   AhopTimings timings{};
 
@@ -108,9 +130,9 @@ struct Engine {
   DevBuf d_dens_orig;                    // [n] density in ORIG order
   DevBuf d_rtab, d_itab;                 // exported tables
 
-  // host copies (module outputs)
-  std::vector<int32_t> h_liste, h_itab;
-  std::vector<double> h_dens, h_rtab;
+  // host copies (module outputs), pinned
+  HostBuf h_liste, h_itab, h_dens, h_rtab;
+  int64_t h_n = 0, h_nused = 0;
 
   // small pinned host scalars
   int64_t* h_scalars = nullptr;

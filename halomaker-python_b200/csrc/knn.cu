@@ -238,7 +238,10 @@ __device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int64
     d = pdist2(qx, qy, qz, A.x[p], A.y[p], A.z[p], A.Lx, A.Ly, A.Lz);
     o = A.orig[p];
   }
-  unsigned mask = __ballot_sync(0xffffffffu, v && d < L.r2);
+  // accept d below the current nv-th distance, or equal to it with a smaller
+  // particle index: the list is the nv smallest (distance, index) pairs
+  int32_t lastk = __shfl_sync(0xffffffffu, L.lo, A.nv - 1);
+  unsigned mask = __ballot_sync(0xffffffffu, v && (d < L.r2 || (d == L.r2 && o < lastk)));
   while (mask) {
     int src = __ffs(mask) - 1;
     double cd = __shfl_sync(0xffffffffu, d, src);
@@ -253,95 +256,242 @@ __device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int64
     if (lane == pos) { L.ld = cd; L.ls = cs; L.lo = co; }
     if (lane >= A.nv) { L.ld = CUDART_INF; L.ls = -1; L.lo = INT_MAX; }
     L.r2 = __shfl_sync(0xffffffffu, L.ld, A.nv - 1);
+    lastk = __shfl_sync(0xffffffffu, L.lo, A.nv - 1);
     mask &= ~(1u << src);
-    mask &= __ballot_sync(0xffffffffu, d < L.r2);
+    mask &= __ballot_sync(0xffffffffu, d < L.r2 || (d == L.r2 && o < lastk));
   }
 }
 
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) knn_density_kernel(KnnArgs A) {
+// Per-query depth-first traversal from the root, nearest child first (used
+// when a query leaf's candidate list overflows).  Leaves skip0/skip1 were
+// already scanned.
+__device__ void query_dfs(const KnnArgs& A, WarpList& L, int64_t s, double qx, double qy, double qz, int lane,
+                          int32_t* s_node, double* s_bd, int64_t skip0, int64_t skip1) {
+  const int top = A.nlev - 1;
+  int sp = 0;
+  if (lane == 0) { s_node[0] = (top << 27) | 0; s_bd[0] = 0.0; }
+  sp = 1;
+  __syncwarp();
+  while (sp > 0) {
+    --sp;
+    const int32_t ent = s_node[sp];
+    const double bd = s_bd[sp];
+    __syncwarp();
+    if (!(bd < L.r2)) continue;
+    const int lvl = ent >> 27;
+    const int64_t j = ent & ((1 << 27) - 1);
+    if (lvl == 0) {
+      if (j == skip0 || j == skip1) continue;
+      leaf_insert(A, L, j, s, qx, qy, qz, lane);
+      continue;
+    }
+    const int64_t c = j * kFan + lane;
+    const bool valid = c < A.lev_cnt[lvl - 1];
+    double bdc = CUDART_INF;
+    if (valid) bdc = box_dist2(A.box + 6 * (A.lev_off[lvl - 1] + c), qx, qy, qz, A.Lx, A.Ly, A.Lz);
+    const bool cand = valid && bdc < L.r2;
+    const unsigned mask = __ballot_sync(0xffffffffu, cand);
+    if (!mask) continue;
+    const int cnt = __popc(mask);
+    if (sp + cnt > kStack) {  // cannot happen for <= 7 levels; guard anyway
+      if (lane == 0) atomicExch(A.err, 1);
+      break;
+    }
+    double best = cand ? bdc : CUDART_INF;
+    int bl = lane;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      int ol = __shfl_xor_sync(0xffffffffu, bl, o);
+      if (ob < best || (ob == best && ol < bl)) { best = ob; bl = ol; }
+    }
+    if (cand) {
+      int r = __popc(mask & ((1u << lane) - 1));
+      int slot;
+      if (lane == bl) slot = sp + cnt - 1;
+      else {
+        int rb = __popc(mask & ((1u << bl) - 1));
+        slot = sp + (r < rb ? r : r - 1);
+      }
+      s_node[slot] = ((lvl - 1) << 27) | (int32_t)c;
+      s_bd[slot] = bdc;
+    }
+    sp += cnt;
+    __syncwarp();
+  }
+}
+
+// SPH density (f90:2816-2838) in the exact evaluation order, and the stored
+// neighbour slots.
+__device__ __forceinline__ void finish_query(const KnnArgs& A, const WarpList& L, int64_t s, int lane) {
+  const int nv = A.nv;
+  const double dlast = __shfl_sync(0xffffffffu, L.ld, nv - 1);
+  const double r = xmul(xsqrt(dlast), 0.5);
+  const double r3 = xmul(xmul(r, r), r);
+  const double unsr = xdiv(1.0, r);
+  double term = 0.0;
+  if (lane < nv - 1) term = xmul(A.m[L.ls], spline(xmul(xsqrt(L.ld), unsr)));
+  double contrib = 0.0;
+  for (int i = 0; i < nv - 1; ++i) contrib = xadd(contrib, __shfl_sync(0xffffffffu, term, i));
+  if (lane == 0) {
+    const double pi_f = (double)3.141592654f;  // f90:58 single-precision literal
+    A.dens[s] = xdiv(xmul(A.xyzlong, xadd(contrib, A.m[s])), xmul(pi_f, r3));
+  }
+  if (lane < A.nstore) A.nei[s * A.nstore + lane] = L.ls;
+}
+
+// Periodic squared distance between two padded boxes (centre, half width).
+__device__ __forceinline__ double boxbox_dist2(const double* __restrict__ a, const double* __restrict__ b,
+                                               double Lx, double Ly, double Lz) {
+  double dx = fabs(a[0] - b[0]); dx = fmin(dx, Lx - dx); dx = fmax(0.0, dx - a[3] - b[3]);
+  double dy = fabs(a[1] - b[1]); dy = fmin(dy, Ly - dy); dy = fmax(0.0, dy - a[4] - b[4]);
+  double dz = fabs(a[2] - b[2]); dz = fmin(dz, Lz - dz); dz = fmax(0.0, dz - a[5] - b[5]);
+  return dx * dx + dy * dy + dz * dz;
+}
+
+// k-th smallest (k = 1..64) of the 64 values held two per lane: warp bitonic
+// sort of (v0, v1) with element index 2*lane + slot; returns the value at
+// sorted position k-1 to every lane.
+__device__ __forceinline__ double warp_kth_of_64(double v0, double v1, int k, int lane) {
+#pragma unroll
+  for (int size = 2; size <= 64; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride >= 1; stride >>= 1) {
+      if (stride == 1) {
+        const int i0 = 2 * lane;  // pair (i0, i0+1) inside the lane
+        const bool asc = ((i0 & size) == 0);
+        const double lo = fmin(v0, v1), hi = fmax(v0, v1);
+        v0 = asc ? lo : hi;
+        v1 = asc ? hi : lo;
+      } else {
+        const int lstride = stride >> 1;
+        const double p0 = __shfl_xor_sync(0xffffffffu, v0, lstride);
+        const double p1 = __shfl_xor_sync(0xffffffffu, v1, lstride);
+        const int i0 = 2 * lane, i1 = 2 * lane + 1;
+        const bool lower = (lane & lstride) == 0;
+        const bool asc0 = ((i0 & size) == 0), asc1 = ((i1 & size) == 0);
+        v0 = (lower == asc0) ? fmin(v0, p0) : fmax(v0, p0);
+        v1 = (lower == asc1) ? fmin(v1, p1) : fmax(v1, p1);
+      }
+    }
+  }
+  const int e = k - 1;
+  const double a = __shfl_sync(0xffffffffu, v0, e >> 1);
+  const double b = __shfl_sync(0xffffffffu, v1, e >> 1);
+  return (e & 1) ? b : a;
+}
+
+constexpr int kMaxCand = 512;  // candidate leaves per query leaf (else per-query DFS)
+
+// One warp per query leaf (its 32 Morton-consecutive particles).
+//  A. every query's nv-th nearest distance among its own leaf and the
+//     adjacent leaf bounds its final kNN radius r_q; R = max_q r_q;
+//  B. one traversal collects every leaf whose box lies within R of this
+//     leaf's box (candidates, nearest-first);
+//  C. each query builds its sorted list from the candidates (own leaves
+//     first), skipping leaves farther than its current nv-th distance.
+// The candidate leaves are shared by the 32 queries, so the traversal is
+// paid once per leaf and the leaf data mostly comes from L1.
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) knn_leaf_kernel(KnnArgs A) {
   __shared__ int32_t s_node[kWarpsPerBlock][kStack];
   __shared__ double s_bd[kWarpsPerBlock][kStack];
+  __shared__ int32_t s_cand[kWarpsPerBlock][kMaxCand];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
+  const int64_t nleaf = A.lev_cnt[0];
   const int top = A.nlev - 1;
-  for (int64_t s = (int64_t)blockIdx.x * kWarpsPerBlock + wib; s < A.n; s += nwarps) {
-    const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
-    WarpList L;
-    L.ld = CUDART_INF; L.ls = -1; L.lo = INT_MAX; L.r2 = CUDART_INF;
-    const int64_t j0 = s / kLeaf;
-    const int64_t j1 = j0 ^ 1;
-    leaf_insert(A, L, j0, s, qx, qy, qz, lane);
-    if (j1 < A.lev_cnt[0]) leaf_insert(A, L, j1, s, qx, qy, qz, lane);
-    // depth-first traversal, nearest child popped first
-    int sp = 0;
-    if (lane == 0) { s_node[wib][0] = (top << 27) | 0; s_bd[wib][0] = 0.0; }
-    sp = 1;
-    __syncwarp();
-    while (sp > 0) {
-      --sp;
-      const int32_t ent = s_node[wib][sp];
-      const double bd = s_bd[wib][sp];
-      __syncwarp();
-      if (!(bd < L.r2)) continue;
-      const int lvl = ent >> 27;
-      const int64_t j = ent & ((1 << 27) - 1);
-      if (lvl == 0) {
-        if (j == j0 || j == j1) continue;
-        leaf_insert(A, L, j, s, qx, qy, qz, lane);
-        continue;
-      }
-      const int64_t c = j * kFan + lane;
-      const bool valid = c < A.lev_cnt[lvl - 1];
-      double bdc = CUDART_INF;
-      if (valid) bdc = box_dist2(A.box + 6 * (A.lev_off[lvl - 1] + c), qx, qy, qz, A.Lx, A.Ly, A.Lz);
-      const bool cand = valid && bdc < L.r2;
-      const unsigned mask = __ballot_sync(0xffffffffu, cand);
-      if (!mask) continue;
-      const int cnt = __popc(mask);
-      if (sp + cnt > kStack) {  // cannot happen for <= 7 levels; guard anyway
-        if (lane == 0) atomicExch(A.err, 1);
-        break;
-      }
-      // nearest candidate goes on top of the stack
-      double best = cand ? bdc : CUDART_INF;
-      int bl = lane;
+  for (int64_t jl = (int64_t)blockIdx.x * kWarpsPerBlock + wib; jl < nleaf; jl += nwarps) {
+    const int64_t jn = (jl + 1 < nleaf) ? jl + 1 : jl - 1;  // adjacent leaf (jn >= 0 when nleaf >= 2)
+    const int64_t s0 = jl * kLeaf;
+    const int nq = (int)((A.n - s0) < kLeaf ? (A.n - s0) : (int64_t)kLeaf);
+    // ---- A: per-query bound from the two leaves
+    double Rq = 0.0;
+    bool ok = true;
+    for (int q = 0; q < nq; ++q) {
+      const int64_t s = s0 + q;
+      const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
+      const int64_t p0 = s0 + lane, p1 = jn * kLeaf + lane;
+      double v0 = CUDART_INF, v1 = CUDART_INF;
+      if (p0 < A.n && p0 != s) v0 = pdist2(qx, qy, qz, A.x[p0], A.y[p0], A.z[p0], A.Lx, A.Ly, A.Lz);
+      if (jn >= 0 && jn != jl && p1 < A.n && p1 != s) v1 = pdist2(qx, qy, qz, A.x[p1], A.y[p1], A.z[p1], A.Lx, A.Ly, A.Lz);
+      const double kth = warp_kth_of_64(v0, v1, A.nv, lane);
+      if (!(kth < CUDART_INF)) ok = false;  // fewer than nv others in the two leaves
+      if (lane == q) Rq = kth;
+    }
+    double R2 = ok ? Rq : CUDART_INF;
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        int ol = __shfl_xor_sync(0xffffffffu, bl, o);
-        if (ob < best || (ob == best && ol < bl)) { best = ob; bl = ol; }
-      }
-      if (cand) {
-        int r = __popc(mask & ((1u << lane) - 1));
-        int slot;
-        if (lane == bl) slot = sp + cnt - 1;
-        else {
-          int rb = __popc(mask & ((1u << bl) - 1));
-          slot = sp + (r < rb ? r : r - 1);
+    for (int o = 16; o > 0; o >>= 1) R2 = fmax(R2, __shfl_xor_sync(0xffffffffu, R2, o));
+    if (!ok) R2 = CUDART_INF;
+    // ---- B: candidate leaves within R of this leaf's box
+    const double* myb = A.box + 6 * jl;
+    int ncand = 0;
+    bool overflow = !(R2 < CUDART_INF);
+    if (!overflow) {
+      const double lim = R2 * (1.0 + 1e-12);
+      int sp = 0;
+      if (lane == 0) { s_node[wib][0] = (top << 27) | 0; }
+      sp = 1;
+      __syncwarp();
+      while (sp > 0 && !overflow) {
+        --sp;
+        const int32_t ent = s_node[wib][sp];
+        __syncwarp();
+        const int lvl = ent >> 27;
+        const int64_t j = ent & ((1 << 27) - 1);
+        const int64_t c = j * kFan + lane;
+        const bool valid = c < A.lev_cnt[lvl - 1];
+        bool cand = false;
+        if (valid) cand = boxbox_dist2(myb, A.box + 6 * (A.lev_off[lvl - 1] + c), A.Lx, A.Ly, A.Lz) <= lim;
+        const unsigned mask = __ballot_sync(0xffffffffu, cand);
+        const int cnt = __popc(mask);
+        if (!cnt) continue;
+        const int r = __popc(mask & ((1u << lane) - 1));
+        if (lvl - 1 == 0) {
+          if (ncand + cnt > kMaxCand) { overflow = true; break; }
+          if (cand) s_cand[wib][ncand + r] = (int32_t)c;
+          ncand += cnt;
+        } else {
+          if (sp + cnt > kStack) { overflow = true; break; }
+          if (cand) s_node[wib][sp + r] = ((lvl - 1) << 27) | (int32_t)c;
+          sp += cnt;
         }
-        s_node[wib][slot] = ((lvl - 1) << 27) | (int32_t)c;
-        s_bd[wib][slot] = bdc;
+        __syncwarp();
       }
-      sp += cnt;
       __syncwarp();
     }
-    // ---- SPH density (f90:2816-2838), exact evaluation order
-    const int nv = A.nv;
-    const double dlast = __shfl_sync(0xffffffffu, L.ld, nv - 1);
-    const double r = xmul(xsqrt(dlast), 0.5);
-    const double r3 = xmul(xmul(r, r), r);
-    const double unsr = xdiv(1.0, r);
-    double term = 0.0;
-    if (lane < nv - 1) term = xmul(A.m[L.ls], spline(xmul(xsqrt(L.ld), unsr)));
-    double contrib = 0.0;
-    for (int i = 0; i < nv - 1; ++i) contrib = xadd(contrib, __shfl_sync(0xffffffffu, term, i));
-    if (lane == 0) {
-      const double pi_f = (double)3.141592654f;  // f90:58 single-precision literal
-      A.dens[s] = xdiv(xmul(A.xyzlong, xadd(contrib, A.m[s])), xmul(pi_f, r3));
+    // ---- C: per-query kNN over the candidates
+    for (int q = 0; q < nq; ++q) {
+      const int64_t s = s0 + q;
+      const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
+      WarpList L;
+      L.ld = CUDART_INF; L.ls = -1; L.lo = INT_MAX; L.r2 = CUDART_INF;
+      leaf_insert(A, L, jl, s, qx, qy, qz, lane);
+      if (jn >= 0 && jn != jl) leaf_insert(A, L, jn, s, qx, qy, qz, lane);
+      if (overflow) {
+        query_dfs(A, L, s, qx, qy, qz, lane, s_node[wib], s_bd[wib], jl, jn);
+      } else {
+        for (int c0 = 0; c0 < ncand; c0 += 32) {
+          const int ci = c0 + lane;
+          int64_t leaf = -1;
+          double bd = CUDART_INF;
+          if (ci < ncand) {
+            leaf = s_cand[wib][ci];
+            if (leaf != jl && leaf != jn) bd = box_dist2(A.box + 6 * leaf, qx, qy, qz, A.Lx, A.Ly, A.Lz);
+          }
+          unsigned mask = __ballot_sync(0xffffffffu, bd < L.r2);
+          while (mask) {
+            const int src = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const double sbd = __shfl_sync(0xffffffffu, bd, src);
+            const int64_t sl = __shfl_sync(0xffffffffu, leaf, src);
+            if (sbd < L.r2) leaf_insert(A, L, sl, s, qx, qy, qz, lane);
+          }
+        }
+      }
+      finish_query(A, L, s, lane);
+      __syncwarp();
     }
-    if (lane < A.nstore) A.nei[s * A.nstore + lane] = L.ls;
-    __syncwarp();
   }
 }
 
@@ -371,14 +521,14 @@ int stage_knn_density(Engine& E) {
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, E.device);
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, knn_density_kernel, kWarpsPerBlock * 32, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, knn_leaf_kernel, kWarpsPerBlock * 32, 0);
   if (per_sm < 1) per_sm = 1;
-  int64_t want = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  int64_t want = (E.lev_cnt[0] + kWarpsPerBlock - 1) / kWarpsPerBlock;
   int64_t grid = (int64_t)nsm * per_sm * 4;
   if (grid > want) grid = want;
   E.launches++;
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[9], E.stream));
-  knn_density_kernel<<<(unsigned)grid, kWarpsPerBlock * 32, 0, E.stream>>>(A);
+  knn_leaf_kernel<<<(unsigned)grid, kWarpsPerBlock * 32, 0, E.stream>>>(A);
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[10], E.stream));
   AHOP_CUDA_TRY(cudaGetLastError());
   int herr = 0;

@@ -48,6 +48,7 @@ namespace ahop {
 constexpr int kNT = 256;        // threads per task block
 constexpr int kIPT = 4;         // items per thread in the reorder sort
 constexpr int kChunk = kNT * kIPT;
+constexpr int kBigGroup = 96;   // groups larger than this are summed by a warp
 constexpr long long kMaxTaskLevels = 4000000LL;  // cap on one task's threshold levels (error, never a hang)
 
 struct Task {
@@ -95,6 +96,7 @@ struct TreeArgs {
   Task* next;
   int32_t* nnext;
   int32_t* err;           // [0] code, [1] detail
+  unsigned long long* stats;  // [8] per-stage counters (see the end of tree_wave_kernel)
 };
 
 __device__ __forceinline__ void set_err(const TreeArgs& A, int code, int detail) {
@@ -401,7 +403,7 @@ __device__ void approx_stats(const TreeArgs& A, SharedTask& T) {
 
 // Exact sums in the reference order for components flagged in cs[..][10].
 // Per-position scratch gs row: 0 imass 1 truemass 2..4 posg 5 rsquare 6 densmoy
-__device__ void exact_stats(const TreeArgs& A, SharedTask& T) {
+__device__ void exact_stats(const TreeArgs& A, SharedTask& T, double* s_terms) {
   const int tid = threadIdx.x;
   const double rhot = T.rhot;
   // phase 1: posref per flagged component (first particle above rhot of its first group)
@@ -418,14 +420,76 @@ __device__ void exact_stats(const TreeArgs& A, SharedTask& T) {
     C[11] = (double)ref;
   }
   __syncthreads();
-  // phase 2: per group sequential sums (members in decreasing particle index)
+  // phase 2: per group sequential sums (members in decreasing particle index).
+  // Small groups: one thread each.  Large groups: a warp computes the
+  // per-member terms 32 at a time (explicitly rounded, so each term has the
+  // reference's bits) and lane 0 adds them in member order -- the same
+  // sequence of roundings as the Fortran loop, without one dependent global
+  // load per member on a single thread.
+  const int lane = tid & 31, warp = tid >> 5;
+  for (int32_t i = T.a + warp; i < T.b; i += kNT / 32) {
+    const int32_t k = A.compidx[i];
+    const double* C = A.cs + 12 * (size_t)(T.a + k);
+    if (C[10] == 0.0) continue;
+    const int32_t g = A.GL[i];
+    const int32_t q0 = A.goff[g], q1 = A.goff[g + 1];
+    if (q1 - q0 <= kBigGroup) continue;
+    const int32_t ref = (int32_t)C[11];
+    const double rx = A.x[ref], ry = A.y[ref], rz = A.z[ref];
+    int32_t imass = 0;
+    double tm = 0, px = 0, py = 0, pz = 0, rs = 0, dm = 0;
+    double* st = s_terms + (size_t)warp * 32 * 6;
+    for (int32_t base = q0; base < q1; base += 32) {
+      const int32_t q = base + lane;
+      double t[6] = {0, 0, 0, 0, 0, -1.0};  // t[5] < 0 marks "not above rhot"
+      if (q < q1) {
+        const int32_t s = A.gmem[q];
+        const double d = A.dens[s];
+        if (d > rhot) {
+          const double xm = A.m[s];
+          double ux = xadd(wrapd(xsub(A.x[s], rx), A.Lx, A.hx), rx);
+          double uy = xadd(wrapd(xsub(A.y[s], ry), A.Ly, A.hy), ry);
+          double uz = xadd(wrapd(xsub(A.z[s], rz), A.Lz, A.hz), rz);
+          t[0] = xm;
+          t[1] = xmul(ux, xm);
+          t[2] = xmul(uy, xm);
+          t[3] = xmul(uz, xm);
+          t[4] = xmul(xm, xadd(xadd(xmul(ux, ux), xmul(uy, uy)), xmul(uz, uz)));
+          t[5] = d;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 6; ++c) st[lane * 6 + c] = t[c];
+      __syncwarp();
+      if (lane == 0) {
+        const int cnt = min(32, q1 - base);
+        for (int l = 0; l < cnt; ++l) {
+          const double* u = st + l * 6;
+          if (u[5] < 0.0) continue;
+          imass += 1;
+          tm = xadd(tm, u[0]);
+          px = xadd(px, u[1]);
+          py = xadd(py, u[2]);
+          pz = xadd(pz, u[3]);
+          rs = xadd(rs, u[4]);
+          dm = xadd(dm, u[5]);
+        }
+      }
+      __syncwarp();
+    }
+    if (lane == 0) {
+      double* G = A.gs + 8 * (size_t)i;
+      G[0] = (double)imass; G[1] = tm; G[2] = px; G[3] = py; G[4] = pz; G[5] = rs; G[6] = dm;
+    }
+  }
   for (int32_t i = T.a + tid; i < T.b; i += kNT) {
     const int32_t k = A.compidx[i];
     const double* C = A.cs + 12 * (size_t)(T.a + k);
     if (C[10] == 0.0) continue;
+    const int32_t g = A.GL[i];
+    if (A.goff[g + 1] - A.goff[g] > kBigGroup) continue;
     const int32_t ref = (int32_t)C[11];
     const double rx = A.x[ref], ry = A.y[ref], rz = A.z[ref];
-    const int32_t g = A.GL[i];
     int32_t imass = 0;
     double tm = 0, px = 0, py = 0, pz = 0, rs = 0, dm = 0;
     for (int32_t q = A.goff[g]; q < A.goff[g + 1]; ++q) {
@@ -495,8 +559,11 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
   __shared__ typename ScanT::TempStorage scan_tmp;
   __shared__ typename MaxScanT::TempStorage maxscan_tmp;
   __shared__ int32_t s_keys[kChunk];
+  __shared__ double s_terms[kNT / 32 * 32 * 6];
   __shared__ SharedTask T;
+  __shared__ long long s_clk[4];  // structural, approx, exact cycles; levels
   const int tid = threadIdx.x;
+  if (tid < 4) s_clk[tid] = 0;
   if (tid == 0) {
     const Task t = tasks[blockIdx.x];
     T.rhot = t.rhot; T.inode = t.inode; T.a = t.a; T.b = t.b; T.level = t.level;
@@ -512,13 +579,17 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
     // rewrites next_event inside the pass
     const bool restructure = T.rhot >= T.next_event;
     __syncthreads();
+    long long c0 = clock64();
     if (restructure) structural_pass<SortT, ScanT, MaxScanT>(A, T, sort_tmp, scan_tmp, maxscan_tmp, s_keys);
+    long long c1 = clock64();
+    if (tid == 0) { s_clk[0] += c1 - c0; s_clk[3] += 1; }
     if (T.nsurv == 0) {  // all groups below the threshold (f90:1348-1351 prints, then ends with no colour)
       if (tid == 0) A.node[T.inode].firstchild = 0;
       break;
     }
     approx_stats(A, T);
     __syncthreads();
+    if (tid == 0) s_clk[1] += clock64() - c1;
     // flag unknown decisions for exact recomputation
     if (tid == 0) T.nexact = 0;
     __syncthreads();
@@ -529,7 +600,11 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
     __syncthreads();
     const int32_t nexact = T.nexact;  // block-uniform after the barrier
     __syncthreads();
-    if (nexact > 0) exact_stats(A, T);
+    if (nexact > 0) {
+      long long c2 = clock64();
+      exact_stats(A, T, s_terms);
+      if (tid == 0) { s_clk[2] += clock64() - c2; atomicAdd(&A.stats[4], 1ULL); }
+    }
     // count significant components
     if (tid == 0) {
       int32_t ns = 0;
@@ -569,7 +644,9 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
       C[10] = (C[9] == 1.0) ? 1.0 : 0.0;
     }
     __syncthreads();
-    exact_stats(A, T);
+    long long c3 = clock64();
+    exact_stats(A, T, s_terms);
+    if (tid == 0) s_clk[2] += clock64() - c3;
     if (tid == 0) {
       int32_t ns2 = 0;
       for (int32_t k = 0; k < T.ncomp; ++k) ns2 += (A.cs[12 * (size_t)(T.a + k) + 9] == 1.0);
@@ -627,6 +704,16 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
       }
     }
     break;
+  }
+  if (tid == 0) {
+    // [0..2] cycles structural/approx/exact, [3] levels, [4] undecided-test
+    // exact passes, [5] max levels of one task, [6] max cycles of one task
+    atomicAdd(&A.stats[0], (unsigned long long)s_clk[0]);
+    atomicAdd(&A.stats[1], (unsigned long long)s_clk[1]);
+    atomicAdd(&A.stats[2], (unsigned long long)s_clk[2]);
+    atomicAdd(&A.stats[3], (unsigned long long)s_clk[3]);
+    atomicMax(&A.stats[5], (unsigned long long)s_clk[3]);
+    atomicMax(&A.stats[6], (unsigned long long)(s_clk[0] + s_clk[1] + s_clk[2]));
   }
 }
 
@@ -832,9 +919,10 @@ int stage_nodes(Engine& E) {
   tasks[1] = reinterpret_cast<Task*>(take((size_t)(nnodesmax + 1) * sizeof(Task)));
   AHOP_CUDA_TRY(E.d_nodes.ensure((size_t)(nnodesmax + 1) * sizeof(NodeRec)));
   AHOP_CUDA_TRY(cudaMemsetAsync(E.d_nodes.p, 0, (size_t)(nnodesmax + 1) * sizeof(NodeRec), st));
-  AHOP_CUDA_TRY(E.d_flags.ensure(64));
-  AHOP_CUDA_TRY(cudaMemsetAsync(E.d_flags.p, 0, 64, st));
+  AHOP_CUDA_TRY(E.d_flags.ensure(256));
+  AHOP_CUDA_TRY(cudaMemsetAsync(E.d_flags.p, 0, 256, st));
   int32_t* flags = E.d_flags.as<int32_t>();  // [0..1] err, [2] nnodes, [3] nnext
+  A.stats = reinterpret_cast<unsigned long long*>(E.d_flags.as<char>() + 128);
   A.err = flags;
   A.nnodes = flags + 2;
   A.nnext = flags + 3;
@@ -923,6 +1011,7 @@ int stage_nodes(Engine& E) {
     AHOP_CUDA_TRY(cudaGetLastError());
   }
   AHOP_CUDA_TRY(cudaMemcpyAsync(h, flags, 8, cudaMemcpyDeviceToHost, st));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(E.tree_stats, E.d_flags.as<char>() + 128, 8 * 8, cudaMemcpyDeviceToHost, st));
   AHOP_CUDA_TRY(cudaStreamSynchronize(st));
   if (h[0] != 0) {
     set_error("membership walk exceeded its bound");

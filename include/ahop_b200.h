@@ -100,8 +100,13 @@ int ahop_get_outputs(AhopOutputs* out);
 /* Device-pointer view of the same outputs after either compute call. */
 int ahop_get_device_outputs(AhopOutputs* out);
 int ahop_get_timings(AhopTimings* t);
-/* replaces close (pyf:67, f90:3227): frees every module buffer. */
+/* replaces close (pyf:67, f90:3227): drops the module outputs.  Device
+ * buffers stay cached for the next compute; ahop_release_device_memory()
+ * frees them. */
 int ahop_close(void);
+/* Frees every device buffer of the finder (no reference counterpart: the
+ * Fortran module has no device memory). */
+int ahop_release_device_memory(void);
 
 /* ---- stage views for parity tests (host copies of device intermediates) ---- */
 /* First k (<= stored count) neighbours of every particle, 1-based ids, sorted by
@@ -121,6 +126,11 @@ int ahop_debug_saddles(int32_t* nconn, int32_t* offsets, int32_t* isad, double* 
  * 3 = hop + groups, 4 = saddles, 5 = everything) for stage-wise parity tests;
  * the stage views above then describe that partial run. */
 int ahop_debug_compute_stages(const double* pos_in, const double* mass_in, int64_t npart, int32_t last_stage);
+/* Structure-tree kernel counters of the last compute: cycles in structural
+ * passes, in per-level statistics and in exact recomputation (summed over
+ * blocks), threshold levels, exact passes for undecided tests, the largest
+ * number of levels of one task and the largest cycle count of one task. */
+int ahop_debug_tree_stats(int64_t* out, int32_t n);
 /* Ask compute to keep the first k neighbours per particle (default nhop). */
 int ahop_debug_set_store_neighbours(int32_t k);
 
