@@ -1,0 +1,42 @@
+"""MSM halo/subhalo selection and member grouping through the C ABI.
+
+After a finder compute, ``select()`` returns what select_with_MS_method_1319
+(src/compute_neiKDtree_mod.py:260-464) and the grouping of NEI:107-119 leave
+in the reference's shared arrays: structure id per particle
+(whereIam_parts), the structure tree (mother/first_sister/first_daughter/
+level) and the members grouped by structure.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+
+
+class AhopStructs(C.Structure):
+    _fields_ = [("nstruct", C.c_int32), ("nb_of_halos", C.c_int32), ("nb_of_subhalos", C.c_int32),
+                ("ngroupruns", C.c_int32), ("nusedpart", C.c_int64), ("whereIam_parts", C.c_void_p),
+                ("mother", C.c_void_p), ("first_sister", C.c_void_p), ("first_daughter", C.c_void_p),
+                ("level", C.c_void_p), ("pids_groupsorted", C.c_void_p), ("run_ids", C.c_void_p),
+                ("run_idxs", C.c_void_p), ("run_counts", C.c_void_p)]
+
+
+def _arr(p, n):
+    if n == 0:
+        return np.empty(0, np.int32)
+    return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_int32)), (n,)).copy()
+
+
+def select() -> dict:
+    lib = L.lib()
+    lib.ahop_select_msm.argtypes = [C.POINTER(AhopStructs)]
+    o = AhopStructs()
+    L.check(lib.ahop_select_msm(C.byref(o)), "select_msm")
+    n, ns, nr = int(o.nusedpart), int(o.nstruct), int(o.ngroupruns)
+    return dict(nstruct=ns, nb_of_halos=int(o.nb_of_halos), nb_of_subhalos=int(o.nb_of_subhalos),
+                whereIam_parts=_arr(o.whereIam_parts, n), mother=_arr(o.mother, ns),
+                first_sister=_arr(o.first_sister, ns), first_daughter=_arr(o.first_daughter, ns),
+                level=_arr(o.level, ns), pids_groupsorted=_arr(o.pids_groupsorted, n),
+                run_ids=_arr(o.run_ids, nr), run_idxs=_arr(o.run_idxs, nr), run_counts=_arr(o.run_counts, nr))

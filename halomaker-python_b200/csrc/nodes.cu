@@ -401,156 +401,265 @@ __device__ void approx_stats(const TreeArgs& A, SharedTask& T) {
   }
 }
 
-// Exact sums in the reference order for components flagged in cs[..][10].
-// Per-position scratch gs row: 0 imass 1 truemass 2..4 posg 5 rsquare 6 densmoy
+// Exact per-group sums in the reference order (treat_particles f90:2317-2401):
+// members in decreasing particle index, only those above rhot, positions
+// unwrapped about posref then shifted back.  G[0..6] = imass, truemass,
+// posg(3), rsquare, densmoy.
+__device__ void group_sums_thread(const TreeArgs& A, int32_t g, double rhot, double rx, double ry, double rz,
+                                  double* G) {
+  int32_t imass = 0;
+  double tm = 0, px = 0, py = 0, pz = 0, rs = 0, dm = 0;
+  for (int32_t q = A.goff[g]; q < A.goff[g + 1]; ++q) {
+    const int32_t s = A.gmem[q];
+    const double d = A.dens[s];
+    if (!(d > rhot)) continue;
+    imass += 1;
+    const double xm = A.m[s];
+    tm = xadd(tm, xm);
+    double ux = wrapd(xsub(A.x[s], rx), A.Lx, A.hx);
+    double uy = wrapd(xsub(A.y[s], ry), A.Ly, A.hy);
+    double uz = wrapd(xsub(A.z[s], rz), A.Lz, A.hz);
+    ux = xadd(ux, rx);
+    uy = xadd(uy, ry);
+    uz = xadd(uz, rz);
+    px = xadd(px, xmul(ux, xm));
+    py = xadd(py, xmul(uy, xm));
+    pz = xadd(pz, xmul(uz, xm));
+    rs = xadd(rs, xmul(xm, xadd(xadd(xmul(ux, ux), xmul(uy, uy)), xmul(uz, uz))));
+    dm = xadd(dm, d);
+  }
+  G[0] = (double)imass; G[1] = tm; G[2] = px; G[3] = py; G[4] = pz; G[5] = rs; G[6] = dm;
+}
+
+// Same sums for a large group by one warp: each lane computes the terms of
+// one member (explicitly rounded, so each term has the reference's bits) and
+// lane 0 adds them in member order -- the same sequence of roundings as the
+// Fortran loop, without one dependent global load per member on one thread.
+// st: 32*6 doubles of warp-private shared memory.
+__device__ void group_sums_warp(const TreeArgs& A, int32_t g, double rhot, double rx, double ry, double rz,
+                                double* G, double* st, int lane) {
+  const int32_t q0 = A.goff[g], q1 = A.goff[g + 1];
+  int32_t imass = 0;
+  double tm = 0, px = 0, py = 0, pz = 0, rs = 0, dm = 0;
+  for (int32_t base = q0; base < q1; base += 32) {
+    const int32_t q = base + lane;
+    double t[6] = {0, 0, 0, 0, 0, -1.0};  // t[5] < 0 marks "not above rhot"
+    if (q < q1) {
+      const int32_t s = A.gmem[q];
+      const double d = A.dens[s];
+      if (d > rhot) {
+        const double xm = A.m[s];
+        const double ux = xadd(wrapd(xsub(A.x[s], rx), A.Lx, A.hx), rx);
+        const double uy = xadd(wrapd(xsub(A.y[s], ry), A.Ly, A.hy), ry);
+        const double uz = xadd(wrapd(xsub(A.z[s], rz), A.Lz, A.hz), rz);
+        t[0] = xm;
+        t[1] = xmul(ux, xm);
+        t[2] = xmul(uy, xm);
+        t[3] = xmul(uz, xm);
+        t[4] = xmul(xm, xadd(xadd(xmul(ux, ux), xmul(uy, uy)), xmul(uz, uz)));
+        t[5] = d;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) st[lane * 6 + c] = t[c];
+    __syncwarp();
+    if (lane == 0) {
+      const int cnt = min(32, q1 - base);
+      for (int l = 0; l < cnt; ++l) {
+        const double* u = st + l * 6;
+        if (u[5] < 0.0) continue;
+        imass += 1;
+        tm = xadd(tm, u[0]);
+        px = xadd(px, u[1]);
+        py = xadd(py, u[2]);
+        pz = xadd(pz, u[3]);
+        rs = xadd(rs, u[4]);
+        dm = xadd(dm, u[5]);
+      }
+    }
+    __syncwarp();
+  }
+  if (lane == 0) { G[0] = (double)imass; G[1] = tm; G[2] = px; G[3] = py; G[4] = pz; G[5] = rs; G[6] = dm; }
+}
+
+// posref of a colour: first particle above rhot of its first group (f90:2340-2344).
+__device__ int32_t colour_posref(const TreeArgs& A, int32_t g0, double rhot) {
+  for (int32_t q = A.goff[g0]; q < A.goff[g0 + 1]; ++q) {
+    const int32_t s = A.gmem[q];
+    if (A.dens[s] > rhot) return s;
+  }
+  set_err(A, 18, g0);  // cannot happen: the peak is above rhot
+  return A.gpeak[g0];
+}
+
+// Fold a colour's group sums in GL order and apply the significance test
+// (f90:1407-1466).  Exact record: C[0] mass_loc, C[1] mass_comp, C[2] densmax,
+// C[3] densmoy, C[4] truemass, C[5..7] posg, C[8] radius, C[9] decision.
+__device__ void colour_fold(const TreeArgs& A, int32_t c0, int32_t c1, double rhot, double* C) {
+  double posg0 = 0, posg1 = 0, posg2 = 0, tm = 0, rsg = 0, dmg = 0, dmax = -1.0, dcm = -1.0;
+  int32_t ml = 0, mc = 0;
+  for (int32_t i = c0; i < c1; ++i) {
+    const double* G = A.gs + 8 * (size_t)i;
+    const int32_t g = A.GL[i];
+    dmax = fmax(dmax, A.densg[g]);
+    const int32_t mt = (int32_t)G[0];
+    posg0 = xadd(posg0, G[2]);
+    posg1 = xadd(posg1, G[3]);
+    posg2 = xadd(posg2, G[4]);
+    rsg = xadd(rsg, G[5]);
+    ml += mt;
+    tm = xadd(tm, G[1]);
+    dmg = xadd(dmg, G[6]);
+    mc = max(mc, mt);
+    if (mt > 0) {
+      const double dmt = xdiv(G[6], (double)mt);
+      dcm = fmax(dcm, xdiv(dmt, xadd(1.0, xdiv(A.fudge, xsqrt((double)mt)))));
+    }
+  }
+  const double p2 = xadd(xadd(xmul(posg0, posg0), xmul(posg1, posg1)), xmul(posg2, posg2));
+  const double rsq = xsqrt(fabs(xdiv(xsub(xmul(tm, rsg), p2), xmul(tm, tm))));
+  const double densmoy = xdiv(dmg, (double)ml);
+  const bool ok = ml >= A.nmembthresh &&
+                  (densmoy > xmul(rhot, xadd(1.0, xdiv(A.fudge, xsqrt((double)ml)))) || dcm > rhot) &&
+                  dmax >= xmul(A.alphap, densmoy) && rsq >= A.epsilon;
+  C[0] = (double)ml; C[1] = (double)mc; C[2] = dmax; C[3] = densmoy; C[4] = tm;
+  C[5] = posg0; C[6] = posg1; C[7] = posg2; C[8] = rsq; C[9] = ok ? 1.0 : 0.0;
+}
+
+// Exact sums in the reference order for the colours flagged in cs[..][10].
 __device__ void exact_stats(const TreeArgs& A, SharedTask& T, double* s_terms) {
   const int tid = threadIdx.x;
   const double rhot = T.rhot;
-  // phase 1: posref per flagged component (first particle above rhot of its first group)
   for (int32_t k = tid; k < T.ncomp; k += kNT) {
     double* C = A.cs + 12 * (size_t)(T.a + k);
     if (C[10] == 0.0) continue;
-    const int32_t g0 = A.GL[A.cstart[T.a + k]];
-    int32_t ref = -1;
-    for (int32_t q = A.goff[g0]; q < A.goff[g0 + 1]; ++q) {
-      int32_t s = A.gmem[q];
-      if (A.dens[s] > rhot) { ref = s; break; }
-    }
-    if (ref < 0) { set_err(A, 18, g0); ref = A.gpeak[g0]; }  // cannot happen: the peak is above rhot
-    C[11] = (double)ref;
+    C[11] = (double)colour_posref(A, A.GL[A.cstart[T.a + k]], rhot);
   }
   __syncthreads();
-  // phase 2: per group sequential sums (members in decreasing particle index).
-  // Small groups: one thread each.  Large groups: a warp computes the
-  // per-member terms 32 at a time (explicitly rounded, so each term has the
-  // reference's bits) and lane 0 adds them in member order -- the same
-  // sequence of roundings as the Fortran loop, without one dependent global
-  // load per member on a single thread.
   const int lane = tid & 31, warp = tid >> 5;
-  for (int32_t i = T.a + warp; i < T.b; i += kNT / 32) {
-    const int32_t k = A.compidx[i];
-    const double* C = A.cs + 12 * (size_t)(T.a + k);
+  for (int32_t i = T.a + warp; i < T.b; i += kNT / 32) {  // large groups: a warp each
+    const double* C = A.cs + 12 * (size_t)(T.a + A.compidx[i]);
     if (C[10] == 0.0) continue;
     const int32_t g = A.GL[i];
-    const int32_t q0 = A.goff[g], q1 = A.goff[g + 1];
-    if (q1 - q0 <= kBigGroup) continue;
+    if (A.goff[g + 1] - A.goff[g] <= kBigGroup) continue;
     const int32_t ref = (int32_t)C[11];
-    const double rx = A.x[ref], ry = A.y[ref], rz = A.z[ref];
-    int32_t imass = 0;
-    double tm = 0, px = 0, py = 0, pz = 0, rs = 0, dm = 0;
-    double* st = s_terms + (size_t)warp * 32 * 6;
-    for (int32_t base = q0; base < q1; base += 32) {
-      const int32_t q = base + lane;
-      double t[6] = {0, 0, 0, 0, 0, -1.0};  // t[5] < 0 marks "not above rhot"
-      if (q < q1) {
-        const int32_t s = A.gmem[q];
-        const double d = A.dens[s];
-        if (d > rhot) {
-          const double xm = A.m[s];
-          double ux = xadd(wrapd(xsub(A.x[s], rx), A.Lx, A.hx), rx);
-          double uy = xadd(wrapd(xsub(A.y[s], ry), A.Ly, A.hy), ry);
-          double uz = xadd(wrapd(xsub(A.z[s], rz), A.Lz, A.hz), rz);
-          t[0] = xm;
-          t[1] = xmul(ux, xm);
-          t[2] = xmul(uy, xm);
-          t[3] = xmul(uz, xm);
-          t[4] = xmul(xm, xadd(xadd(xmul(ux, ux), xmul(uy, uy)), xmul(uz, uz)));
-          t[5] = d;
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < 6; ++c) st[lane * 6 + c] = t[c];
-      __syncwarp();
-      if (lane == 0) {
-        const int cnt = min(32, q1 - base);
-        for (int l = 0; l < cnt; ++l) {
-          const double* u = st + l * 6;
-          if (u[5] < 0.0) continue;
-          imass += 1;
-          tm = xadd(tm, u[0]);
-          px = xadd(px, u[1]);
-          py = xadd(py, u[2]);
-          pz = xadd(pz, u[3]);
-          rs = xadd(rs, u[4]);
-          dm = xadd(dm, u[5]);
-        }
-      }
-      __syncwarp();
-    }
-    if (lane == 0) {
-      double* G = A.gs + 8 * (size_t)i;
-      G[0] = (double)imass; G[1] = tm; G[2] = px; G[3] = py; G[4] = pz; G[5] = rs; G[6] = dm;
-    }
+    group_sums_warp(A, g, rhot, A.x[ref], A.y[ref], A.z[ref], A.gs + 8 * (size_t)i, s_terms + warp * 32 * 6, lane);
   }
-  for (int32_t i = T.a + tid; i < T.b; i += kNT) {
-    const int32_t k = A.compidx[i];
-    const double* C = A.cs + 12 * (size_t)(T.a + k);
+  for (int32_t i = T.a + tid; i < T.b; i += kNT) {  // small groups: a thread each
+    const double* C = A.cs + 12 * (size_t)(T.a + A.compidx[i]);
     if (C[10] == 0.0) continue;
     const int32_t g = A.GL[i];
     if (A.goff[g + 1] - A.goff[g] > kBigGroup) continue;
     const int32_t ref = (int32_t)C[11];
-    const double rx = A.x[ref], ry = A.y[ref], rz = A.z[ref];
-    int32_t imass = 0;
-    double tm = 0, px = 0, py = 0, pz = 0, rs = 0, dm = 0;
-    for (int32_t q = A.goff[g]; q < A.goff[g + 1]; ++q) {
-      const int32_t s = A.gmem[q];
-      const double d = A.dens[s];
-      if (!(d > rhot)) continue;
-      imass += 1;
-      const double xm = A.m[s];
-      tm = xadd(tm, xm);
-      double ux = wrapd(xsub(A.x[s], rx), A.Lx, A.hx);
-      double uy = wrapd(xsub(A.y[s], ry), A.Ly, A.hy);
-      double uz = wrapd(xsub(A.z[s], rz), A.Lz, A.hz);
-      ux = xadd(ux, rx);
-      uy = xadd(uy, ry);
-      uz = xadd(uz, rz);
-      px = xadd(px, xmul(ux, xm));
-      py = xadd(py, xmul(uy, xm));
-      pz = xadd(pz, xmul(uz, xm));
-      rs = xadd(rs, xmul(xm, xadd(xadd(xmul(ux, ux), xmul(uy, uy)), xmul(uz, uz))));
-      dm = xadd(dm, d);
-    }
-    double* G = A.gs + 8 * (size_t)i;
-    G[0] = (double)imass; G[1] = tm; G[2] = px; G[3] = py; G[4] = pz; G[5] = rs; G[6] = dm;
+    group_sums_thread(A, g, rhot, A.x[ref], A.y[ref], A.z[ref], A.gs + 8 * (size_t)i);
   }
   __syncthreads();
-  // phase 3: fold over groups in GL order and test (f90:1407-1466)
   for (int32_t k = tid; k < T.ncomp; k += kNT) {
     double* C = A.cs + 12 * (size_t)(T.a + k);
     if (C[10] == 0.0) continue;
-    const int32_t c0 = A.cstart[T.a + k], c1 = comp_end(A, T, k);
-    double posg0 = 0, posg1 = 0, posg2 = 0, tm = 0, rsg = 0, dmg = 0, dmax = -1.0, dcm = -1.0;
-    int32_t ml = 0, mc = 0;
-    for (int32_t i = c0; i < c1; ++i) {
-      const double* G = A.gs + 8 * (size_t)i;
-      const int32_t g = A.GL[i];
-      dmax = fmax(dmax, A.densg[g]);
-      const int32_t mt = (int32_t)G[0];
-      posg0 = xadd(posg0, G[2]);
-      posg1 = xadd(posg1, G[3]);
-      posg2 = xadd(posg2, G[4]);
-      rsg = xadd(rsg, G[5]);
-      ml += mt;
-      tm = xadd(tm, G[1]);
-      dmg = xadd(dmg, G[6]);
-      mc = max(mc, mt);
-      if (mt > 0) {
-        const double dmt = xdiv(G[6], (double)mt);
-        dcm = fmax(dcm, xdiv(dmt, xadd(1.0, xdiv(A.fudge, xsqrt((double)mt)))));
-      }
-    }
-    const double p2 = xadd(xadd(xmul(posg0, posg0), xmul(posg1, posg1)), xmul(posg2, posg2));
-    const double rsq = xsqrt(fabs(xdiv(xsub(xmul(tm, rsg), p2), xmul(tm, tm))));
-    const double densmoy = xdiv(dmg, (double)ml);
-    const bool ok = ml >= A.nmembthresh &&
-                    (densmoy > xmul(rhot, xadd(1.0, xdiv(A.fudge, xsqrt((double)ml)))) || dcm > rhot) &&
-                    dmax >= xmul(A.alphap, densmoy) && rsq >= A.epsilon;
-    // exact record: 0 mass_loc 1 mass_comp 2 densmax 3 densmoy 4 truemass 5..7 posg 8 radius 9 decision
-    C[0] = (double)ml; C[1] = (double)mc; C[2] = dmax; C[3] = densmoy; C[4] = tm;
-    C[5] = posg0; C[6] = posg1; C[7] = posg2; C[8] = rsq; C[9] = ok ? 1.0 : 0.0;
+    colour_fold(A, A.cstart[T.a + k], comp_end(A, T, k), rhot, C);
   }
   __syncthreads();
+}
+
+// ------------------------------------------------ root level on the whole grid
+// The first iteration of the root task (rhot = rho_threshold over every group,
+// f90:930-958) colours all groups at once; it runs here as grid-wide kernels
+// instead of one block.  Colours are connected components of the saddle graph
+// (every saddle exceeds rho_threshold), ordered by their smallest group id,
+// groups inside a colour by id -- the reference's idgroup order.
+__global__ void root_union_kernel(const TreeArgs A, double rhot) {
+  const int32_t g = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (g > A.ngroups) return;
+  for (int32_t e = A.soff[g - 1]; e < A.soff[g]; ++e) {
+    if (!(A.srho[e] > rhot)) break;
+    uf_union(A.par, g - 1, A.sisad[e] - 1);
+  }
+}
+
+__global__ void root_roots_kernel(const TreeArgs A, int32_t* keys, int32_t* vals) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.ngroups) return;
+  keys[i] = uf_find(A.par, i);
+  vals[i] = i + 1;
+}
+
+// heads of colour runs (keys sorted) -> cstart via an exclusive scan of flags
+__global__ void root_heads_kernel(const TreeArgs A, const int32_t* keys, int32_t* flag) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > A.ngroups) return;
+  flag[i] = (i < A.ngroups && (i == 0 || keys[i] != keys[i - 1])) ? 1 : 0;
+  if (i < A.ngroups) A.pos_of[A.GL[i]] = i;
+}
+
+__global__ void root_cstart_kernel(const TreeArgs A, const int32_t* flag, const int32_t* scan) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.ngroups) return;
+  if (flag[i]) A.cstart[scan[i]] = i;
+  A.compidx[i] = scan[i] + flag[i] - 1;
+}
+
+// one block per colour: exact sums and the significance test
+__global__ void __launch_bounds__(kNT) root_colour_kernel(const TreeArgs A, int32_t ncomp, double rhot) {
+  __shared__ double s_terms[kNT / 32 * 32 * 6];
+  __shared__ int32_t s_ref;
+  const int32_t k = blockIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int32_t c0 = A.cstart[k], c1 = (k + 1 < ncomp) ? A.cstart[k + 1] : A.ngroups;
+  if (tid == 0) s_ref = colour_posref(A, A.GL[c0], rhot);
+  __syncthreads();
+  const int32_t ref = s_ref;
+  const double rx = A.x[ref], ry = A.y[ref], rz = A.z[ref];
+  for (int32_t i = c0 + warp; i < c1; i += kNT / 32) {
+    const int32_t g = A.GL[i];
+    if (A.goff[g + 1] - A.goff[g] > kBigGroup)
+      group_sums_warp(A, g, rhot, rx, ry, rz, A.gs + 8 * (size_t)i, s_terms + warp * 32 * 6, lane);
+  }
+  for (int32_t i = c0 + tid; i < c1; i += kNT) {
+    const int32_t g = A.GL[i];
+    if (A.goff[g + 1] - A.goff[g] <= kBigGroup) group_sums_thread(A, g, rhot, rx, ry, rz, A.gs + 8 * (size_t)i);
+  }
+  __syncthreads();
+  if (tid == 0) colour_fold(A, c0, c1, rhot, A.cs + 12 * (size_t)k);
+}
+
+__global__ void root_okflag_kernel(const TreeArgs A, int32_t ncomp, int32_t* flag) {
+  const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > ncomp) return;
+  flag[k] = (k < ncomp && A.cs[12 * (size_t)k + 9] == 1.0) ? 1 : 0;
+}
+
+// level-1 nodes in colour order (reserve_nodes_block gives 1..nsisters),
+// child tasks (f90:1484-1571), deepest node per group
+__global__ void root_nodes_kernel(const TreeArgs A, int32_t ncomp, const int32_t* flag, const int32_t* rank,
+                                  int32_t nsisters, double rhot, Task* next) {
+  const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ncomp || !flag[k]) return;
+  const double* C = A.cs + 12 * (size_t)k;
+  const int32_t is = rank[k];
+  const int32_t io = 1 + is;
+  NodeRec& nd = A.node[io];
+  nd.mother = 0;
+  nd.densmax = C[2];
+  nd.sister = is > 0 ? io - 1 : 0;
+  nd.nsisters = nsisters;
+  nd.mass = (int32_t)C[0];
+  nd.truemass = C[4];
+  double pf0 = xdiv(C[5], C[4]), pf1 = xdiv(C[6], C[4]), pf2 = xdiv(C[7], C[4]);
+  nd.radius = C[8];
+  nd.density = C[3];
+  if (pf0 >= A.hx) pf0 = xsub(pf0, A.Lx); else if (pf0 < -A.hx) pf0 = xadd(pf0, A.Lx);
+  if (pf1 >= A.hy) pf1 = xsub(pf1, A.Ly); else if (pf1 < -A.hy) pf1 = xadd(pf1, A.Ly);
+  if (pf2 >= A.hz) pf2 = xsub(pf2, A.Lz); else if (pf2 < -A.hz) pf2 = xadd(pf2, A.Lz);
+  nd.pos[0] = pf0; nd.pos[1] = pf1; nd.pos[2] = pf2;
+  nd.rho_saddle = rhot;
+  nd.level = 1;
+  nd.firstchild = 0;
+  if (nd.mass == 0) set_err(A, 15, io);
+  const int32_t c0 = A.cstart[k], c1 = (k + 1 < ncomp) ? A.cstart[k + 1] : A.ngroups;
+  next[is] = Task{xmul(rhot, xadd(1.0, xdiv(A.fudge, xsqrt(C[1])))), io, c0, c1, 1};
+  for (int32_t i = c0; i < c1; ++i) A.deepnode[A.GL[i]] = io;
+  if (is == nsisters - 1) A.node[0].firstchild = io;  // f90:1540
 }
 
 template <class SortT, class ScanT, class MaxScanT>
@@ -957,6 +1066,70 @@ int stage_nodes(Engine& E) {
   int32_t ntasks = 1;
   int cur = 0;
   int32_t* h = reinterpret_cast<int32_t*>(E.h_scalars);
+  // ---- root level on the whole grid
+  {
+    const double rhot = P.rho_threshold;
+    const unsigned gb = (unsigned)((ng + T - 1) / T);
+    E.launches++;
+    iota_kernel<<<gb, T, 0, st>>>(A.par, ng, 0);
+    E.launches++;
+    root_union_kernel<<<gb, T, 0, st>>>(A, rhot);
+    E.launches++;
+    root_roots_kernel<<<gb, T, 0, st>>>(A, A.cnt, A.run);
+    AHOP_CUDA_TRY(cudaGetLastError());
+    int kb = 1;
+    while ((1LL << kb) <= (int64_t)ng) ++kb;
+    size_t t1 = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, t1, A.cnt, A.par, A.run, A.GL, ng, 0, kb, st);
+    AHOP_CUDA_TRY(E.d_cub.ensure(t1));
+    E.cub_calls++;
+    AHOP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(E.d_cub.p, t1, A.cnt, A.par, A.run, A.GL, ng, 0, kb, st));
+    E.launches++;
+    root_heads_kernel<<<(unsigned)((ng + 1 + T - 1) / T), T, 0, st>>>(A, A.par, A.cnt);
+    t1 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, t1, A.cnt, A.run, ng + 1, st);
+    AHOP_CUDA_TRY(E.d_cub.ensure(t1));
+    E.cub_calls++;
+    AHOP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(E.d_cub.p, t1, A.cnt, A.run, ng + 1, st));
+    E.launches++;
+    root_cstart_kernel<<<gb, T, 0, st>>>(A, A.cnt, A.run);
+    AHOP_CUDA_TRY(cudaMemcpyAsync(h + 4, A.run + ng, 4, cudaMemcpyDeviceToHost, st));
+    AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+    const int32_t ncomp = h[4];
+    E.launches++;
+    root_colour_kernel<<<ncomp, kNT, 0, st>>>(A, ncomp, rhot);
+    E.launches++;
+    root_okflag_kernel<<<(unsigned)((ncomp + 1 + T - 1) / T), T, 0, st>>>(A, ncomp, A.cnt);
+    t1 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, t1, A.cnt, A.run, ncomp + 1, st);
+    AHOP_CUDA_TRY(E.d_cub.ensure(t1));
+    E.cub_calls++;
+    AHOP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(E.d_cub.p, t1, A.cnt, A.run, ncomp + 1, st));
+    AHOP_CUDA_TRY(cudaMemcpyAsync(h + 4, A.run + ncomp, 4, cudaMemcpyDeviceToHost, st));
+    AHOP_CUDA_TRY(cudaMemcpyAsync(h, flags, 8, cudaMemcpyDeviceToHost, st));
+    AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h[0] != 0) {
+      set_error("structure tree invariant failed at the root level (code " + std::to_string(h[0]) + ")");
+      return AHOP_EINVARIANT;
+    }
+    const int32_t nsis = h[4];
+    if (nsis >= 2) {
+      // the root branches at once (the usual case): level-1 nodes 1..nsis
+      E.launches++;
+      root_nodes_kernel<<<(unsigned)((ncomp + T - 1) / T), T, 0, st>>>(A, ncomp, A.cnt, A.run, nsis, rhot,
+                                                                       tasks[1]);
+      AHOP_CUDA_TRY(cudaGetLastError());
+      AHOP_CUDA_TRY(cudaMemcpyAsync(A.nnodes, &nsis, 4, cudaMemcpyHostToDevice, st));
+      ntasks = nsis;
+      cur = 1;
+    } else {
+      // zero or one significant colour: the root task continues (f90:1577-1626)
+      // on the general path from the initial group order
+      E.launches++;
+      init_groups_kernel<<<(unsigned)((ng + 1 + T - 1) / T), T, 0, st>>>(ng, A.GL, A.pos_of, A.deepnode);
+      AHOP_CUDA_TRY(cudaGetLastError());
+    }
+  }
   for (int wave = 0; ntasks > 0; ++wave) {
     if (wave > 100000) { set_error("structure tree: too many waves"); return AHOP_ELIMIT; }
     A.next = tasks[cur ^ 1];

@@ -134,6 +134,27 @@ int ahop_debug_tree_stats(int64_t* out, int32_t n);
 /* Ask compute to keep the first k neighbours per particle (default nhop). */
 int ahop_debug_set_store_neighbours(int32_t k);
 
+/* ---- halo/subhalo selection (MSM) and member grouping --------------------------
+ * Replaces select_with_MS_method_1319 (src/compute_neiKDtree_mod.py:260-464)
+ * and the member grouping of compute_adaptahop_131 (NEI:107-119), on the
+ * device outputs of the last compute.  Structure ids are 1-based; particles in
+ * no node get 0.  mother/first_sister/first_daughter/level are the
+ * reference's mother_1319/first_sister_1319/first_daughter_1319/level_1319
+ * (-1 = none, 0 = no mother).  pids_groupsorted lists 0-based particle
+ * indices grouped by structure id (ascending), members in increasing index;
+ * run_ids/run_idxs/run_counts are np.unique(..., return_index=True,
+ * return_counts=True) of the sorted ids.  Host views, valid until the next
+ * call. */
+typedef struct {
+  int32_t nstruct, nb_of_halos, nb_of_subhalos, ngroupruns;
+  int64_t nusedpart;
+  const int32_t* whereIam_parts;
+  const int32_t *mother, *first_sister, *first_daughter, *level;
+  const int32_t* pids_groupsorted;
+  const int32_t *run_ids, *run_idxs, *run_counts;
+} AhopStructs;
+int ahop_select_msm(AhopStructs* out);
+
 /* ---- batched halo properties ------------------------------------------------
  * Replaces the per-halo reductions of src/compute_halo_props.py run by
  * _compute_halo_props (CHP:270-301): det_mass_17, det_center_18 (densest
