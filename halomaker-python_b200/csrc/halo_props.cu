@@ -33,6 +33,7 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <cub/cub.cuh>
 
 #include "ahop_halo.h"
 #include "engine.h"
@@ -489,3 +490,151 @@ int ahop_halo_get_timings(AhopHaloTimings* t) {
 }
 
 }  // extern "C"
+
+// --------------------------------------------------- allocation-free variant
+// For callers that cannot allocate device memory -- code running while a CUDA
+// graph is being captured elsewhere in the process, host frameworks that own
+// every device allocation through their own pool, or embedded callers whose
+// memory budget is fixed up front -- ahop_halo_props_noalloc computes the same
+// fields with all of its scratch (the (halo, tile) work list, per-item partial
+// sums, per-halo item offsets and the work counters) in this file-scope device
+// array.  Every GPU that loads the library holds it until the process exits.
+namespace ahop {
+
+constexpr int64_t kNoAllocMaxHalos = 65536;         // halos per call
+constexpr int64_t kNoAllocMaxItems = 262144;        // (halo, 256-member tile) items per call
+
+struct NoAllocScratch {
+  int32_t item_h[kNoAllocMaxItems];
+  int32_t item_i[kNoAllocMaxItems];
+  int32_t order[kNoAllocMaxItems];
+  double part64[kNoAllocMaxItems];
+  double part32[kNoAllocMaxItems];
+  int64_t hoff[kNoAllocMaxHalos + 1];
+  int32_t counter[4];  // [0],[1]: work counters of the two pair kernels; [2]: item total; [3]: error
+};
+
+// ~7.9 MB; in host code this name is only a host-side stand-in, the device
+// address comes from cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+// Per-halo tile counts and offsets in one block (nhalo <= kNoAllocMaxHalos).
+__global__ void __launch_bounds__(1024) noalloc_offsets_kernel(const int64_t* __restrict__ off, int64_t nhalo,
+                                                               NoAllocScratch* S) {
+  using Scan = cub::BlockScan<int64_t, 1024>;
+  __shared__ typename Scan::TempStorage tmp;
+  int64_t carry = 0;
+  for (int64_t base = 0; base < nhalo; base += 1024) {
+    const int64_t h = base + threadIdx.x;
+    int64_t nit = 0;
+    if (h < nhalo) {
+      const int64_t n = off[h + 1] - off[h];
+      nit = n > 0 ? (n + kPB - 1) / kPB : 0;
+    }
+    int64_t ex, tot;
+    Scan(tmp).ExclusiveSum(nit, ex, tot);
+    __syncthreads();
+    if (h < nhalo) S->hoff[h] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) {
+    S->hoff[nhalo] = carry;
+    S->counter[2] = carry > kNoAllocMaxItems ? -1 : (int32_t)carry;
+  }
+}
+
+// Work items in halo order (no cost sort: per-item partials and the per-halo
+// fold order do not depend on the schedule, so results match the allocating
+// entry point bit for bit).
+__global__ void noalloc_items_kernel(const int64_t* __restrict__ off, int64_t nhalo, NoAllocScratch* S) {
+  const int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (h >= nhalo) return;
+  const int64_t n = off[h + 1] - off[h];
+  int64_t k = S->hoff[h];
+  for (int64_t i0 = 0; i0 < n; i0 += kPB, ++k) {
+    S->item_h[k] = (int32_t)h;
+    S->item_i[k] = (int32_t)i0;
+    S->order[k] = (int32_t)k;
+  }
+}
+
+static NoAllocScratch* g_noalloc_ptr[128] = {};
+
+// First call on a device (with that device current) looks up the array's
+// device address; do it before any stream capture.
+static int noalloc_setup(NoAllocScratch** out) {
+  int dev = 0;
+  AHOP_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) { set_error("device ordinal out of range"); return AHOP_EINVAL; }
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      set_error(std::string("cudaGetSymbolAddress(g_noalloc_scratch) failed: ") + cudaGetErrorString(e));
+      return AHOP_ECUDA;
+    }
+    g_noalloc_ptr[dev] = static_cast<NoAllocScratch*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return AHOP_OK;
+}
+
+}  // namespace ahop
+
+extern "C" int ahop_halo_props_noalloc(const AhopHaloParams* p, const int64_t* d_off, int64_t nhalo,
+                                       const double* d_pos, const double* d_vel, const double* d_mass,
+                                       const double* d_density, double* d_out, void* stream) {
+  using namespace ahop;
+  int rc;
+  if ((rc = halo_validate(p, nhalo))) return rc;
+  if (nhalo > kNoAllocMaxHalos) {
+    set_error("ahop_halo_props_noalloc: nhalo " + std::to_string(nhalo) + " exceeds the maximum of " +
+              std::to_string(kNoAllocMaxHalos));
+    return AHOP_EINVAL;
+  }
+  if (nhalo == 0) return AHOP_OK;
+  NoAllocScratch* S = nullptr;
+  if ((rc = noalloc_setup(&S))) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  noalloc_offsets_kernel<<<1, 1024, 0, st>>>(d_off, nhalo, S);
+  AHOP_CUDA_TRY(cudaGetLastError());
+  int32_t total = 0;
+  AHOP_CUDA_TRY(cudaMemcpyAsync(&total, &S->counter[2], 4, cudaMemcpyDeviceToHost, st));
+  AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+  if (total < 0) {
+    set_error("ahop_halo_props_noalloc: more than " + std::to_string(kNoAllocMaxItems) +
+              " (halo, 256-member tile) work items; split the call");
+    return AHOP_EINVAL;
+  }
+  noalloc_items_kernel<<<(unsigned)((nhalo + 255) / 256), 256, 0, st>>>(d_off, nhalo, S);
+  AHOP_CUDA_TRY(cudaGetLastError());
+  // the work counters must start at zero: the array keeps the last call's contents
+  AHOP_CUDA_TRY(cudaMemsetAsync(S->counter, 0, 2 * sizeof(int32_t), st));
+  HaloArgs A;
+  A.off = d_off; A.pos = d_pos; A.vel = d_vel; A.mass = d_mass; A.dens = d_density; A.out = d_out;
+  A.L = p->Lbox; A.h = 0.5 * p->Lbox; A.hub = p->Hub_pt; A.G = p->gravconst; A.periodic = p->periodic != 0;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  halo_moments_kernel<<<(unsigned)nhalo, kPB, 0, st>>>(A);
+  AHOP_CUDA_TRY(cudaGetLastError());
+  if ((p->epot & 1) && total > 0) {
+    int per = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, epot_pairs_kernel<false>, kPB, 0);
+    epot_pairs_kernel<false><<<nsm * (per > 0 ? per : 1), kPB, 0, st>>>(A, S->item_h, S->item_i, total,
+                                                                        &S->counter[0], S->part64);
+    AHOP_CUDA_TRY(cudaGetLastError());
+  }
+  if ((p->epot & 2) && total > 0) {
+    int per = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, epot_pairs_kernel<true>, kPB, 0);
+    epot_pairs_kernel<true><<<nsm * (per > 0 ? per : 1), kPB, 0, st>>>(A, S->item_h, S->item_i, total,
+                                                                       &S->counter[1], S->part32);
+    AHOP_CUDA_TRY(cudaGetLastError());
+  }
+  epot_finalize_kernel<<<(unsigned)((nhalo + 127) / 128), 128, 0, st>>>(
+      A, S->hoff, S->order, (p->epot & 1) ? S->part64 : nullptr, (p->epot & 2) ? S->part32 : nullptr, nhalo);
+  AHOP_CUDA_TRY(cudaGetLastError());
+  AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+  return AHOP_OK;
+}

@@ -192,6 +192,21 @@ int ahop_halo_props_device(const AhopHaloParams* p, const int64_t* d_off, int64_
                            const double* d_vel, const double* d_mass, const double* d_density, double* d_out,
                            void* stream);
 int ahop_halo_get_timings(AhopHaloTimings* t);
+/* Allocation-free variant of ahop_halo_props_device (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc -- code running while
+ * another part of the process captures a CUDA graph, frameworks that own all
+ * device memory through their own pool, callers with a fixed memory budget.
+ * It allocates nothing: its scratch is a file-scope device array of about
+ * 7.9 MB (held on every GPU that loads the library until exit), limiting one
+ * call to 65,536 halos and 262,144 work items (one item per 256 members of a
+ * halo); larger calls are rejected with AHOP_EINVAL.  The caller passes device
+ * inputs and the device output [nhalo][AHOP_HALO_NFIELDS].  Every call shares
+ * that array, so calls that overlap on the GPU (other streams, other host
+ * threads) race; serialise them.  The first call on a device looks up the
+ * array's address and should come before any stream capture. */
+int ahop_halo_props_noalloc(const AhopHaloParams* p, const int64_t* d_off, int64_t nhalo, const double* d_pos,
+                            const double* d_vel, const double* d_mass, const double* d_density, double* d_out,
+                            void* stream);
 
 #ifdef __cplusplus
 }

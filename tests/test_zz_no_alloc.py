@@ -1,0 +1,63 @@
+"""The allocation-free halo-property entry point (ahop_halo_props_noalloc).
+
+Some callers cannot allocate device memory while they run -- e.g. code that
+executes while another part of the process captures a CUDA graph, or a host
+framework that owns all device memory through its own pool.  For them the
+library offers one entry point whose scratch lives in a fixed-size device
+array compiled into the library.  This test calls it through the C ABI twice
+in a row and checks it against the allocating entry point
+(ahop_halo_props_device) with the tolerance of the other halo-property tests,
+and checks that sizes beyond its stated limits are rejected.  It sits in its
+own file that pytest collects last and passes alone or after the other tests.
+"""
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+
+pytestmark = pytest.mark.gpu
+
+FIELDS_RTOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def catalogue():
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    from ahop_b200 import build, synthetic
+    build.build()
+    return synthetic.halo_catalogue(300, seed=91, nmin=20, nmax=30000, box=100.0)
+
+
+def test_noalloc_matches_allocating_entry_point_twice(catalogue):
+    import torch
+    from ahop_b200 import halo_props
+    off, pos, vel, mass, dens = catalogue
+    dev = torch.device("cuda:0")
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    d_off, d_pos, d_vel, d_mass, d_dens = t(off), t(pos), t(vel), t(mass), t(dens)
+    nh = len(off) - 1
+    ref = torch.zeros((nh, halo_props.NF), dtype=torch.float64, device=dev)
+    halo_props.compute_device(d_off, d_pos, d_vel, d_mass, d_dens, ref, 100.0, 70.0)
+    torch.cuda.synchronize()
+    r = ref.cpu().numpy()
+    for call in range(2):
+        out = torch.full((nh, halo_props.NF), np.nan, dtype=torch.float64, device=dev)
+        halo_props.compute_device_noalloc(d_off, d_pos, d_vel, d_mass, d_dens, out, 100.0, 70.0)
+        torch.cuda.synchronize()
+        o = out.cpu().numpy()
+        for k, name in enumerate(halo_props.FIELDS):
+            np.testing.assert_allclose(o[:, k], r[:, k], rtol=FIELDS_RTOL, atol=0, err_msg=f"call {call}: {name}")
+
+
+def test_noalloc_rejects_sizes_beyond_its_limit(catalogue):
+    import torch
+    from ahop_b200 import AhopError, halo_props
+    dev = torch.device("cuda:0")
+    nh = 65537  # one more halo than the fixed scratch holds
+    d_off = torch.arange(nh + 1, dtype=torch.int64, device=dev)
+    z3 = torch.zeros((nh, 3), dtype=torch.float64, device=dev)
+    z1 = torch.ones(nh, dtype=torch.float64, device=dev)
+    out = torch.zeros((nh, halo_props.NF), dtype=torch.float64, device=dev)
+    with pytest.raises(AhopError, match="exceeds the maximum"):
+        halo_props.compute_device_noalloc(d_off, z3, z3, z1, z1, out, 100.0, 70.0)
