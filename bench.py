@@ -136,6 +136,49 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def halo_section(args, torch):
+    """Batched direct-sum potential: FP32-compensated vs FP64 forms on the GPU.
+
+    Workload: 20,000 halos with member counts from dN/dn ~ n^-1.9 on
+    [20, 2e6] (seed 3), NFW positions (c=10) and Gaussian velocities in a
+    100-unit periodic box; pairs = sum n(n-1)/2.  Each form is timed alone
+    (CUDA events around its persistent pair kernel) over the same work list.
+    """
+    import numpy as np
+    from ahop_b200 import halo_props, synthetic
+    off, pos, vel, mass, dens = synthetic.halo_catalogue(args.nhalo, seed=3, nmin=20, nmax=2_000_000, box=100.0)
+    dev = torch.device("cuda")
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    d_off, d_pos, d_vel, d_mass, d_dens = t(off), t(pos), t(vel), t(mass), t(dens)
+    nh = len(off) - 1
+    out = torch.zeros((nh, halo_props.NF), dtype=torch.float64, device=dev)
+    st = torch.cuda.current_stream()
+    halo_props.compute_device(d_off, d_pos, d_vel, d_mass, d_dens, out, 100.0, 70.0, epot=3, stream=st)
+    o = out.cpu().numpy()
+    ep64, ep32 = o[:, halo_props.FIELDS.index("ep64")], o[:, halo_props.FIELDS.index("ep32c")]
+    ok = ep64 != 0
+    rel = float(np.max(np.abs(ep32[ok] - ep64[ok]) / np.abs(ep64[ok])))
+    t64, t32 = [], []
+    for _ in range(max(1, args.steps)):
+        halo_props.compute_device(d_off, d_pos, d_vel, d_mass, d_dens, out, 100.0, 70.0, epot=1, stream=st)
+        t64.append(halo_props.timings()["epot64"])
+        halo_props.compute_device(d_off, d_pos, d_vel, d_mass, d_dens, out, 100.0, 70.0, epot=2, stream=st)
+        t32.append(halo_props.timings()["epot32c"])
+    tm = halo_props.timings()
+    pairs = float(tm["pairs"])
+    m64, m32 = statistics.mean(t64), statistics.mean(t32)
+    nominal_fp32 = 148 * 128 * 2 * 1.965e9 / 1e12  # TFLOP/s, non-tensor FP32 at max clock
+    return {"workload": f"{nh} halos, {int(off[-1])} members, counts n^-1.9 on [20, 2e6], seed 3",
+            "pairs": pairs, "fp64_ms": m64, "fp32c_ms": m32,
+            "fp64_pairs_per_s": pairs / (m64 / 1e3), "fp32c_pairs_per_s": pairs / (m32 / 1e3),
+            "fp32c_over_fp64": m64 / m32, "max_rel_err_fp32c_vs_fp64": rel, "tolerance": 1e-6,
+            "roofline": {"bound": "fp32 cuda cores", "flop_per_pair": 20,
+                         "achieved": 20 * pairs / (m32 / 1e3) / 1e12, "peak": nominal_fp32, "unit": "TFLOP/s",
+                         "frac": 20 * pairs / (m32 / 1e3) / 1e12 / nominal_fp32,
+                         "peak_source": "nominal (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz)"},
+            "moments_ms": tm["moments"], "items": int(tm["items"])}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -144,6 +187,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--npart", type=int, default=0, help="override the workload size (testing)")
+    ap.add_argument("--no-halo", action="store_true", help="skip the batched halo E_pot section")
+    ap.add_argument("--nhalo", type=int, default=20000, help="halos in the E_pot section")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -242,18 +287,22 @@ def main():
     achieved = alg / (knn_avg / 1e3) / 1e9
     traffic = None
     try:
-        prof = json.load(open(os.path.join(REPO, "profiles", "knn_density_traffic.json")))
+        prof = json.load(open(os.path.join(REPO, "profiles", "knn_density_traffic.txt")))
         traffic = prof["dram_bytes_per_particle"] * n
     except Exception:
         pass
-    roof = {"kernel": "knn_density_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    roof = {"kernel": "knn_leaf_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "alg_bytes_per_launch": alg,
             "launch_ms": knn_avg, "peak_source": "measured" if peaks else "fallback"}
-    ts = (C.c_int64 * 8)()
-    lib.ahop_debug_tree_stats(ts, 8)
+    ts = (C.c_int64 * 13)()
+    lib.ahop_debug_tree_stats(ts, 13)
     tree_stats = {"structural_Mcycles": ts[0] / 1e6, "level_stats_Mcycles": ts[1] / 1e6,
                   "exact_Mcycles": ts[2] / 1e6, "levels": ts[3], "undecided_exact_passes": ts[4],
-                  "max_levels_one_task": ts[5], "max_Mcycles_one_task": ts[6] / 1e6}
+                  "max_levels_one_task": ts[5], "max_Mcycles_one_task": ts[6] / 1e6,
+                  "structural_passes": ts[7]}
+    nql = max(1, ts[8])
+    knn_stats = {"query_leaves": ts[8], "cand_leaves_per_query_leaf": ts[9] / nql,
+                 "leaf_visits_per_query": ts[10] / n, "insertions_per_query": ts[11] / n, "overflow_leaves": ts[12]}
     mean_stage = {k: statistics.mean(s[k] for s in stage) for k in
                   ("tree", "knn_density", "hop_groups", "saddles", "nodes", "membership", "total")}
     line = {"metric": METRIC, "value": value, "unit": "Mpart/s", "n_gpus": world, "steps": args.steps,
@@ -266,7 +315,9 @@ def main():
             "roofline": roof, "stages_ms": mean_stage,
             "gpu_launches": int(stage[-1]["kernel_launches"]) * args.steps,
             "cub_calls_per_step": int(stage[-1]["cub_calls"]), "tree_waves": int(stage[-1]["tree_waves"]),
-            "nnodes": nnodes, "tree_stats": tree_stats, "clocks": clk.summary()}
+            "nnodes": nnodes, "tree_stats": tree_stats, "knn_stats": knn_stats, "clocks": clk.summary()}
+    if not args.no_halo:
+        line["halo_epot"] = halo_section(args, torch)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, dt, nth, _ = cpu_sample_rate()
         line["cpu_baseline"] = {"value": rate, "unit": "Mpart/s", "cores": nth, "kind": "port",

@@ -39,7 +39,8 @@ class AhopOutputs(C.Structure):
 
 class AhopTimings(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("upload", "tree", "knn_density", "hop_groups", "saddles", "nodes",
-                                         "membership", "download", "total", "knn_kernel")] + [
+                                         "membership", "download", "total", "knn_kernel", "nodes_prep",
+                                         "nodes_root", "nodes_waves", "nodes_order")] + [
         (n, C.c_int32) for n in ("kernel_launches", "cub_calls", "tree_waves", "hop_passes")]
 
 

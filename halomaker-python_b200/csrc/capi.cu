@@ -116,6 +116,10 @@ static void fill_timings(Engine& E, bool host) {
   t.download = host ? el(7, 8) : 0.f;
   t.total = host ? el(0, 8) : el(1, 7);
   t.knn_kernel = el(9, 10);
+  t.nodes_prep = el(5, 11);
+  t.nodes_root = el(11, 12);
+  t.nodes_waves = el(12, 13);
+  t.nodes_order = el(13, 6);
   t.kernel_launches = E.launches;
   t.cub_calls = E.cub_calls;
   t.tree_waves = E.waves;
@@ -330,6 +334,7 @@ int ahop_debug_compute_stages(const double* pos_in, const double* mass_in, int64
 int ahop_debug_tree_stats(int64_t* out, int32_t n) {
   Engine& E = engine();
   for (int i = 0; i < n && i < 8; ++i) out[i] = (int64_t)E.tree_stats[i];
+  for (int i = 8; i < n && i < 13; ++i) out[i] = (int64_t)E.knn_stats[i - 8];
   return AHOP_OK;
 }
 

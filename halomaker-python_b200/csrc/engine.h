@@ -80,9 +80,10 @@ struct Engine {
   Params prm;
   int device = -1;
   cudaStream_t stream = nullptr;  // stream of the current call
-  cudaEvent_t ev[12] = {};
+  cudaEvent_t ev[16] = {};
   int32_t launches = 0, cub_calls = 0, waves = 0, hop_passes = 0;  // counters of the current compute
   unsigned long long tree_stats[8] = {};                             // structure-tree kernel counters
+  unsigned long long knn_stats[5] = {};                              // kNN kernel counters
   bool events_ready = false;
   AhopTimings timings{};
 

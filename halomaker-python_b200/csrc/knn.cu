@@ -207,6 +207,7 @@ struct KnnArgs {
   int32_t* nei; // [n][nstore] sorted-slot ids
   double* dens; // [n]
   int* err;     // error flag (stack overflow)
+  unsigned long long* kstats;  // [0] query leaves [1] candidate leaves [2] leaf visits [3] insertions [4] overflows
 };
 
 constexpr int kWarpsPerBlock = 8;
@@ -229,7 +230,8 @@ struct WarpList {
 };
 
 __device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int64_t leaf, int64_t self, double qx,
-                                            double qy, double qz, int lane) {
+                                            double qy, double qz, int lane, unsigned& nvis, unsigned& nins) {
+  ++nvis;
   int64_t p = leaf * kLeaf + lane;
   bool v = (p < A.n) && (p != self);
   double d = CUDART_INF;
@@ -243,6 +245,7 @@ __device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int64
   int32_t lastk = __shfl_sync(0xffffffffu, L.lo, A.nv - 1);
   unsigned mask = __ballot_sync(0xffffffffu, v && (d < L.r2 || (d == L.r2 && o < lastk)));
   while (mask) {
+    ++nins;
     int src = __ffs(mask) - 1;
     double cd = __shfl_sync(0xffffffffu, d, src);
     int32_t co = __shfl_sync(0xffffffffu, o, src);
@@ -266,7 +269,7 @@ __device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int64
 // when a query leaf's candidate list overflows).  Leaves skip0/skip1 were
 // already scanned.
 __device__ void query_dfs(const KnnArgs& A, WarpList& L, int64_t s, double qx, double qy, double qz, int lane,
-                          int32_t* s_node, double* s_bd, int64_t skip0, int64_t skip1) {
+                          int32_t* s_node, double* s_bd, int64_t skip0, int64_t skip1, unsigned& nvis, unsigned& nins) {
   const int top = A.nlev - 1;
   int sp = 0;
   if (lane == 0) { s_node[0] = (top << 27) | 0; s_bd[0] = 0.0; }
@@ -282,7 +285,7 @@ __device__ void query_dfs(const KnnArgs& A, WarpList& L, int64_t s, double qx, d
     const int64_t j = ent & ((1 << 27) - 1);
     if (lvl == 0) {
       if (j == skip0 || j == skip1) continue;
-      leaf_insert(A, L, j, s, qx, qy, qz, lane);
+      leaf_insert(A, L, j, s, qx, qy, qz, lane, nvis, nins);
       continue;
     }
     const int64_t c = j * kFan + lane;
@@ -461,15 +464,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) knn_leaf_kernel(KnnArgs A
       __syncwarp();
     }
     // ---- C: per-query kNN over the candidates
+    unsigned nvis = 0, nins = 0;
     for (int q = 0; q < nq; ++q) {
       const int64_t s = s0 + q;
       const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
       WarpList L;
       L.ld = CUDART_INF; L.ls = -1; L.lo = INT_MAX; L.r2 = CUDART_INF;
-      leaf_insert(A, L, jl, s, qx, qy, qz, lane);
-      if (jn >= 0 && jn != jl) leaf_insert(A, L, jn, s, qx, qy, qz, lane);
+      leaf_insert(A, L, jl, s, qx, qy, qz, lane, nvis, nins);
+      if (jn >= 0 && jn != jl) leaf_insert(A, L, jn, s, qx, qy, qz, lane, nvis, nins);
       if (overflow) {
-        query_dfs(A, L, s, qx, qy, qz, lane, s_node[wib], s_bd[wib], jl, jn);
+        query_dfs(A, L, s, qx, qy, qz, lane, s_node[wib], s_bd[wib], jl, jn, nvis, nins);
       } else {
         for (int c0 = 0; c0 < ncand; c0 += 32) {
           const int ci = c0 + lane;
@@ -485,12 +489,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) knn_leaf_kernel(KnnArgs A
             mask &= mask - 1;
             const double sbd = __shfl_sync(0xffffffffu, bd, src);
             const int64_t sl = __shfl_sync(0xffffffffu, leaf, src);
-            if (sbd < L.r2) leaf_insert(A, L, sl, s, qx, qy, qz, lane);
+            if (sbd < L.r2) leaf_insert(A, L, sl, s, qx, qy, qz, lane, nvis, nins);
           }
         }
       }
       finish_query(A, L, s, lane);
       __syncwarp();
+    }
+    if (lane == 0 && A.kstats) {
+      atomicAdd(&A.kstats[0], 1ULL);
+      atomicAdd(&A.kstats[1], (unsigned long long)ncand);
+      atomicAdd(&A.kstats[2], (unsigned long long)nvis);
+      atomicAdd(&A.kstats[3], (unsigned long long)nins);
+      if (overflow) atomicAdd(&A.kstats[4], 1ULL);
     }
   }
 }
@@ -515,9 +526,10 @@ int stage_knn_density(Engine& E) {
   A.nstore = E.nstore;
   A.nei = E.d_nei.as<int32_t>();
   A.dens = E.d_dens.as<double>();
-  AHOP_CUDA_TRY(E.d_flags.ensure(64));
-  AHOP_CUDA_TRY(cudaMemsetAsync(E.d_flags.p, 0, 64, E.stream));
+  AHOP_CUDA_TRY(E.d_flags.ensure(256));
+  AHOP_CUDA_TRY(cudaMemsetAsync(E.d_flags.p, 0, 256, E.stream));
   A.err = E.d_flags.as<int>();
+  A.kstats = reinterpret_cast<unsigned long long*>(E.d_flags.as<char>() + 64);
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, E.device);
   int per_sm = 0;
@@ -533,6 +545,7 @@ int stage_knn_density(Engine& E) {
   AHOP_CUDA_TRY(cudaGetLastError());
   int herr = 0;
   AHOP_CUDA_TRY(cudaMemcpyAsync(&herr, E.d_flags.p, 4, cudaMemcpyDeviceToHost, E.stream));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(E.knn_stats, E.d_flags.as<char>() + 64, 5 * 8, cudaMemcpyDeviceToHost, E.stream));
   AHOP_CUDA_TRY(cudaStreamSynchronize(E.stream));
   if (herr) { set_error("kNN traversal stack overflow"); return AHOP_ELIMIT; }
   return AHOP_OK;

@@ -90,6 +90,7 @@ struct TreeArgs {
   double* gs;             // [ng][8] per-position scratch sums
   double* cs;             // [ng][12] per-component scratch
   int32_t* deepnode;      // [ng+1]
+  int32_t* gcur;          // [ng+1] members above the group's last threshold
   NodeRec* node;          // [nnodesmax+1]
   int32_t nnodesmax;
   int32_t* nnodes;        // counter
@@ -110,14 +111,30 @@ __device__ __forceinline__ double wrapd(double d, double L, double h) {
   return d;
 }
 
-// number of members of group g with density > rhot (members sorted by decreasing density)
+// number of members of group g with density > rhot (members sorted by
+// decreasing density).  A group's threshold only rises (a task's rhot grows
+// and children start above their parent), so the count is searched downward
+// from the group's previous count: a galloping step then a binary search.
 __device__ __forceinline__ int32_t count_above(const TreeArgs& A, int32_t g, double rhot) {
-  int32_t lo = A.goff[g], hi = A.goff[g + 1];  // find first index with rdesc <= rhot
-  while (lo < hi) {
-    int32_t mid = (lo + hi) >> 1;
-    if (A.rdesc[mid] > rhot) lo = mid + 1; else hi = mid;
+  const double* r = A.rdesc + A.goff[g];
+  const int32_t hi = A.gcur[g];  // members [0, hi) were above the group's previous threshold
+  if (hi == 0 || r[hi - 1] > rhot) return hi;
+  // r[j] <= rhot; gallop down until an index above rhot (or 0) brackets the answer
+  int32_t j = hi - 1, lo = 0, step = 1;
+  while (true) {
+    const int32_t k = j - step;
+    if (k < 0) { lo = 0; break; }
+    if (r[k] > rhot) { lo = k + 1; break; }
+    j = k;
+    step <<= 1;
   }
-  return lo - A.goff[g];
+  int32_t a2 = lo, b2 = j;  // first index with r <= rhot lies in [lo, j]
+  while (a2 < b2) {
+    const int32_t mid = (a2 + b2) >> 1;
+    if (r[mid] > rhot) a2 = mid + 1; else b2 = mid;
+  }
+  A.gcur[g] = a2;
+  return a2;
 }
 
 __device__ int32_t uf_find(int32_t* par, int32_t i) {
@@ -463,22 +480,37 @@ __device__ void group_sums_warp(const TreeArgs& A, int32_t g, double rhot, doubl
 #pragma unroll
     for (int c = 0; c < 6; ++c) st[lane * 6 + c] = t[c];
     __syncwarp();
-    if (lane == 0) {
+    // lanes 0..5 each run one of the six sequential sums, lane 6 the count:
+    // the same additions in the same order as a single thread would do
+    if (lane < 7) {
       const int cnt = min(32, q1 - base);
+      double acc = (lane == 0) ? tm : (lane == 1) ? px : (lane == 2) ? py : (lane == 3) ? pz : (lane == 4) ? rs : dm;
+      const int col = (lane == 0) ? 0 : (lane == 1) ? 1 : (lane == 2) ? 2 : (lane == 3) ? 3 : (lane == 4) ? 4 : 5;
+      int cntg = 0;
       for (int l = 0; l < cnt; ++l) {
         const double* u = st + l * 6;
         if (u[5] < 0.0) continue;
-        imass += 1;
-        tm = xadd(tm, u[0]);
-        px = xadd(px, u[1]);
-        py = xadd(py, u[2]);
-        pz = xadd(pz, u[3]);
-        rs = xadd(rs, u[4]);
-        dm = xadd(dm, u[5]);
+        ++cntg;
+        if (lane < 6) acc = xadd(acc, u[col]);
       }
+      if (lane == 0) tm = acc;
+      else if (lane == 1) px = acc;
+      else if (lane == 2) py = acc;
+      else if (lane == 3) pz = acc;
+      else if (lane == 4) rs = acc;
+      else if (lane == 5) dm = acc;
+      else imass += cntg;
     }
     __syncwarp();
   }
+  // gather the seven chains to lane 0
+  tm = __shfl_sync(0xffffffffu, tm, 0);
+  px = __shfl_sync(0xffffffffu, px, 1);
+  py = __shfl_sync(0xffffffffu, py, 2);
+  pz = __shfl_sync(0xffffffffu, pz, 3);
+  rs = __shfl_sync(0xffffffffu, rs, 4);
+  dm = __shfl_sync(0xffffffffu, dm, 5);
+  imass = __shfl_sync(0xffffffffu, imass, 6);
   if (lane == 0) { G[0] = (double)imass; G[1] = tm; G[2] = px; G[3] = py; G[4] = pz; G[5] = rs; G[6] = dm; }
 }
 
@@ -689,7 +721,10 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
     const bool restructure = T.rhot >= T.next_event;
     __syncthreads();
     long long c0 = clock64();
-    if (restructure) structural_pass<SortT, ScanT, MaxScanT>(A, T, sort_tmp, scan_tmp, maxscan_tmp, s_keys);
+    if (restructure) {
+      structural_pass<SortT, ScanT, MaxScanT>(A, T, sort_tmp, scan_tmp, maxscan_tmp, s_keys);
+      if (tid == 0) atomicAdd(&A.stats[7], 1ULL);
+    }
     long long c1 = clock64();
     if (tid == 0) { s_clk[0] += c1 - c0; s_clk[3] += 1; }
     if (T.nsurv == 0) {  // all groups below the threshold (f90:1348-1351 prints, then ends with no colour)
@@ -827,11 +862,13 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
 }
 
 // ------------------------------------------------------- setup / membership / order
-__global__ void init_groups_kernel(int32_t ng, int32_t* GL, int32_t* pos_of, int32_t* deepnode) {
+__global__ void init_groups_kernel(int32_t ng, int32_t* GL, int32_t* pos_of, int32_t* deepnode, int32_t* gcur,
+                                   const int32_t* goff) {
   int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < ng) {
     GL[i] = i + 1;
     pos_of[i + 1] = i;
+    gcur[i + 1] = goff[i + 2] - goff[i + 1];
   }
   if (i <= ng) deepnode[i] = 0;
 }
@@ -964,6 +1001,7 @@ int stage_nodes(Engine& E) {
   const int T = 256;
   AHOP_CUDA_TRY(E.d_liste.ensure(n * 4));
   E.nnodes = 0;
+  for (int k = 11; k <= 13; ++k) AHOP_CUDA_TRY(cudaEventRecord(E.ev[k], st));
   if (ng == 0) {
     AHOP_CUDA_TRY(cudaMemsetAsync(E.d_liste.p, 0, n * 4, st));
     return AHOP_OK;
@@ -1000,12 +1038,13 @@ int stage_nodes(Engine& E) {
         P.ylongs2, P.zlongs2, E.d_gmem_rho_pref.as<double>());
     AHOP_CUDA_TRY(cudaGetLastError());
   }
+  AHOP_CUDA_TRY(cudaEventRecord(E.ev[11], st));
   // ---- tree scratch
   const size_t G = (size_t)ng + 1;
   const size_t bytes_i = G * 4;
   // every sub-array starts on a 256-byte boundary: size the buffer with the rounding
   auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
-  const size_t need = r256(bytes_i) * 10 + r256(G * 8 * 8) + r256(G * 12 * 8) +
+  const size_t need = r256(bytes_i) * 11 + r256(G * 8 * 8) + r256(G * 12 * 8) +
                       r256((size_t)(nnodesmax + 1) * sizeof(Task)) * 2;
   AHOP_CUDA_TRY(E.d_tree_scratch.ensure(need));
   char* p = static_cast<char*>(E.d_tree_scratch.p);
@@ -1021,6 +1060,7 @@ int stage_nodes(Engine& E) {
   A.compidx = reinterpret_cast<int32_t*>(take(bytes_i));
   A.gn = reinterpret_cast<int32_t*>(take(bytes_i));
   A.deepnode = reinterpret_cast<int32_t*>(take(bytes_i));
+  A.gcur = reinterpret_cast<int32_t*>(take(bytes_i));
   A.gs = reinterpret_cast<double*>(take(G * 8 * 8));
   A.cs = reinterpret_cast<double*>(take(G * 12 * 8));
   Task* tasks[2];
@@ -1053,7 +1093,7 @@ int stage_nodes(Engine& E) {
   A.node = E.d_nodes.as<NodeRec>();
   A.nnodesmax = nnodesmax;
   E.launches++;
-  init_groups_kernel<<<(unsigned)((ng + 1 + T - 1) / T), T, 0, st>>>(ng, A.GL, A.pos_of, A.deepnode);
+  init_groups_kernel<<<(unsigned)((ng + 1 + T - 1) / T), T, 0, st>>>(ng, A.GL, A.pos_of, A.deepnode, A.gcur, A.goff);
   AHOP_CUDA_TRY(cudaGetLastError());
   // root node 0 (f90:934-943): mass and truemass stay 0, densmax = max peak density
   {
@@ -1126,10 +1166,11 @@ int stage_nodes(Engine& E) {
       // zero or one significant colour: the root task continues (f90:1577-1626)
       // on the general path from the initial group order
       E.launches++;
-      init_groups_kernel<<<(unsigned)((ng + 1 + T - 1) / T), T, 0, st>>>(ng, A.GL, A.pos_of, A.deepnode);
+      init_groups_kernel<<<(unsigned)((ng + 1 + T - 1) / T), T, 0, st>>>(ng, A.GL, A.pos_of, A.deepnode, A.gcur, A.goff);
       AHOP_CUDA_TRY(cudaGetLastError());
     }
   }
+  AHOP_CUDA_TRY(cudaEventRecord(E.ev[12], st));
   for (int wave = 0; ntasks > 0; ++wave) {
     if (wave > 100000) { set_error("structure tree: too many waves"); return AHOP_ELIMIT; }
     A.next = tasks[cur ^ 1];
@@ -1148,6 +1189,7 @@ int stage_nodes(Engine& E) {
     cur ^= 1;
     E.waves = wave + 1;
   }
+  AHOP_CUDA_TRY(cudaEventRecord(E.ev[13], st));
   const int32_t nn = h[2];
   E.nnodes = nn;
   // ---- membership (f90:1297-1306 paint order => deepest node above rho_saddle)

@@ -73,6 +73,9 @@ typedef struct {
 typedef struct {
   float upload, tree, knn_density, hop_groups, saddles, nodes, membership, download, total;
   float knn_kernel; /* the fused kNN + density kernel alone */
+  /* parts of `nodes`: per-group density-sorted members and running sums,
+   * root level, task waves, membership + renumbering + tables */
+  float nodes_prep, nodes_root, nodes_waves, nodes_order;
   int32_t kernel_launches, cub_calls, tree_waves, hop_passes;
 } AhopTimings;
 
@@ -126,10 +129,12 @@ int ahop_debug_saddles(int32_t* nconn, int32_t* offsets, int32_t* isad, double* 
  * 3 = hop + groups, 4 = saddles, 5 = everything) for stage-wise parity tests;
  * the stage views above then describe that partial run. */
 int ahop_debug_compute_stages(const double* pos_in, const double* mass_in, int64_t npart, int32_t last_stage);
-/* Structure-tree kernel counters of the last compute: cycles in structural
- * passes, in per-level statistics and in exact recomputation (summed over
- * blocks), threshold levels, exact passes for undecided tests, the largest
- * number of levels of one task and the largest cycle count of one task. */
+/* Kernel counters of the last compute: [0..7] structure tree -- cycles in
+ * structural passes, in per-level statistics and in exact recomputation
+ * (summed over blocks), threshold levels, exact passes for undecided tests,
+ * the largest number of levels of one task, the largest cycle count of one
+ * task, structural passes; [8..12] kNN -- query leaves, candidate leaves,
+ * leaf visits, list insertions, leaves that fell back to per-query search. */
 int ahop_debug_tree_stats(int64_t* out, int32_t n);
 /* Ask compute to keep the first k neighbours per particle (default nhop). */
 int ahop_debug_set_store_neighbours(int32_t k);
@@ -207,6 +212,30 @@ int ahop_halo_get_timings(AhopHaloTimings* t);
 int ahop_halo_props_noalloc(const AhopHaloParams* p, const int64_t* d_off, int64_t nhalo, const double* d_pos,
                             const double* d_vel, const double* d_mass, const double* d_density, double* d_out,
                             void* stream);
+
+/* ---- differentiation -----------------------------------------------------------
+ * SPH density with FIXED neighbour lists (nei[n][nvoisins], 0-based particle
+ * indices sorted by distance at the lists' reference configuration) and its
+ * adjoint with respect to positions; the gradient of each halo's direct-sum
+ * potential.  The density forward is omp_compute_density (f90:2816-2838)
+ * with the same rounding, so with the finder's own lists it reproduces the
+ * finder's densities bit for bit; the potential is det_halo_energies_1b3's
+ * direct sum (CHP:1413-1427).  All pointers are device memory; gpos is
+ * accumulated into (zero it first). */
+typedef struct {
+  int32_t nvoisins, pad;
+  double xlong, ylong, zlong;
+} AhopAdjParams;
+int ahop_density_fixed(const AhopAdjParams* p, const double* d_pos, const double* d_mass, const int32_t* d_nei,
+                       int64_t n, double* d_dens, void* stream);
+int ahop_density_adjoint(const AhopAdjParams* p, const double* d_pos, const double* d_mass, const int32_t* d_nei,
+                         int64_t n, const double* d_gdens, double* d_gpos, void* stream);
+/* dE_h/dx scaled by gh[h], accumulated into gpos; centre[h] = index (within
+ * the halo) of the densest member, the origin of the min-image separations;
+ * h_off is the host copy of d_off. */
+int ahop_epot_grad(const AhopHaloParams* p, const int64_t* d_off, const int64_t* h_off, int64_t nhalo,
+                   const double* d_pos, const double* d_mass, const int32_t* d_centre, const double* d_gh,
+                   double* d_gpos, void* stream);
 
 #ifdef __cplusplus
 }
