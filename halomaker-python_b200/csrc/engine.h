@@ -82,7 +82,7 @@ struct Engine {
   cudaStream_t stream = nullptr;  // stream of the current call
   cudaEvent_t ev[16] = {};
   int32_t launches = 0, cub_calls = 0, waves = 0, hop_passes = 0;  // counters of the current compute
-  unsigned long long tree_stats[8] = {};                             // structure-tree kernel counters
+  unsigned long long tree_stats[11] = {};                             // structure-tree kernel counters
   unsigned long long knn_stats[5] = {};                              // kNN kernel counters
   bool events_ready = false;
   AhopTimings timings{};
@@ -90,6 +90,7 @@ struct Engine {
   int64_t n = 0;          // particles in the current run
   int32_t nstore = 16;    // neighbours stored per particle
   int32_t req_store = 0;  // requested via debug API (0 = nhop)
+  bool task_profile = false;  // per-task structure-tree profile (debug API)
   bool have_result = false;
 
   // inputs / sorted particle arrays
@@ -126,6 +127,10 @@ struct Engine {
   // nodes
   DevBuf d_nodes;                        // NodeRec[nnodesmax+1]
   DevBuf d_tree_scratch;
+  DevBuf d_tprof;                        // per-task profile rows (debug)
+  DevBuf d_pairs;                        // (node, group) pair keys, sort double buffer
+  DevBuf d_pair_sums;                    // [npairs][8] per-pair sums
+  DevBuf d_node_aux;                     // per node: pair range, posref
   int32_t nnodes = 0;
   DevBuf d_liste;                        // [n] node id per ORIG particle (1-based), 0 none
   DevBuf d_dens_orig;                    // [n] density in ORIG order

@@ -97,7 +97,8 @@ struct TreeArgs {
   Task* next;
   int32_t* nnext;
   int32_t* err;           // [0] code, [1] detail
-  unsigned long long* stats;  // [8] per-stage counters (see the end of tree_wave_kernel)
+  unsigned long long* stats;  // [11] counters (see the end of tree_wave_kernel; [8..10] undecided tests)
+  long long* tprof;       // [nnodesmax+1][16] per-task profile row by node id, or null
 };
 
 __device__ __forceinline__ void set_err(const TreeArgs& A, int code, int detail) {
@@ -175,7 +176,7 @@ __device__ __forceinline__ double atomic_min_pos(double* addr, double v) {
 struct SharedTask {
   double rhot;
   double next_event;
-  int32_t inode, a, b, level, ncomp, nsurv, nsisters, done, nexact, inode1;
+  int32_t inode, a, b, level, ncomp, nsurv, nsisters, done, nexact, inode1, kk;
   int32_t flag;
   long long iters;
 };
@@ -183,10 +184,15 @@ struct SharedTask {
 template <class SortT, class ScanT, class MaxScanT>
 __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT::TempStorage& sort_tmp,
                                 typename ScanT::TempStorage& scan_tmp, typename MaxScanT::TempStorage& maxscan_tmp,
-                                int32_t* s_keys) {
+                                int32_t* s_keys, long long* ph) {
   const int tid = threadIdx.x;
   const int32_t a = T.a, b = T.b;
   const double rhot = T.rhot;
+  long long tl = clock64();
+  // thread 0 charges the cycles since the last mark to phase k
+  auto mark = [&](int k) {
+    if (tid == 0) { const long long t = clock64(); ph[k] += t - tl; tl = t; }
+  };
   if (tid == 0) T.next_event = DBL_MAX;
   for (int32_t i = a + tid; i < b; i += kNT) {
     A.par[i] = i;
@@ -194,23 +200,30 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
     A.run[i] = 0;
   }
   __syncthreads();
-  // union over saddle edges above rhot (rows sorted by decreasing saddle)
+  mark(0);
+  // union over saddle edges above rhot (rows sorted by decreasing saddle);
+  // the next event is the smallest peak density or saddle still above rhot
+  double ev = DBL_MAX;
   for (int32_t i = a + tid; i < b; i += kNT) {
     int32_t g = A.GL[i];
     double dg = A.densg[g];
     if (!(dg > rhot)) continue;
-    atomic_min_pos(&T.next_event, dg);
+    ev = fmin(ev, dg);
     int32_t e0 = A.soff[g - 1], e1 = A.soff[g];
     for (int32_t e = e0; e < e1; ++e) {
       double r = A.srho[e];
       if (!(r > rhot)) break;
-      atomic_min_pos(&T.next_event, r);
+      ev = fmin(ev, r);
       int32_t j = A.pos_of[A.sisad[e]];
       if (j < a || j >= b) { set_err(A, 11, g); continue; }  // f90:1229-1233
       uf_union(A.par, i, j);
     }
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) ev = fmin(ev, __shfl_xor_sync(0xffffffffu, ev, o));
+  if ((tid & 31) == 0 && ev < DBL_MAX) atomic_min_pos(&T.next_event, ev);
   __syncthreads();
+  mark(1);
   for (int32_t i = a + tid; i < b; i += kNT) {
     int32_t g = A.GL[i];
     if (A.densg[g] > rhot) {
@@ -222,6 +235,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
     }
   }
   __syncthreads();
+  mark(2);
   // exclusive scan of component sizes over root positions -> component offsets (in cnt)
   int32_t carry = 0;
   for (int32_t c0 = a; c0 < b; c0 += kNT) {
@@ -235,19 +249,22 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
     __syncthreads();
   }
   const int32_t nsurv = carry;
+  mark(3);
   // stable reorder by root, chunk by chunk: inside a chunk a stable block
   // radix sort groups equal roots; a run's rank is its offset from the run
   // head (block max-scan of head indices); run[] carries ranks across chunks
+  const int32_t sent = b - a;  // key of dropped groups, above every root offset
+  const int kbits = 32 - __clz(sent);
   for (int32_t c0 = a; c0 < b; c0 += kChunk) {
     int32_t keys[kIPT], vals[kIPT];
 #pragma unroll
     for (int k = 0; k < kIPT; ++k) {
       int32_t i = c0 + tid * kIPT + k;
       int32_t r = (i < b) ? A.par[i] : -1;
-      keys[k] = (r >= 0) ? (r - a) : INT_MAX;
+      keys[k] = (r >= 0) ? (r - a) : sent;
       vals[k] = i;
     }
-    SortT(sort_tmp).Sort(keys, vals);
+    SortT(sort_tmp).Sort(keys, vals, 0, kbits);
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < kIPT; ++k) s_keys[tid * kIPT + k] = keys[k];
@@ -264,7 +281,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
     for (int k = 0; k < kIPT; ++k) {
       int q = tid * kIPT + k;
       tail[k] = (q == kChunk - 1) || (s_keys[q + 1] != keys[k]);
-      if (keys[k] == INT_MAX) continue;
+      if (keys[k] == sent) continue;
       int32_t r = keys[k] + a;
       int32_t np = a + A.cnt[r] + A.run[r] + (q - headq[k]);
       if (np < a || np >= b) { set_err(A, 17, np); continue; }
@@ -274,10 +291,11 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
 #pragma unroll
     for (int k = 0; k < kIPT; ++k) {
       int q = tid * kIPT + k;
-      if (tail[k] && keys[k] != INT_MAX) A.run[keys[k] + a] += q - headq[k] + 1;
+      if (tail[k] && keys[k] != sent) A.run[keys[k] + a] += q - headq[k] + 1;
     }
     __syncthreads();
   }
+  mark(4);
   // copy back, positions, component starts
   for (int32_t i = a + tid; i < a + nsurv; i += kNT) {
     int32_t g = A.GL2[i];
@@ -285,6 +303,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
     A.pos_of[g] = i;
   }
   __syncthreads();
+  mark(5);
   // component starts: root positions r (par[r] == r before reorder) map to start a + cnt[r]
   // collect them in order with a scan over root flags
   carry = 0;
@@ -298,17 +317,31 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
     carry += tot;
     __syncthreads();
   }
+  const int32_t ncomp = carry;
+  mark(6);
   if (tid == 0) {
-    T.ncomp = carry;
+    T.ncomp = ncomp;
     T.nsurv = nsurv;
     T.b = a + nsurv;
   }
+  // component index of every surviving position: inclusive scan of the
+  // component-start flags (run[] is free after the reorder)
+  for (int32_t i = a + tid; i < a + nsurv; i += kNT) A.run[i] = 0;
   __syncthreads();
-  for (int32_t k = tid; k < T.ncomp; k += kNT) {
-    const int32_t c1 = (k + 1 < T.ncomp) ? A.cstart[a + k + 1] : T.b;
-    for (int32_t i = A.cstart[a + k]; i < c1; ++i) A.compidx[i] = k;
+  for (int32_t k = tid; k < ncomp; k += kNT) A.run[A.cstart[a + k]] = 1;
+  __syncthreads();
+  carry = 0;
+  for (int32_t c0 = a; c0 < a + nsurv; c0 += kNT) {
+    const int32_t i = c0 + tid;
+    const int32_t v = (i < a + nsurv) ? A.run[i] : 0;
+    int32_t inc, tot;
+    ScanT(scan_tmp).InclusiveSum(v, inc, tot);
+    __syncthreads();
+    if (i < a + nsurv) A.compidx[i] = carry + inc - 1;
+    carry += tot;
   }
   __syncthreads();
+  mark(7);
 }
 
 __device__ __forceinline__ int32_t comp_end(const TreeArgs& A, const SharedTask& T, int32_t k) {
@@ -318,8 +351,9 @@ __device__ __forceinline__ int32_t comp_end(const TreeArgs& A, const SharedTask&
 // -------------------------------------------------------------------------
 // Per-component quantities.  cs row (12 doubles) for component k at index a+k:
 //  0 mass_loc  1 mass_comp  2 densmax  3 sum rho  4 M  5 Sx 6 Sy 7 Sz 8 Q
-//  9 decision (0 false, 1 true, 2 unknown)  10 exact flag  11 unused
-// Exact per-component results overwrite 0..3 and set 9 to 0/1.
+//  9 decision (0 false, 1 true, 2 unknown)  10 exact flag  11 posref
+// (9..11 hold the component's anchor while its groups' terms are formed).
+// An exact recomputation overwrites 0..9 (colour_fold).
 
 __device__ __forceinline__ int tri_and(int p, int q) {
   if (p == 0 || q == 0) return 0;
@@ -338,84 +372,133 @@ __device__ __forceinline__ int tri_gt(double v, double t, double e) {
   return 2;
 }
 
-__device__ void approx_stats(const TreeArgs& A, SharedTask& T) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const double rhot = T.rhot;
+// Approximate terms of the group at position i for its component's anchor
+// (a: x, y, z of the peak of the component's first group).  gs row:
+// 0 densg, 1 sum rho, 2 mass, 3..5 first moments about the anchor, 6 second
+// moment, 7 tri-state test "mean density of the group above rhot";
+// gn[i] = members above rhot (exact).
+__device__ __forceinline__ void position_terms(const TreeArgs& A, int32_t i, double rhot, const double* a) {
   const double u = 1.1102230246251565e-16;
-  for (int32_t k = warp; k < T.ncomp; k += kNT / 32) {
-    const int32_t c0 = A.cstart[T.a + k], c1 = comp_end(A, T, k);
-    const int32_t g0 = A.GL[c0];
-    const int32_t p0 = A.gpeak[g0];
-    const double ax = A.x[p0], ay = A.y[p0], az = A.z[p0];
-    long long nl = 0;
-    int32_t nmax = 0;
-    double dmax = -1.0, S = 0, M = 0, Sx = 0, Sy = 0, Sz = 0, Q = 0;
-    int triB = 0;  // densmoy_comp_max > rhot
-    for (int32_t i = c0 + lane; i < c1; i += 32) {
-      const int32_t g = A.GL[i];
-      const int32_t ng = count_above(A, g, rhot);
-      A.gn[i] = ng;
-      nl += ng;
-      nmax = max(nmax, ng);
-      dmax = fmax(dmax, A.densg[g]);
-      if (ng > 0) {
-        const double* P = A.pref + 6 * (size_t)(A.goff[g] + ng - 1);
-        const double sg = P[0];
-        S += sg;
-        const int32_t pg = A.gpeak[g];
-        double dx = wrapd(A.x[pg] - ax, A.Lx, A.hx), dy = wrapd(A.y[pg] - ay, A.Ly, A.hy),
-               dz = wrapd(A.z[pg] - az, A.Lz, A.hz);
-        const double mg = P[1];
-        M += mg;
-        Sx += P[2] + mg * dx;
-        Sy += P[3] + mg * dy;
-        Sz += P[4] + mg * dz;
-        Q += P[5] + 2.0 * (dx * P[2] + dy * P[3] + dz * P[4]) + mg * (dx * dx + dy * dy + dz * dz);
-        const double dn = (double)ng;
-        const double vg = (sg / dn) / (1.0 + A.fudge / sqrt(dn));
-        triB = tri_or(triB, tri_gt(vg, rhot, (2.0 * dn + 8.0) * u * fabs(vg) * 1.01));
-      }
-    }
-    // warp reductions
+  const int32_t g = A.GL[i];
+  const int32_t ng = count_above(A, g, rhot);
+  double* G = A.gs + 8 * (size_t)i;
+  A.gn[i] = ng;
+  double t[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (ng > 0) {
+    const double* P = A.pref + 6 * (size_t)(A.goff[g] + ng - 1);
+    const int32_t pg = A.gpeak[g];
+    const double dx = wrapd(A.x[pg] - a[0], A.Lx, A.hx), dy = wrapd(A.y[pg] - a[1], A.Ly, A.hy),
+                 dz = wrapd(A.z[pg] - a[2], A.Lz, A.hz);
+    const double sg = P[0], mg = P[1];
+    t[0] = sg;
+    t[1] = mg;
+    t[2] = P[2] + mg * dx;
+    t[3] = P[3] + mg * dy;
+    t[4] = P[4] + mg * dz;
+    t[5] = P[5] + 2.0 * (dx * P[2] + dy * P[3] + dz * P[4]) + mg * (dx * dx + dy * dy + dz * dz);
+    const double dn = (double)ng;
+    const double vg = (sg / dn) / (1.0 + A.fudge / sqrt(dn));
+    t[6] = (double)tri_gt(vg, rhot, (2.0 * dn + 8.0) * u * fabs(vg) * 1.01);
+  }
+  G[0] = A.densg[g];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      nl += __shfl_xor_sync(0xffffffffu, nl, o);
-      nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
-      dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
-      S += __shfl_xor_sync(0xffffffffu, S, o);
-      M += __shfl_xor_sync(0xffffffffu, M, o);
-      Sx += __shfl_xor_sync(0xffffffffu, Sx, o);
-      Sy += __shfl_xor_sync(0xffffffffu, Sy, o);
-      Sz += __shfl_xor_sync(0xffffffffu, Sz, o);
-      Q += __shfl_xor_sync(0xffffffffu, Q, o);
-      triB = tri_or(triB, __shfl_xor_sync(0xffffffffu, triB, o));
-    }
-    if (lane == 0) {
-      double* C = A.cs + 12 * (size_t)(T.a + k);
-      const double n = (double)nl;
-      C[0] = n; C[1] = (double)nmax; C[2] = dmax; C[3] = S;
-      C[4] = M; C[5] = Sx; C[6] = Sy; C[7] = Sz; C[8] = Q;
-      int dec;
-      if (nl < A.nmembthresh) {
-        dec = 0;
-      } else {
-        const double dm = S / n;
-        const double edm = (2.0 * n + 8.0) * u * dm * 1.01;
-        const double thrA = xmul(rhot, xadd(1.0, xdiv(A.fudge, xsqrt(n))));
-        const int tA = tri_gt(dm, thrA, edm);
-        // dmax >= alphap * densmoy, densmoy known to +-edm
-        const double tiny = 8.0 * u * fabs(A.alphap * dm);
-        const int tC = (dmax >= A.alphap * (dm + edm) + tiny) ? 1
-                       : (dmax < A.alphap * (dm - edm) - tiny ? 0 : 2);
-        double r2 = Q / M - (Sx * Sx + Sy * Sy + Sz * Sz) / (M * M);
-        const double r = sqrt(fabs(r2));
-        const int tD = (r >= A.epsilon * (1.0 + 1e-6) + 1e-300) ? 1 : (r < A.epsilon * (1.0 - 1e-6) ? 0 : 2);
-        dec = tri_and(tri_and(tri_or(tA, triB), tC), tD);
-      }
-      C[9] = (double)dec;
-      C[10] = 0.0;
+  for (int c = 0; c < 7; ++c) G[1 + c] = t[c];
+}
+
+// Sum the gs rows of positions [c0, c1) over one warp and decide the
+// significance test (f90:1459-1463) in three states from the rigorous
+// rounding bounds; lane 0 writes cs row C.
+__device__ void component_decide(const TreeArgs& A, int32_t c0, int32_t c1, double rhot, double* C, int lane) {
+  const double u = 1.1102230246251565e-16;
+  long long nl = 0;
+  int32_t nmax = 0;
+  double dmax = -1.0, S = 0, M = 0, Sx = 0, Sy = 0, Sz = 0, Q = 0;
+  int triB = 0;  // densmoy_comp_max > rhot
+#pragma unroll 4
+  for (int32_t i = c0 + lane; i < c1; i += 32) {
+    const double* G = A.gs + 8 * (size_t)i;
+    const int32_t ng = A.gn[i];
+    nl += ng;
+    nmax = max(nmax, ng);
+    dmax = fmax(dmax, G[0]);
+    S += G[1];
+    M += G[2];
+    Sx += G[3];
+    Sy += G[4];
+    Sz += G[5];
+    Q += G[6];
+    triB = tri_or(triB, (int)G[7]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    nl += __shfl_xor_sync(0xffffffffu, nl, o);
+    nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+    dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    S += __shfl_xor_sync(0xffffffffu, S, o);
+    M += __shfl_xor_sync(0xffffffffu, M, o);
+    Sx += __shfl_xor_sync(0xffffffffu, Sx, o);
+    Sy += __shfl_xor_sync(0xffffffffu, Sy, o);
+    Sz += __shfl_xor_sync(0xffffffffu, Sz, o);
+    Q += __shfl_xor_sync(0xffffffffu, Q, o);
+    triB = tri_or(triB, __shfl_xor_sync(0xffffffffu, triB, o));
+  }
+  if (lane != 0) return;
+  const double n = (double)nl;
+  C[0] = n; C[1] = (double)nmax; C[2] = dmax; C[3] = S;
+  C[4] = M; C[5] = Sx; C[6] = Sy; C[7] = Sz; C[8] = Q;
+  int dec;
+  if (nl < A.nmembthresh) {
+    dec = 0;
+  } else {
+    const double dm = S / n;
+    const double edm = (2.0 * n + 8.0) * u * dm * 1.01;
+    const double thrA = xmul(rhot, xadd(1.0, xdiv(A.fudge, xsqrt(n))));
+    const int tA = tri_gt(dm, thrA, edm);
+    // dmax >= alphap * densmoy, densmoy known to +-edm
+    const double tiny = 8.0 * u * fabs(A.alphap * dm);
+    const int tC = (dmax >= A.alphap * (dm + edm) + tiny) ? 1
+                   : (dmax < A.alphap * (dm - edm) - tiny ? 0 : 2);
+    // radius test r >= epsilon.  The reference forms r^2 from absolute
+    // coordinates (|u| <= L after the unwrap about posref), so its own value
+    // carries up to ~(18n+48)u L^2 of cancellation error; these sums carry up
+    // to ~3(2n+8)u * 3L^2 * 2 more.  Decide only outside both.
+    const double r2 = Q / M - (Sx * Sx + Sy * Sy + Sz * Sz) / (M * M);
+    const double Lm = fmax(A.Lx, fmax(A.Ly, A.Lz));
+    const double er2 = ((18.0 * n + 48.0) + 18.0 * (2.0 * n + 8.0)) * u * Lm * Lm * 1.01;
+    const double e2 = A.epsilon * A.epsilon;
+    const int tD = (r2 - er2 >= e2 * (1.0 + 16.0 * u)) ? 1 : (r2 + er2 < e2 * (1.0 - 16.0 * u) ? 0 : 2);
+    const int tAB = tri_or(tA, triB);
+    dec = tri_and(tri_and(tAB, tC), tD);
+    if (dec == 2) {
+      if (tAB == 2) atomicAdd(&A.stats[8], 1ULL);
+      if (tC == 2) atomicAdd(&A.stats[9], 1ULL);
+      if (tD == 2) atomicAdd(&A.stats[10], 1ULL);
     }
   }
+  C[9] = (double)dec;
+  C[10] = (dec == 2) ? 1.0 : 0.0;  // undecided: recompute exactly
+}
+
+// Approximate statistics of every component of the task: anchors, then the
+// groups' terms position-parallel over the whole block, then a warp per
+// component sums them and decides.
+__device__ void approx_stats(const TreeArgs& A, SharedTask& T) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const double rhot = T.rhot;
+  const int32_t a = T.a, b = T.b, ncomp = T.ncomp;
+  for (int32_t k = tid; k < ncomp; k += kNT) {
+    const int32_t p0 = A.gpeak[A.GL[A.cstart[a + k]]];
+    double* C = A.cs + 12 * (size_t)(a + k);
+    C[9] = A.x[p0];
+    C[10] = A.y[p0];
+    C[11] = A.z[p0];
+  }
+  __syncthreads();
+  for (int32_t i = a + tid; i < b; i += kNT) position_terms(A, i, rhot, A.cs + 12 * (size_t)(a + A.compidx[i]) + 9);
+  __syncthreads();
+  for (int32_t k = warp; k < ncomp; k += kNT / 32)
+    component_decide(A, A.cstart[a + k], comp_end(A, T, k), rhot, A.cs + 12 * (size_t)(a + k), lane);
+  __syncthreads();
 }
 
 // Exact per-group sums in the reference order (treat_particles f90:2317-2401):
@@ -449,22 +532,25 @@ __device__ void group_sums_thread(const TreeArgs& A, int32_t g, double rhot, dou
 }
 
 // Same sums for a large group by one warp: each lane computes the terms of
-// one member (explicitly rounded, so each term has the reference's bits) and
-// lane 0 adds them in member order -- the same sequence of roundings as the
-// Fortran loop, without one dependent global load per member on one thread.
-// st: 32*6 doubles of warp-private shared memory.
+// one member (explicitly rounded, so each term has the reference's bits); the
+// terms of the members above rhot are packed in member order and lanes 0..5
+// each run one of the six sequential sums over them -- the same sequence of
+// roundings as the Fortran loop, without one dependent global load per
+// member on one thread.  st: 32*6 doubles of warp-private shared memory.
 __device__ void group_sums_warp(const TreeArgs& A, int32_t g, double rhot, double rx, double ry, double rz,
                                 double* G, double* st, int lane) {
   const int32_t q0 = A.goff[g], q1 = A.goff[g + 1];
   int32_t imass = 0;
-  double tm = 0, px = 0, py = 0, pz = 0, rs = 0, dm = 0;
+  double acc = 0.0;  // lane c < 6 carries sum c: truemass, posg(3), rsquare, densmoy
   for (int32_t base = q0; base < q1; base += 32) {
     const int32_t q = base + lane;
-    double t[6] = {0, 0, 0, 0, 0, -1.0};  // t[5] < 0 marks "not above rhot"
+    bool ok = false;
+    double t[6];
     if (q < q1) {
       const int32_t s = A.gmem[q];
       const double d = A.dens[s];
       if (d > rhot) {
+        ok = true;
         const double xm = A.m[s];
         const double ux = xadd(wrapd(xsub(A.x[s], rx), A.Lx, A.hx), rx);
         const double uy = xadd(wrapd(xsub(A.y[s], ry), A.Ly, A.hy), ry);
@@ -477,40 +563,27 @@ __device__ void group_sums_warp(const TreeArgs& A, int32_t g, double rhot, doubl
         t[5] = d;
       }
     }
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    const int cnt = __popc(m);
+    if (ok) {
+      const int slot = __popc(m & ((1u << lane) - 1));
 #pragma unroll
-    for (int c = 0; c < 6; ++c) st[lane * 6 + c] = t[c];
-    __syncwarp();
-    // lanes 0..5 each run one of the six sequential sums, lane 6 the count:
-    // the same additions in the same order as a single thread would do
-    if (lane < 7) {
-      const int cnt = min(32, q1 - base);
-      double acc = (lane == 0) ? tm : (lane == 1) ? px : (lane == 2) ? py : (lane == 3) ? pz : (lane == 4) ? rs : dm;
-      const int col = (lane == 0) ? 0 : (lane == 1) ? 1 : (lane == 2) ? 2 : (lane == 3) ? 3 : (lane == 4) ? 4 : 5;
-      int cntg = 0;
-      for (int l = 0; l < cnt; ++l) {
-        const double* u = st + l * 6;
-        if (u[5] < 0.0) continue;
-        ++cntg;
-        if (lane < 6) acc = xadd(acc, u[col]);
-      }
-      if (lane == 0) tm = acc;
-      else if (lane == 1) px = acc;
-      else if (lane == 2) py = acc;
-      else if (lane == 3) pz = acc;
-      else if (lane == 4) rs = acc;
-      else if (lane == 5) dm = acc;
-      else imass += cntg;
+      for (int c = 0; c < 6; ++c) st[slot * 6 + c] = t[c];
     }
     __syncwarp();
+    if (lane < 6) {
+#pragma unroll 8
+      for (int l = 0; l < cnt; ++l) acc = xadd(acc, st[l * 6 + lane]);
+    }
+    imass += cnt;
+    __syncwarp();
   }
-  // gather the seven chains to lane 0
-  tm = __shfl_sync(0xffffffffu, tm, 0);
-  px = __shfl_sync(0xffffffffu, px, 1);
-  py = __shfl_sync(0xffffffffu, py, 2);
-  pz = __shfl_sync(0xffffffffu, pz, 3);
-  rs = __shfl_sync(0xffffffffu, rs, 4);
-  dm = __shfl_sync(0xffffffffu, dm, 5);
-  imass = __shfl_sync(0xffffffffu, imass, 6);
+  const double tm = __shfl_sync(0xffffffffu, acc, 0);
+  const double px = __shfl_sync(0xffffffffu, acc, 1);
+  const double py = __shfl_sync(0xffffffffu, acc, 2);
+  const double pz = __shfl_sync(0xffffffffu, acc, 3);
+  const double rs = __shfl_sync(0xffffffffu, acc, 4);
+  const double dm = __shfl_sync(0xffffffffu, acc, 5);
   if (lane == 0) { G[0] = (double)imass; G[1] = tm; G[2] = px; G[3] = py; G[4] = pz; G[5] = rs; G[6] = dm; }
 }
 
@@ -631,11 +704,37 @@ __global__ void root_cstart_kernel(const TreeArgs A, const int32_t* flag, const 
   A.compidx[i] = scan[i] + flag[i] - 1;
 }
 
-// one block per colour: exact sums and the significance test
+// anchor of every colour (peak of its first group) in cs[k][9..11]
+__global__ void root_anchor_kernel(const TreeArgs A, int32_t ncomp) {
+  const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ncomp) return;
+  const int32_t p0 = A.gpeak[A.GL[A.cstart[k]]];
+  double* C = A.cs + 12 * (size_t)k;
+  C[9] = A.x[p0];
+  C[10] = A.y[p0];
+  C[11] = A.z[p0];
+}
+
+__global__ void root_terms_kernel(const TreeArgs A, double rhot) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.ngroups) return;
+  position_terms(A, i, rhot, A.cs + 12 * (size_t)A.compidx[i] + 9);
+}
+
+// a warp per colour: approximate sums and the three-state test
+__global__ void root_decide_kernel(const TreeArgs A, int32_t ncomp, double rhot) {
+  const int32_t k = (int32_t)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+  if (k >= ncomp) return;
+  const int32_t c1 = (k + 1 < ncomp) ? A.cstart[k + 1] : A.ngroups;
+  component_decide(A, A.cstart[k], c1, rhot, A.cs + 12 * (size_t)k, threadIdx.x & 31);
+}
+
+// one block per undecided colour: exact sums and the significance test
 __global__ void __launch_bounds__(kNT) root_colour_kernel(const TreeArgs A, int32_t ncomp, double rhot) {
   __shared__ double s_terms[kNT / 32 * 32 * 6];
   __shared__ int32_t s_ref;
   const int32_t k = blockIdx.x;
+  if (A.cs[12 * (size_t)k + 10] == 0.0) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int32_t c0 = A.cstart[k], c1 = (k + 1 < ncomp) ? A.cstart[k + 1] : A.ngroups;
   if (tid == 0) s_ref = colour_posref(A, A.GL[c0], rhot);
@@ -676,22 +775,20 @@ __global__ void root_nodes_kernel(const TreeArgs A, int32_t ncomp, const int32_t
   nd.sister = is > 0 ? io - 1 : 0;
   nd.nsisters = nsisters;
   nd.mass = (int32_t)C[0];
-  nd.truemass = C[4];
-  double pf0 = xdiv(C[5], C[4]), pf1 = xdiv(C[6], C[4]), pf2 = xdiv(C[7], C[4]);
-  nd.radius = C[8];
-  nd.density = C[3];
-  if (pf0 >= A.hx) pf0 = xsub(pf0, A.Lx); else if (pf0 < -A.hx) pf0 = xadd(pf0, A.Lx);
-  if (pf1 >= A.hy) pf1 = xsub(pf1, A.Ly); else if (pf1 < -A.hy) pf1 = xadd(pf1, A.Ly);
-  if (pf2 >= A.hz) pf2 = xsub(pf2, A.Lz); else if (pf2 < -A.hz) pf2 = xadd(pf2, A.Lz);
-  nd.pos[0] = pf0; nd.pos[1] = pf1; nd.pos[2] = pf2;
   nd.rho_saddle = rhot;
   nd.level = 1;
   nd.firstchild = 0;
   if (nd.mass == 0) set_err(A, 15, io);
   const int32_t c0 = A.cstart[k], c1 = (k + 1 < ncomp) ? A.cstart[k + 1] : A.ngroups;
   next[is] = Task{xmul(rhot, xadd(1.0, xdiv(A.fudge, xsqrt(C[1])))), io, c0, c1, 1};
-  for (int32_t i = c0; i < c1; ++i) A.deepnode[A.GL[i]] = io;
   if (is == nsisters - 1) A.node[0].firstchild = io;  // f90:1540
+}
+
+__global__ void root_deepnode_kernel(const TreeArgs A, const int32_t* flag, const int32_t* rank) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.ngroups) return;
+  const int32_t k = A.compidx[i];
+  if (flag[k]) A.deepnode[A.GL[i]] = 1 + rank[k];
 }
 
 template <class SortT, class ScanT, class MaxScanT>
@@ -702,9 +799,12 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
   __shared__ int32_t s_keys[kChunk];
   __shared__ double s_terms[kNT / 32 * 32 * 6];
   __shared__ SharedTask T;
-  __shared__ long long s_clk[4];  // structural, approx, exact cycles; levels
+  __shared__ long long s_clk[6];  // structural, approx, exact cycles; levels; structural passes; max ncomp
+  __shared__ long long s_ph[8];   // cycles per phase of the structural passes
   const int tid = threadIdx.x;
-  if (tid < 4) s_clk[tid] = 0;
+  const long long t_start = clock64();
+  if (tid < 6) s_clk[tid] = 0;
+  if (tid < 8) s_ph[tid] = 0;
   if (tid == 0) {
     const Task t = tasks[blockIdx.x];
     T.rhot = t.rhot; T.inode = t.inode; T.a = t.a; T.b = t.b; T.level = t.level;
@@ -722,38 +822,36 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
     __syncthreads();
     long long c0 = clock64();
     if (restructure) {
-      structural_pass<SortT, ScanT, MaxScanT>(A, T, sort_tmp, scan_tmp, maxscan_tmp, s_keys);
-      if (tid == 0) atomicAdd(&A.stats[7], 1ULL);
+      structural_pass<SortT, ScanT, MaxScanT>(A, T, sort_tmp, scan_tmp, maxscan_tmp, s_keys, s_ph);
+      if (tid == 0) { atomicAdd(&A.stats[7], 1ULL); s_clk[4] += 1; }
     }
     long long c1 = clock64();
-    if (tid == 0) { s_clk[0] += c1 - c0; s_clk[3] += 1; }
+    if (tid == 0) { s_clk[0] += c1 - c0; s_clk[3] += 1; s_clk[5] = max(s_clk[5], (long long)T.ncomp); }
     if (T.nsurv == 0) {  // all groups below the threshold (f90:1348-1351 prints, then ends with no colour)
       if (tid == 0) A.node[T.inode].firstchild = 0;
       break;
     }
     approx_stats(A, T);
-    __syncthreads();
-    if (tid == 0) s_clk[1] += clock64() - c1;
-    // flag unknown decisions for exact recomputation
-    if (tid == 0) T.nexact = 0;
-    __syncthreads();
-    for (int32_t k = tid; k < T.ncomp; k += kNT) {
-      double* C = A.cs + 12 * (size_t)(T.a + k);
-      if (C[9] == 2.0) { C[10] = 1.0; atomicAdd(&T.nexact, 1); }
+    if (tid == 0) {
+      s_clk[1] += clock64() - c1;
+      T.nexact = 0;
+      T.nsisters = 0;
+      T.kk = -1;
     }
     __syncthreads();
-    const int32_t nexact = T.nexact;  // block-uniform after the barrier
+    for (int32_t k = tid; k < T.ncomp; k += kNT)
+      if (A.cs[12 * (size_t)(T.a + k) + 10] != 0.0) atomicAdd(&T.nexact, 1);
     __syncthreads();
-    if (nexact > 0) {
+    if (T.nexact > 0) {  // undecided tests: exact sums in the reference order
       long long c2 = clock64();
       exact_stats(A, T, s_terms);
       if (tid == 0) { s_clk[2] += clock64() - c2; atomicAdd(&A.stats[4], 1ULL); }
     }
-    // count significant components
-    if (tid == 0) {
-      int32_t ns = 0;
-      for (int32_t k = 0; k < T.ncomp; ++k) ns += (A.cs[12 * (size_t)(T.a + k) + 9] == 1.0);
-      T.nsisters = ns;
+    for (int32_t k = tid; k < T.ncomp; k += kNT) {
+      if (A.cs[12 * (size_t)(T.a + k) + 9] == 1.0) {
+        atomicAdd(&T.nsisters, 1);
+        T.kk = k;  // the significant component when there is exactly one
+      }
     }
     __syncthreads();
     const int32_t ns = T.nsisters;
@@ -763,10 +861,7 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
     }
     if (ns == 1) {
       if (tid == 0) {
-        int32_t kk = 0;
-        for (int32_t k = 0; k < T.ncomp; ++k)
-          if (A.cs[12 * (size_t)(T.a + k) + 9] == 1.0) kk = k;
-        const double mc = A.cs[12 * (size_t)(T.a + kk) + 1];
+        const double mc = A.cs[12 * (size_t)(T.a + T.kk) + 1];
         const double rnew = xmul(T.rhot, xadd(1.0, xdiv(A.fudge, xsqrt(mc))));
         if (T.nsurv > 1) {
           T.rhot = rnew;
@@ -782,70 +877,55 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
       if (T.done) break;
       continue;
     }
-    // ---- branching: exact sums for the significant components, then nodes
-    for (int32_t k = tid; k < T.ncomp; k += kNT) {
-      double* C = A.cs + 12 * (size_t)(T.a + k);
-      C[10] = (C[9] == 1.0) ? 1.0 : 0.0;
-    }
-    __syncthreads();
-    long long c3 = clock64();
-    exact_stats(A, T, s_terms);
-    if (tid == 0) s_clk[2] += clock64() - c3;
+    // ---- branching (f90:1484-1571): one node per significant component in
+    // colour order.  Counts, densmax and the child thresholds are exact here;
+    // truemass, position, radius and mean density are formed after the
+    // waves (node_sums), in the reference's summation order.
     if (tid == 0) {
-      int32_t ns2 = 0;
-      for (int32_t k = 0; k < T.ncomp; ++k) ns2 += (A.cs[12 * (size_t)(T.a + k) + 9] == 1.0);
-      // the exact pass only recomputes components already decided significant
-      if (ns2 != ns) set_err(A, 13, T.inode);
       const int32_t first = atomicAdd(A.nnodes, ns) + 1;
-      if (first + ns - 1 > A.nnodesmax) { set_err(A, 14, first); ns2 = 0; }
+      if (first + ns - 1 > A.nnodesmax) set_err(A, 14, first);
       T.inode1 = first;
-      T.nsisters = (ns2 == ns) ? ns : 0;
+      T.done = (first + ns - 1 > A.nnodesmax);
     }
     __syncthreads();
-    if (T.nsisters == 0) break;
-    if (tid == 0) {
-      int32_t is = 0;
-      for (int32_t k = 0; k < T.ncomp; ++k) {
+    if (T.done) break;
+    {
+      int32_t carry = 0;
+      for (int32_t k0 = 0; k0 < T.ncomp; k0 += kNT) {
+        const int32_t k = k0 + tid;
         const double* C = A.cs + 12 * (size_t)(T.a + k);
-        if (C[9] != 1.0) continue;
-        const int32_t io = T.inode1 + is;
-        NodeRec& nd = A.node[io];
-        nd.mother = T.inode;
-        nd.densmax = C[2];
-        nd.sister = is > 0 ? io - 1 : 0;
-        nd.nsisters = T.nsisters;
-        nd.mass = (int32_t)C[0];
-        nd.truemass = C[4];
-        double pf0 = xdiv(C[5], C[4]), pf1 = xdiv(C[6], C[4]), pf2 = xdiv(C[7], C[4]);
-        nd.radius = C[8];
-        nd.density = C[3];
-        if (pf0 >= A.hx) pf0 = xsub(pf0, A.Lx); else if (pf0 < -A.hx) pf0 = xadd(pf0, A.Lx);
-        if (pf1 >= A.hy) pf1 = xsub(pf1, A.Ly); else if (pf1 < -A.hy) pf1 = xadd(pf1, A.Ly);
-        if (pf2 >= A.hz) pf2 = xsub(pf2, A.Lz); else if (pf2 < -A.hz) pf2 = xadd(pf2, A.Lz);
-        nd.pos[0] = pf0; nd.pos[1] = pf1; nd.pos[2] = pf2;
-        nd.rho_saddle = T.rhot;
-        nd.level = T.level + 1;
-        nd.firstchild = 0;
-        if (nd.mass == 0) set_err(A, 15, io);  // f90:1506-1510
-        // child task (f90:1543-1556)
-        const double rc = xmul(T.rhot, xadd(1.0, xdiv(A.fudge, xsqrt(C[1]))));
-        const int32_t slot = atomicAdd(A.nnext, 1);
-        A.next[slot] = Task{rc, io, A.cstart[T.a + k], comp_end(A, T, k), T.level + 1};
-        ++is;
+        const int sig = (k < T.ncomp && C[9] == 1.0) ? 1 : 0;
+        int32_t ex, tot;
+        ScanT(scan_tmp).ExclusiveSum(sig, ex, tot);
+        __syncthreads();
+        if (k < T.ncomp) A.cnt[T.a + k] = sig ? T.inode1 + carry + ex : 0;  // node of component k
+        if (sig) {
+          const int32_t is = carry + ex;
+          const int32_t io = T.inode1 + is;
+          NodeRec& nd = A.node[io];
+          nd.mother = T.inode;
+          nd.densmax = C[2];
+          nd.sister = is > 0 ? io - 1 : 0;
+          nd.nsisters = ns;
+          nd.mass = (int32_t)C[0];
+          nd.rho_saddle = T.rhot;
+          nd.level = T.level + 1;
+          nd.firstchild = 0;
+          if (nd.mass == 0) set_err(A, 15, io);  // f90:1506-1510
+          // child task (f90:1543-1556)
+          const double rc = xmul(T.rhot, xadd(1.0, xdiv(A.fudge, xsqrt(C[1]))));
+          const int32_t slot = atomicAdd(A.nnext, 1);
+          A.next[slot] = Task{rc, io, A.cstart[T.a + k], comp_end(A, T, k), T.level + 1};
+        }
+        carry += tot;
       }
-      A.node[T.inode].firstchild = T.inode1 + T.nsisters - 1;  // f90:1540
     }
+    if (tid == 0) A.node[T.inode].firstchild = T.inode1 + ns - 1;  // f90:1540
     __syncthreads();
     // deepest node per group
-    {
-      int32_t is = 0;
-      for (int32_t k = 0; k < T.ncomp; ++k) {
-        const double* C = A.cs + 12 * (size_t)(T.a + k);
-        if (C[9] != 1.0) continue;
-        const int32_t io = T.inode1 + is;
-        for (int32_t i = A.cstart[T.a + k] + tid; i < comp_end(A, T, k); i += kNT) A.deepnode[A.GL[i]] = io;
-        ++is;
-      }
+    for (int32_t i = T.a + tid; i < T.b; i += kNT) {
+      const int32_t io = A.cnt[T.a + A.compidx[i]];
+      if (io > 0) A.deepnode[A.GL[i]] = io;
     }
     break;
   }
@@ -858,7 +938,152 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
     atomicAdd(&A.stats[3], (unsigned long long)s_clk[3]);
     atomicMax(&A.stats[5], (unsigned long long)s_clk[3]);
     atomicMax(&A.stats[6], (unsigned long long)(s_clk[0] + s_clk[1] + s_clk[2]));
+    if (A.tprof) {
+      const Task t = tasks[blockIdx.x];
+      long long* r = A.tprof + 16 * (size_t)t.inode;
+      r[0] = t.b - t.a;       // groups in the task's range
+      r[1] = s_clk[3];        // levels
+      r[2] = s_clk[4];        // structural passes
+      r[3] = s_clk[0];        // cycles: structural
+      r[4] = s_clk[1];        // cycles: approximate statistics
+      r[5] = s_clk[2];        // cycles: exact sums
+      r[6] = clock64() - t_start;  // cycles: whole task
+      r[7] = s_clk[5];        // largest component count at one level
+      for (int k = 0; k < 8; ++k) r[8 + k] = s_ph[k];  // structural phases
+    }
   }
+}
+
+// ------------------------------------------------------------- node sums
+// truemass, position, radius and mean density of every created node, in the
+// reference's order: treat_particles (f90:2317-2401) per group at the node's
+// creation threshold, posref from the first group, then the fold over the
+// colour's groups in colour order (f90:1407-1432), which is ascending group
+// id (a colour's groups keep their relative order through every reorder).
+// A node's groups are the groups whose deepest node lies in its subtree, so
+// every (node, group) pair is independent: all of them are summed at once
+// after the waves instead of inside the task that created the node.
+
+// pairs per group: the depth of its deepest node; cnt[ng] = 0 closes the scan
+__global__ void pair_count_kernel(const TreeArgs A, int32_t nn, int32_t* cnt) {
+  const int32_t g = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (g > A.ngroups + 1) return;
+  if (g == A.ngroups + 1) { cnt[A.ngroups] = 0; return; }
+  int32_t d = 0, N = A.deepnode[g];
+  while (N > 0 && d <= nn) {
+    ++d;
+    N = A.node[N].mother;
+  }
+  if (d > nn) { set_err(A, 19, g); d = 0; }  // a cycle in the mother links
+  cnt[g - 1] = d;
+}
+
+__global__ void pair_emit_kernel(const TreeArgs A, const int32_t* __restrict__ off,
+                                 unsigned long long* __restrict__ keys) {
+  const int32_t g = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (g > A.ngroups) return;
+  int32_t p = off[g - 1];
+  const int32_t p1 = off[g];
+  for (int32_t N = A.deepnode[g]; N > 0 && p < p1; N = A.node[N].mother)
+    keys[p++] = ((unsigned long long)N << 32) | (unsigned)g;
+}
+
+// pair range [nstart[N], nend[N]) of every node in the sorted pair keys
+__global__ void node_range_kernel(const unsigned long long* __restrict__ keys, int64_t np, int32_t* nstart,
+                                  int32_t* nend) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  const int32_t N = (int32_t)(keys[p] >> 32);
+  if (p == 0 || (int32_t)(keys[p - 1] >> 32) != N) nstart[N] = (int32_t)p;
+  if (p == np - 1 || (int32_t)(keys[p + 1] >> 32) != N) nend[N] = (int32_t)(p + 1);
+}
+
+// posref of every node (f90:2340-2344): the first member, in list order, of
+// its first group above its threshold; a warp per node
+__global__ void node_posref_kernel(const TreeArgs A, int32_t nn, const unsigned long long* __restrict__ keys,
+                                   const int32_t* __restrict__ nstart, const int32_t* __restrict__ nend,
+                                   int32_t* __restrict__ posref) {
+  const int32_t N = (int32_t)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) + 1;
+  const int lane = threadIdx.x & 31;
+  if (N > nn) return;
+  if (nstart[N] >= nend[N]) {
+    if (lane == 0) { set_err(A, 20, N); posref[N] = 0; }
+    return;
+  }
+  const int32_t g0 = (int32_t)(keys[nstart[N]] & 0xffffffffu);
+  const double rhot = A.node[N].rho_saddle;
+  const int32_t q1 = A.goff[g0 + 1];
+  for (int32_t base = A.goff[g0]; base < q1; base += 32) {
+    const int32_t q = base + lane;
+    const int32_t s = (q < q1) ? A.gmem[q] : -1;
+    const bool ok = (s >= 0) && A.dens[s] > rhot;
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    if (m) {
+      if (lane == __ffs(m) - 1) posref[N] = s;
+      return;
+    }
+  }
+  if (lane == 0) { set_err(A, 18, g0); posref[N] = A.gpeak[g0]; }  // cannot happen: the peak is above
+}
+
+// per (node, group) pair sums, a thread per pair of a small group
+__global__ void pair_sums_kernel(const TreeArgs A, const unsigned long long* __restrict__ keys, int64_t np,
+                                 const int32_t* __restrict__ posref, double* __restrict__ ps) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  const int32_t N = (int32_t)(keys[p] >> 32), g = (int32_t)(keys[p] & 0xffffffffu);
+  if (A.goff[g + 1] - A.goff[g] > kBigGroup) return;
+  const int32_t ref = posref[N];
+  group_sums_thread(A, g, A.node[N].rho_saddle, A.x[ref], A.y[ref], A.z[ref], ps + 8 * p);
+}
+
+// the same for pairs of large groups, a warp per pair
+__global__ void __launch_bounds__(256) pair_sums_warp_kernel(const TreeArgs A,
+                                                             const unsigned long long* __restrict__ keys,
+                                                             int64_t np, const int32_t* __restrict__ posref,
+                                                             double* __restrict__ ps) {
+  __shared__ double st[8][32 * 6];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t nw = (int64_t)gridDim.x * 8;
+  for (int64_t p = (int64_t)blockIdx.x * 8 + wib; p < np; p += nw) {
+    const int32_t N = (int32_t)(keys[p] >> 32), g = (int32_t)(keys[p] & 0xffffffffu);
+    if (A.goff[g + 1] - A.goff[g] <= kBigGroup) continue;
+    const int32_t ref = posref[N];
+    group_sums_warp(A, g, A.node[N].rho_saddle, A.x[ref], A.y[ref], A.z[ref], ps + 8 * p, st[wib], lane);
+  }
+}
+
+// fold every node's pair sums in ascending group id and write its fields
+// (f90:1407-1432, 1511-1538)
+__global__ void node_fold_kernel(const TreeArgs A, int32_t nn, const int32_t* __restrict__ nstart,
+                                 const int32_t* __restrict__ nend, const double* __restrict__ ps) {
+  const int32_t N = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (N > nn) return;
+  double posg0 = 0, posg1 = 0, posg2 = 0, tm = 0, rsg = 0, dmg = 0;
+  int32_t ml = 0;
+  for (int32_t p = nstart[N]; p < nend[N]; ++p) {
+    const double* G = ps + 8 * (size_t)p;
+    posg0 = xadd(posg0, G[2]);
+    posg1 = xadd(posg1, G[3]);
+    posg2 = xadd(posg2, G[4]);
+    rsg = xadd(rsg, G[5]);
+    ml += (int32_t)G[0];
+    tm = xadd(tm, G[1]);
+    dmg = xadd(dmg, G[6]);
+  }
+  NodeRec& nd = A.node[N];
+  if (ml != nd.mass) set_err(A, 21, N);
+  const double p2 = xadd(xadd(xmul(posg0, posg0), xmul(posg1, posg1)), xmul(posg2, posg2));
+  nd.radius = xsqrt(fabs(xdiv(xsub(xmul(tm, rsg), p2), xmul(tm, tm))));
+  nd.density = xdiv(dmg, (double)ml);
+  nd.truemass = tm;
+  double pf0 = xdiv(posg0, tm), pf1 = xdiv(posg1, tm), pf2 = xdiv(posg2, tm);
+  if (pf0 >= A.hx) pf0 = xsub(pf0, A.Lx); else if (pf0 < -A.hx) pf0 = xadd(pf0, A.Lx);
+  if (pf1 >= A.hy) pf1 = xsub(pf1, A.Ly); else if (pf1 < -A.hy) pf1 = xadd(pf1, A.Ly);
+  if (pf2 >= A.hz) pf2 = xsub(pf2, A.Lz); else if (pf2 < -A.hz) pf2 = xadd(pf2, A.Lz);
+  nd.pos[0] = pf0;
+  nd.pos[1] = pf1;
+  nd.pos[2] = pf2;
 }
 
 // ------------------------------------------------------- setup / membership / order
@@ -1072,6 +1297,12 @@ int stage_nodes(Engine& E) {
   AHOP_CUDA_TRY(cudaMemsetAsync(E.d_flags.p, 0, 256, st));
   int32_t* flags = E.d_flags.as<int32_t>();  // [0..1] err, [2] nnodes, [3] nnext
   A.stats = reinterpret_cast<unsigned long long*>(E.d_flags.as<char>() + 128);
+  A.tprof = nullptr;
+  if (E.task_profile) {
+    AHOP_CUDA_TRY(E.d_tprof.ensure((size_t)(nnodesmax + 1) * 128));
+    AHOP_CUDA_TRY(cudaMemsetAsync(E.d_tprof.p, 0, (size_t)(nnodesmax + 1) * 128, st));
+    A.tprof = E.d_tprof.as<long long>();
+  }
   A.err = flags;
   A.nnodes = flags + 2;
   A.nnext = flags + 3;
@@ -1136,7 +1367,10 @@ int stage_nodes(Engine& E) {
     AHOP_CUDA_TRY(cudaMemcpyAsync(h + 4, A.run + ng, 4, cudaMemcpyDeviceToHost, st));
     AHOP_CUDA_TRY(cudaStreamSynchronize(st));
     const int32_t ncomp = h[4];
-    E.launches++;
+    E.launches += 4;
+    root_anchor_kernel<<<(unsigned)((ncomp + T - 1) / T), T, 0, st>>>(A, ncomp);
+    root_terms_kernel<<<gb, T, 0, st>>>(A, rhot);
+    root_decide_kernel<<<(unsigned)(((int64_t)ncomp * 32 + T - 1) / T), T, 0, st>>>(A, ncomp, rhot);
     root_colour_kernel<<<ncomp, kNT, 0, st>>>(A, ncomp, rhot);
     E.launches++;
     root_okflag_kernel<<<(unsigned)((ncomp + 1 + T - 1) / T), T, 0, st>>>(A, ncomp, A.cnt);
@@ -1158,6 +1392,8 @@ int stage_nodes(Engine& E) {
       E.launches++;
       root_nodes_kernel<<<(unsigned)((ncomp + T - 1) / T), T, 0, st>>>(A, ncomp, A.cnt, A.run, nsis, rhot,
                                                                        tasks[1]);
+      E.launches++;
+      root_deepnode_kernel<<<gb, T, 0, st>>>(A, A.cnt, A.run);
       AHOP_CUDA_TRY(cudaGetLastError());
       AHOP_CUDA_TRY(cudaMemcpyAsync(A.nnodes, &nsis, 4, cudaMemcpyHostToDevice, st));
       ntasks = nsis;
@@ -1189,9 +1425,65 @@ int stage_nodes(Engine& E) {
     cur ^= 1;
     E.waves = wave + 1;
   }
-  AHOP_CUDA_TRY(cudaEventRecord(E.ev[13], st));
   const int32_t nn = h[2];
   E.nnodes = nn;
+  // ---- node sums in the reference order (deferred from the waves)
+  if (nn > 0) {
+    const unsigned gb1 = (unsigned)((ng + 1 + T - 1) / T);
+    E.launches++;
+    pair_count_kernel<<<gb1, T, 0, st>>>(A, nn, A.cnt);
+    AHOP_CUDA_TRY(cudaGetLastError());
+    size_t t1 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, t1, A.cnt, A.run, ng + 1, st);
+    AHOP_CUDA_TRY(E.d_cub.ensure(t1));
+    E.cub_calls++;
+    AHOP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(E.d_cub.p, t1, A.cnt, A.run, ng + 1, st));
+    AHOP_CUDA_TRY(cudaMemcpyAsync(h + 4, A.run + ng, 4, cudaMemcpyDeviceToHost, st));
+    AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+    const int64_t np = h[4];
+    if (np > 0) {
+      AHOP_CUDA_TRY(E.d_pairs.ensure((size_t)np * 16));
+      AHOP_CUDA_TRY(E.d_pair_sums.ensure((size_t)np * 64));
+      AHOP_CUDA_TRY(E.d_node_aux.ensure((size_t)(nn + 1) * 12));
+      unsigned long long* k0 = E.d_pairs.as<unsigned long long>();
+      unsigned long long* k1 = k0 + np;
+      int32_t* nstart = E.d_node_aux.as<int32_t>();
+      int32_t* nend = nstart + (nn + 1);
+      int32_t* posref = nend + (nn + 1);
+      E.launches++;
+      pair_emit_kernel<<<gb1, T, 0, st>>>(A, A.run, k0);
+      AHOP_CUDA_TRY(cudaGetLastError());
+      int nb = 1;
+      while ((1LL << nb) <= (int64_t)nn) ++nb;
+      cub::DoubleBuffer<unsigned long long> kb(k0, k1);
+      t1 = 0;
+      cub::DeviceRadixSort::SortKeys(nullptr, t1, kb, (int)np, 0, 32 + nb, st);
+      AHOP_CUDA_TRY(E.d_cub.ensure(t1));
+      E.cub_calls++;
+      AHOP_CUDA_TRY(cub::DeviceRadixSort::SortKeys(E.d_cub.p, t1, kb, (int)np, 0, 32 + nb, st));
+      const unsigned long long* keys = kb.Current();
+      AHOP_CUDA_TRY(cudaMemsetAsync(nstart, 0, (size_t)(nn + 1) * 8, st));
+      const unsigned pb = (unsigned)((np + T - 1) / T);
+      E.launches++;
+      node_range_kernel<<<pb, T, 0, st>>>(keys, np, nstart, nend);
+      E.launches++;
+      node_posref_kernel<<<(unsigned)(((int64_t)nn * 32 + T - 1) / T), T, 0, st>>>(A, nn, keys, nstart, nend,
+                                                                                    posref);
+      E.launches++;
+      pair_sums_kernel<<<pb, T, 0, st>>>(A, keys, np, posref, E.d_pair_sums.as<double>());
+      int nsm = 148;
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, E.device);
+      int64_t wblocks = (np + 7) / 8;
+      if (wblocks > (int64_t)nsm * 8) wblocks = (int64_t)nsm * 8;
+      E.launches++;
+      pair_sums_warp_kernel<<<(unsigned)wblocks, 256, 0, st>>>(A, keys, np, posref, E.d_pair_sums.as<double>());
+      E.launches++;
+      node_fold_kernel<<<(unsigned)((nn + T - 1) / T), T, 0, st>>>(A, nn, nstart, nend,
+                                                                    E.d_pair_sums.as<double>());
+      AHOP_CUDA_TRY(cudaGetLastError());
+    }
+  }
+  AHOP_CUDA_TRY(cudaEventRecord(E.ev[13], st));
   // ---- membership (f90:1297-1306 paint order => deepest node above rho_saddle)
   E.launches++;
   membership_kernel<<<(unsigned)((n + T - 1) / T), T, 0, st>>>(E.d_group.as<int32_t>(), E.d_dens.as<double>(),
@@ -1226,7 +1518,7 @@ int stage_nodes(Engine& E) {
     AHOP_CUDA_TRY(cudaGetLastError());
   }
   AHOP_CUDA_TRY(cudaMemcpyAsync(h, flags, 8, cudaMemcpyDeviceToHost, st));
-  AHOP_CUDA_TRY(cudaMemcpyAsync(E.tree_stats, E.d_flags.as<char>() + 128, 8 * 8, cudaMemcpyDeviceToHost, st));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(E.tree_stats, E.d_flags.as<char>() + 128, 11 * 8, cudaMemcpyDeviceToHost, st));
   AHOP_CUDA_TRY(cudaStreamSynchronize(st));
   if (h[0] != 0) {
     set_error("membership walk exceeded its bound");

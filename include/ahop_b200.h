@@ -134,8 +134,19 @@ int ahop_debug_compute_stages(const double* pos_in, const double* mass_in, int64
  * (summed over blocks), threshold levels, exact passes for undecided tests,
  * the largest number of levels of one task, the largest cycle count of one
  * task, structural passes; [8..12] kNN -- query leaves, candidate leaves,
- * leaf visits, list insertions, leaves that fell back to per-query search. */
+ * leaf visits, list insertions, leaves that fell back to per-query search;
+ * [13..15] significance tests left undecided by the approximate sums, by
+ * part: density, densmax, radius. */
 int ahop_debug_tree_stats(int64_t* out, int32_t n);
+/* Per-task structure-tree profile (off by default; turning it on costs one
+ * store per task).  Row k (16 int64) describes the task of node k: groups in
+ * its range, levels, structural passes, cycles in structural passes, in
+ * approximate statistics, in exact sums, in the whole task, the largest
+ * component count at one level, then the cycles of the eight phases of the
+ * structural passes (reset, union, find, offsets, reorder, copy, starts,
+ * component index).  Rows of nodes without a task stay 0. */
+int ahop_debug_set_task_profile(int32_t on);
+int ahop_debug_task_profile(int64_t* out, int32_t maxrows);
 /* Ask compute to keep the first k neighbours per particle (default nhop). */
 int ahop_debug_set_store_neighbours(int32_t k);
 
