@@ -265,6 +265,70 @@ __device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int64
   }
 }
 
+__device__ __forceinline__ bool key_less(double da, int32_t oa, double db, int32_t ob) {
+  return da < db || (da == db && oa < ob);
+}
+
+// A query's first list: the nv smallest (distance, index) pairs among its own
+// leaf jl and the adjacent leaf jn, by a warp bitonic sort of the 64
+// candidates (two per lane, element 2*lane + slot) instead of up to 63
+// one-at-a-time insertions.  Empty candidates are (+inf, INT_MAX) and sort last.
+__device__ __forceinline__ void init_two_leaves(const KnnArgs& A, WarpList& L, int64_t jl, int64_t jn, int64_t self,
+                                                double qx, double qy, double qz, int lane, unsigned& nvis) {
+  double d0 = CUDART_INF, d1 = CUDART_INF;
+  int32_t o0 = INT_MAX, o1 = INT_MAX, s0 = -1, s1 = -1;
+  const int64_t p0 = jl * kLeaf + lane;
+  if (p0 < A.n && p0 != self) {
+    d0 = pdist2(qx, qy, qz, A.x[p0], A.y[p0], A.z[p0], A.Lx, A.Ly, A.Lz);
+    o0 = A.orig[p0];
+    s0 = (int32_t)p0;
+  }
+  ++nvis;
+  if (jn >= 0 && jn != jl) {
+    const int64_t p1 = jn * kLeaf + lane;
+    if (p1 < A.n && p1 != self) {
+      d1 = pdist2(qx, qy, qz, A.x[p1], A.y[p1], A.z[p1], A.Lx, A.Ly, A.Lz);
+      o1 = A.orig[p1];
+      s1 = (int32_t)p1;
+    }
+    ++nvis;
+  }
+#pragma unroll
+  for (int size = 2; size <= 64; size <<= 1) {
+    const bool asc = ((2 * lane) & size) == 0;  // same for both elements of the lane
+#pragma unroll
+    for (int stride = size >> 1; stride >= 1; stride >>= 1) {
+      if (stride == 1) {
+        const bool sw = asc ? key_less(d1, o1, d0, o0) : key_less(d0, o0, d1, o1);
+        if (sw) {
+          const double td = d0; d0 = d1; d1 = td;
+          const int32_t to = o0; o0 = o1; o1 = to;
+          const int32_t ts = s0; s0 = s1; s1 = ts;
+        }
+      } else {
+        const int ls = stride >> 1;  // partner lane distance
+        const double pd0 = __shfl_xor_sync(0xffffffffu, d0, ls), pd1 = __shfl_xor_sync(0xffffffffu, d1, ls);
+        const int32_t po0 = __shfl_xor_sync(0xffffffffu, o0, ls), po1 = __shfl_xor_sync(0xffffffffu, o1, ls);
+        const int32_t ps0 = __shfl_xor_sync(0xffffffffu, s0, ls), ps1 = __shfl_xor_sync(0xffffffffu, s1, ls);
+        const bool kmin = (((lane & ls) == 0) == asc);  // this lane keeps the smaller of the pair
+        if (kmin ? key_less(pd0, po0, d0, o0) : key_less(d0, o0, pd0, po0)) { d0 = pd0; o0 = po0; s0 = ps0; }
+        if (kmin ? key_less(pd1, po1, d1, o1) : key_less(d1, o1, pd1, po1)) { d1 = pd1; o1 = po1; s1 = ps1; }
+      }
+    }
+  }
+  // sorted element e sits in lane e/2, slot e%2
+  const int src = lane >> 1;
+  const double a0 = __shfl_sync(0xffffffffu, d0, src), a1 = __shfl_sync(0xffffffffu, d1, src);
+  const int32_t b0 = __shfl_sync(0xffffffffu, o0, src), b1 = __shfl_sync(0xffffffffu, o1, src);
+  const int32_t c0 = __shfl_sync(0xffffffffu, s0, src), c1 = __shfl_sync(0xffffffffu, s1, src);
+  const bool odd = lane & 1;
+  L.ld = odd ? a1 : a0;
+  L.lo = odd ? b1 : b0;
+  L.ls = odd ? c1 : c0;
+  if (lane >= A.nv) { L.ld = CUDART_INF; L.ls = -1; L.lo = INT_MAX; }
+  L.r2 = __shfl_sync(0xffffffffu, L.ld, A.nv - 1);
+}
+
 // Per-query depth-first traversal from the root, nearest child first (used
 // when a query leaf's candidate list overflows).  Leaves skip0/skip1 were
 // already scanned.
@@ -469,9 +533,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) knn_leaf_kernel(KnnArgs A
       const int64_t s = s0 + q;
       const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
       WarpList L;
-      L.ld = CUDART_INF; L.ls = -1; L.lo = INT_MAX; L.r2 = CUDART_INF;
-      leaf_insert(A, L, jl, s, qx, qy, qz, lane, nvis, nins);
-      if (jn >= 0 && jn != jl) leaf_insert(A, L, jn, s, qx, qy, qz, lane, nvis, nins);
+      init_two_leaves(A, L, jl, jn, s, qx, qy, qz, lane, nvis);
       if (overflow) {
         query_dfs(A, L, s, qx, qy, qz, lane, s_node[wib], s_bd[wib], jl, jn, nvis, nins);
       } else {

@@ -49,6 +49,8 @@ constexpr int kNT = 256;        // threads per task block
 constexpr int kIPT = 4;         // items per thread in the reorder sort
 constexpr int kChunk = kNT * kIPT;
 constexpr int kBigGroup = 96;   // groups larger than this are summed by a warp
+constexpr int kRowWarp = 32;    // saddle-row prefixes longer than this are linked by a warp
+constexpr int kMaxBigRows = 512;
 constexpr long long kMaxTaskLevels = 4000000LL;  // cap on one task's threshold levels (error, never a hang)
 
 struct Task {
@@ -91,6 +93,7 @@ struct TreeArgs {
   double* cs;             // [ng][12] per-component scratch
   int32_t* deepnode;      // [ng+1]
   int32_t* gcur;          // [ng+1] members above the group's last threshold
+  int32_t* ecur;          // [ng+1] saddle-row entries above the group's last threshold
   NodeRec* node;          // [nnodesmax+1]
   int32_t nnodesmax;
   int32_t* nnodes;        // counter
@@ -138,6 +141,30 @@ __device__ __forceinline__ int32_t count_above(const TreeArgs& A, int32_t g, dou
   return a2;
 }
 
+// number of saddle-row entries of group g above rhot (the row is sorted by
+// decreasing saddle), searched downward from the previous count like
+// count_above.
+__device__ __forceinline__ int32_t edges_above(const TreeArgs& A, int32_t g, double rhot) {
+  const double* r = A.srho + A.soff[g - 1];
+  const int32_t hi = A.ecur[g];
+  if (hi == 0 || r[hi - 1] > rhot) return hi;
+  int32_t j = hi - 1, lo = 0, step = 1;
+  while (true) {
+    const int32_t k = j - step;
+    if (k < 0) { lo = 0; break; }
+    if (r[k] > rhot) { lo = k + 1; break; }
+    j = k;
+    step <<= 1;
+  }
+  int32_t a2 = lo, b2 = j;
+  while (a2 < b2) {
+    const int32_t mid = (a2 + b2) >> 1;
+    if (r[mid] > rhot) a2 = mid + 1; else b2 = mid;
+  }
+  A.ecur[g] = a2;
+  return a2;
+}
+
 __device__ int32_t uf_find(int32_t* par, int32_t i) {
   // path halving; every chain ends at a self-parent
   for (int it = 0; it < (1 << 26); ++it) {
@@ -177,14 +204,14 @@ struct SharedTask {
   double rhot;
   double next_event;
   int32_t inode, a, b, level, ncomp, nsurv, nsisters, done, nexact, inode1, kk;
-  int32_t flag;
+  int32_t flag, nbig;
   long long iters;
 };
 
 template <class SortT, class ScanT, class MaxScanT>
 __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT::TempStorage& sort_tmp,
                                 typename ScanT::TempStorage& scan_tmp, typename MaxScanT::TempStorage& maxscan_tmp,
-                                int32_t* s_keys, long long* ph) {
+                                int32_t* s_keys, int32_t* s_big, long long* ph) {
   const int tid = threadIdx.x;
   const int32_t a = T.a, b = T.b;
   const double rhot = T.rhot;
@@ -193,7 +220,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   auto mark = [&](int k) {
     if (tid == 0) { const long long t = clock64(); ph[k] += t - tl; tl = t; }
   };
-  if (tid == 0) T.next_event = DBL_MAX;
+  if (tid == 0) { T.next_event = DBL_MAX; T.nbig = 0; }
   for (int32_t i = a + tid; i < b; i += kNT) {
     A.par[i] = i;
     A.cnt[i] = 0;
@@ -201,27 +228,51 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   }
   __syncthreads();
   mark(0);
-  // union over saddle edges above rhot (rows sorted by decreasing saddle);
-  // the next event is the smallest peak density or saddle still above rhot
+  // union over saddle edges above rhot (a prefix of each row, rows sorted by
+  // decreasing saddle).  Each undirected edge is linked once, from the row of
+  // its smaller group id; rows with more than kRowWarp such edges are linked
+  // by a whole warp afterwards.  The next event is the smallest peak density
+  // or saddle still above rhot (the last edge of each prefix).
   double ev = DBL_MAX;
   for (int32_t i = a + tid; i < b; i += kNT) {
-    int32_t g = A.GL[i];
-    double dg = A.densg[g];
+    const int32_t g = A.GL[i];
+    const double dg = A.densg[g];
     if (!(dg > rhot)) continue;
     ev = fmin(ev, dg);
-    int32_t e0 = A.soff[g - 1], e1 = A.soff[g];
-    for (int32_t e = e0; e < e1; ++e) {
-      double r = A.srho[e];
-      if (!(r > rhot)) break;
-      ev = fmin(ev, r);
-      int32_t j = A.pos_of[A.sisad[e]];
+    const int32_t e0 = A.soff[g - 1];
+    const int32_t ne = edges_above(A, g, rhot);
+    if (ne == 0) continue;
+    ev = fmin(ev, A.srho[e0 + ne - 1]);
+    if (ne > kRowWarp) {
+      const int32_t slot = atomicAdd(&T.nbig, 1);
+      if (slot < kMaxBigRows) { s_big[slot] = i; continue; }
+    }
+    for (int32_t e = e0; e < e0 + ne; ++e) {
+      const int32_t h = A.sisad[e];
+      const int32_t j = A.pos_of[h];
       if (j < a || j >= b) { set_err(A, 11, g); continue; }  // f90:1229-1233
-      uf_union(A.par, i, j);
+      if (h > g) uf_union(A.par, i, j);
     }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) ev = fmin(ev, __shfl_xor_sync(0xffffffffu, ev, o));
   if ((tid & 31) == 0 && ev < DBL_MAX) atomic_min_pos(&T.next_event, ev);
+  __syncthreads();
+  {
+    const int lane = tid & 31;
+    const int32_t nbig = min(T.nbig, kMaxBigRows);
+    for (int32_t bi = tid >> 5; bi < nbig; bi += kNT / 32) {
+      const int32_t i = s_big[bi];
+      const int32_t g = A.GL[i];
+      const int32_t e0 = A.soff[g - 1], e1 = e0 + A.ecur[g];
+      for (int32_t e = e0 + lane; e < e1; e += 32) {
+        const int32_t h = A.sisad[e];
+        const int32_t j = A.pos_of[h];
+        if (j < a || j >= b) { set_err(A, 11, g); continue; }
+        if (h > g) uf_union(A.par, i, j);
+      }
+    }
+  }
   __syncthreads();
   mark(1);
   for (int32_t i = a + tid; i < b; i += kNT) {
@@ -355,21 +406,15 @@ __device__ __forceinline__ int32_t comp_end(const TreeArgs& A, const SharedTask&
 // (9..11 hold the component's anchor while its groups' terms are formed).
 // An exact recomputation overwrites 0..9 (colour_fold).
 
-__device__ __forceinline__ int tri_and(int p, int q) {
-  if (p == 0 || q == 0) return 0;
-  if (p == 1 && q == 1) return 1;
-  return 2;
-}
-__device__ __forceinline__ int tri_or(int p, int q) {
-  if (p == 1 || q == 1) return 1;
-  if (p == 0 && q == 0) return 0;
-  return 2;
-}
-// tri-state comparison v > t with uncertainty e on v
+// Three-state outcomes as bit sets: bit 0 "can be true", bit 1 "can be
+// false" -- kTrue = 1, kFalse = 2, kUnknown = 3.  Branch-free.
+constexpr int kTrue = 1, kFalse = 2, kUnknown = 3;
+__device__ __forceinline__ int tri_and(int p, int q) { return (p & q & 1) | ((p | q) & 2); }
+__device__ __forceinline__ int tri_or(int p, int q) { return ((p | q) & 1) | (p & q & 2); }
+// v > t with v known to +-e (NaN: unknown)
 __device__ __forceinline__ int tri_gt(double v, double t, double e) {
-  if (v - e > t) return 1;
-  if (v + e <= t) return 0;
-  return 2;
+  const bool can_true = !(v + e <= t), can_false = !(v - e > t);
+  return (can_true ? 1 : 0) | (can_false ? 2 : 0);
 }
 
 // Approximate terms of the group at position i for its component's anchor
@@ -383,7 +428,7 @@ __device__ __forceinline__ void position_terms(const TreeArgs& A, int32_t i, dou
   const int32_t ng = count_above(A, g, rhot);
   double* G = A.gs + 8 * (size_t)i;
   A.gn[i] = ng;
-  double t[7] = {0, 0, 0, 0, 0, 0, 0};
+  double t[7] = {0, 0, 0, 0, 0, 0, (double)kFalse};
   if (ng > 0) {
     const double* P = A.pref + 6 * (size_t)(A.goff[g] + ng - 1);
     const int32_t pg = A.gpeak[g];
@@ -413,7 +458,7 @@ __device__ void component_decide(const TreeArgs& A, int32_t c0, int32_t c1, doub
   long long nl = 0;
   int32_t nmax = 0;
   double dmax = -1.0, S = 0, M = 0, Sx = 0, Sy = 0, Sz = 0, Q = 0;
-  int triB = 0;  // densmoy_comp_max > rhot
+  int triB = kFalse;  // densmoy_comp_max > rhot
 #pragma unroll 4
   for (int32_t i = c0 + lane; i < c1; i += 32) {
     const double* G = A.gs + 8 * (size_t)i;
@@ -456,8 +501,8 @@ __device__ void component_decide(const TreeArgs& A, int32_t c0, int32_t c1, doub
     const int tA = tri_gt(dm, thrA, edm);
     // dmax >= alphap * densmoy, densmoy known to +-edm
     const double tiny = 8.0 * u * fabs(A.alphap * dm);
-    const int tC = (dmax >= A.alphap * (dm + edm) + tiny) ? 1
-                   : (dmax < A.alphap * (dm - edm) - tiny ? 0 : 2);
+    const bool c_true = dmax >= A.alphap * (dm + edm) + tiny, c_false = dmax < A.alphap * (dm - edm) - tiny;
+    const int tC = (c_false ? 0 : 1) | (c_true ? 0 : 2);
     // radius test r >= epsilon.  The reference forms r^2 from absolute
     // coordinates (|u| <= L after the unwrap about posref), so its own value
     // carries up to ~(18n+48)u L^2 of cancellation error; these sums carry up
@@ -466,13 +511,14 @@ __device__ void component_decide(const TreeArgs& A, int32_t c0, int32_t c1, doub
     const double Lm = fmax(A.Lx, fmax(A.Ly, A.Lz));
     const double er2 = ((18.0 * n + 48.0) + 18.0 * (2.0 * n + 8.0)) * u * Lm * Lm * 1.01;
     const double e2 = A.epsilon * A.epsilon;
-    const int tD = (r2 - er2 >= e2 * (1.0 + 16.0 * u)) ? 1 : (r2 + er2 < e2 * (1.0 - 16.0 * u) ? 0 : 2);
-    const int tAB = tri_or(tA, triB);
-    dec = tri_and(tri_and(tAB, tC), tD);
+    const bool d_true = r2 - er2 >= e2 * (1.0 + 16.0 * u), d_false = r2 + er2 < e2 * (1.0 - 16.0 * u);
+    const int tD = (d_false ? 0 : 1) | (d_true ? 0 : 2);
+    const int t = tri_and(tri_and(tri_or(tA, triB), tC), tD);
+    dec = (t == kTrue) ? 1 : (t == kFalse ? 0 : 2);
     if (dec == 2) {
-      if (tAB == 2) atomicAdd(&A.stats[8], 1ULL);
-      if (tC == 2) atomicAdd(&A.stats[9], 1ULL);
-      if (tD == 2) atomicAdd(&A.stats[10], 1ULL);
+      if (tA == kUnknown) atomicAdd(&A.stats[8], 1ULL);
+      if (triB == kUnknown) atomicAdd(&A.stats[9], 1ULL);
+      if (tC == kUnknown || tD == kUnknown) atomicAdd(&A.stats[10], 1ULL);
     }
   }
   C[9] = (double)dec;
@@ -673,12 +719,17 @@ __device__ void exact_stats(const TreeArgs& A, SharedTask& T, double* s_terms) {
 // instead of one block.  Colours are connected components of the saddle graph
 // (every saddle exceeds rho_threshold), ordered by their smallest group id,
 // groups inside a colour by id -- the reference's idgroup order.
+// a warp per group: its lanes link the row's edges above rhot (the row's
+// prefix), each undirected edge from its smaller group id
 __global__ void root_union_kernel(const TreeArgs A, double rhot) {
-  const int32_t g = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int32_t g = (int32_t)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) + 1;
+  const int lane = threadIdx.x & 31;
   if (g > A.ngroups) return;
-  for (int32_t e = A.soff[g - 1]; e < A.soff[g]; ++e) {
+  const int32_t e1 = A.soff[g];
+  for (int32_t e = A.soff[g - 1] + lane; e < e1; e += 32) {
     if (!(A.srho[e] > rhot)) break;
-    uf_union(A.par, g - 1, A.sisad[e] - 1);
+    const int32_t h = A.sisad[e];
+    if (h > g) uf_union(A.par, g - 1, h - 1);
   }
 }
 
@@ -801,6 +852,7 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
   __shared__ SharedTask T;
   __shared__ long long s_clk[6];  // structural, approx, exact cycles; levels; structural passes; max ncomp
   __shared__ long long s_ph[8];   // cycles per phase of the structural passes
+  __shared__ int32_t s_big[kMaxBigRows];  // positions whose edge prefix is linked by a warp
   const int tid = threadIdx.x;
   const long long t_start = clock64();
   if (tid < 6) s_clk[tid] = 0;
@@ -822,7 +874,7 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
     __syncthreads();
     long long c0 = clock64();
     if (restructure) {
-      structural_pass<SortT, ScanT, MaxScanT>(A, T, sort_tmp, scan_tmp, maxscan_tmp, s_keys, s_ph);
+      structural_pass<SortT, ScanT, MaxScanT>(A, T, sort_tmp, scan_tmp, maxscan_tmp, s_keys, s_big, s_ph);
       if (tid == 0) { atomicAdd(&A.stats[7], 1ULL); s_clk[4] += 1; }
     }
     long long c1 = clock64();
@@ -1087,15 +1139,16 @@ __global__ void node_fold_kernel(const TreeArgs A, int32_t nn, const int32_t* __
 }
 
 // ------------------------------------------------------- setup / membership / order
-__global__ void init_groups_kernel(int32_t ng, int32_t* GL, int32_t* pos_of, int32_t* deepnode, int32_t* gcur,
-                                   const int32_t* goff) {
+__global__ void init_groups_kernel(const TreeArgs A) {
+  const int32_t ng = A.ngroups;
   int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < ng) {
-    GL[i] = i + 1;
-    pos_of[i + 1] = i;
-    gcur[i + 1] = goff[i + 2] - goff[i + 1];
+    A.GL[i] = i + 1;
+    A.pos_of[i + 1] = i;
+    A.gcur[i + 1] = A.goff[i + 2] - A.goff[i + 1];
+    A.ecur[i + 1] = A.soff[i + 1] - A.soff[i];
   }
-  if (i <= ng) deepnode[i] = 0;
+  if (i <= ng) A.deepnode[i] = 0;
 }
 
 // per-group members in decreasing density: gather keys for the segmented sort
@@ -1269,7 +1322,7 @@ int stage_nodes(Engine& E) {
   const size_t bytes_i = G * 4;
   // every sub-array starts on a 256-byte boundary: size the buffer with the rounding
   auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
-  const size_t need = r256(bytes_i) * 11 + r256(G * 8 * 8) + r256(G * 12 * 8) +
+  const size_t need = r256(bytes_i) * 12 + r256(G * 8 * 8) + r256(G * 12 * 8) +
                       r256((size_t)(nnodesmax + 1) * sizeof(Task)) * 2;
   AHOP_CUDA_TRY(E.d_tree_scratch.ensure(need));
   char* p = static_cast<char*>(E.d_tree_scratch.p);
@@ -1286,6 +1339,7 @@ int stage_nodes(Engine& E) {
   A.gn = reinterpret_cast<int32_t*>(take(bytes_i));
   A.deepnode = reinterpret_cast<int32_t*>(take(bytes_i));
   A.gcur = reinterpret_cast<int32_t*>(take(bytes_i));
+  A.ecur = reinterpret_cast<int32_t*>(take(bytes_i));
   A.gs = reinterpret_cast<double*>(take(G * 8 * 8));
   A.cs = reinterpret_cast<double*>(take(G * 12 * 8));
   Task* tasks[2];
@@ -1324,7 +1378,7 @@ int stage_nodes(Engine& E) {
   A.node = E.d_nodes.as<NodeRec>();
   A.nnodesmax = nnodesmax;
   E.launches++;
-  init_groups_kernel<<<(unsigned)((ng + 1 + T - 1) / T), T, 0, st>>>(ng, A.GL, A.pos_of, A.deepnode, A.gcur, A.goff);
+  init_groups_kernel<<<(unsigned)((ng + 1 + T - 1) / T), T, 0, st>>>(A);
   AHOP_CUDA_TRY(cudaGetLastError());
   // root node 0 (f90:934-943): mass and truemass stay 0, densmax = max peak density
   {
@@ -1344,7 +1398,7 @@ int stage_nodes(Engine& E) {
     E.launches++;
     iota_kernel<<<gb, T, 0, st>>>(A.par, ng, 0);
     E.launches++;
-    root_union_kernel<<<gb, T, 0, st>>>(A, rhot);
+    root_union_kernel<<<(unsigned)(((int64_t)ng * 32 + T - 1) / T), T, 0, st>>>(A, rhot);
     E.launches++;
     root_roots_kernel<<<gb, T, 0, st>>>(A, A.cnt, A.run);
     AHOP_CUDA_TRY(cudaGetLastError());
@@ -1402,7 +1456,7 @@ int stage_nodes(Engine& E) {
       // zero or one significant colour: the root task continues (f90:1577-1626)
       // on the general path from the initial group order
       E.launches++;
-      init_groups_kernel<<<(unsigned)((ng + 1 + T - 1) / T), T, 0, st>>>(ng, A.GL, A.pos_of, A.deepnode, A.gcur, A.goff);
+      init_groups_kernel<<<(unsigned)((ng + 1 + T - 1) / T), T, 0, st>>>(A);
       AHOP_CUDA_TRY(cudaGetLastError());
     }
   }
