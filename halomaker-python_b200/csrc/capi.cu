@@ -281,7 +281,8 @@ static void release_device(Engine& E) {
                     &E.d_gmem, &E.d_gmem_rho, &E.d_gmem_rho_pref, &E.d_sad_key, &E.d_sad_key2, &E.d_sad_val,
                     &E.d_sad_val2, &E.d_sad_cnt, &E.d_sad_keep, &E.d_sad_kpos, &E.d_flags, &E.d_soff,
                     &E.d_sisad, &E.d_srho, &E.d_nodes, &E.d_tree_scratch, &E.d_liste, &E.d_dens_orig,
-                    &E.d_rtab, &E.d_itab, &E.d_tprof, &E.d_pairs, &E.d_pair_sums, &E.d_node_aux};
+                    &E.d_rtab, &E.d_itab, &E.d_tprof, &E.d_pairs, &E.d_pair_sums, &E.d_node_aux,
+                    &E.d_forest, &E.d_moff, &E.d_misad, &E.d_mrho};
   if (E.device >= 0) cudaSetDevice(E.device);
   for (DevBuf* b : bufs) b->release();
   E.h_liste.release(); E.h_dens.release(); E.h_rtab.release(); E.h_itab.release();
@@ -336,6 +337,8 @@ int ahop_debug_tree_stats(int64_t* out, int32_t n) {
   for (int i = 0; i < n && i < 8; ++i) out[i] = (int64_t)E.tree_stats[i];
   for (int i = 8; i < n && i < 13; ++i) out[i] = (int64_t)E.knn_stats[i - 8];
   for (int i = 13; i < n && i < 16; ++i) out[i] = (int64_t)E.tree_stats[i - 5];
+  if (n > 16) out[16] = E.forest_rounds;
+  if (n > 17) out[17] = E.forest_edges;
   return AHOP_OK;
 }
 

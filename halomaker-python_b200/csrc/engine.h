@@ -82,6 +82,7 @@ struct Engine {
   cudaStream_t stream = nullptr;  // stream of the current call
   cudaEvent_t ev[16] = {};
   int32_t launches = 0, cub_calls = 0, waves = 0, hop_passes = 0;  // counters of the current compute
+  int32_t forest_rounds = 0, forest_edges = 0;                        // saddle forest of the current compute
   unsigned long long tree_stats[11] = {};                             // structure-tree kernel counters
   unsigned long long knn_stats[5] = {};                              // kNN kernel counters
   bool events_ready = false;
@@ -128,6 +129,10 @@ struct Engine {
   DevBuf d_nodes;                        // NodeRec[nnodesmax+1]
   DevBuf d_tree_scratch;
   DevBuf d_tprof;                        // per-task profile rows (debug)
+  DevBuf d_forest;                       // saddle-forest scratch
+  DevBuf d_moff, d_misad, d_mrho;        // saddle forest CSR (rows by decreasing saddle)
+  int32_t* m_isad = nullptr;             // sorted forest rows inside d_misad / d_mrho
+  double* m_rho = nullptr;
   DevBuf d_pairs;                        // (node, group) pair keys, sort double buffer
   DevBuf d_pair_sums;                    // [npairs][8] per-pair sums
   DevBuf d_node_aux;                     // per node: pair range, posref
@@ -153,6 +158,7 @@ int stage_knn_density(Engine& E);
 int stage_hop_groups(Engine& E);
 int stage_saddles(Engine& E);
 int stage_nodes(Engine& E);
+int build_saddle_forest(Engine& E);  // maximum spanning forest of the saddle rows (forest.cu)
 
 }  // namespace ahop
 

@@ -71,7 +71,7 @@ struct TreeArgs {
   const double* rdesc;    // member densities, decreasing density (same offsets)
   const double* pref;     // [nact][6] running sums in decreasing-density order:
                           // rho, m, m*dx, m*dy, m*dz, m*|d|^2 (d relative to the group peak)
-  // saddles
+  // saddle forest (maximum spanning forest of the saddle rows)
   const int32_t* soff;    // [ng+1] row g at [soff[g-1], soff[g])
   const int32_t* sisad;
   const double* srho;
@@ -1316,6 +1316,12 @@ int stage_nodes(Engine& E) {
         P.ylongs2, P.zlongs2, E.d_gmem_rho_pref.as<double>());
     AHOP_CUDA_TRY(cudaGetLastError());
   }
+  // ---- maximum spanning forest of the saddle graph: the colours at every
+  // threshold are its components, so the tree links only its edges
+  {
+    const int rc = build_saddle_forest(E);
+    if (rc) return rc;
+  }
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[11], st));
   // ---- tree scratch
   const size_t G = (size_t)ng + 1;
@@ -1370,9 +1376,9 @@ int stage_nodes(Engine& E) {
   A.gmem = E.d_gmem.as<int32_t>();
   A.rdesc = rdesc - 0;  // indexed with goff (which starts group 1 at 0)
   A.pref = E.d_gmem_rho_pref.as<double>();
-  A.soff = E.d_soff.as<int32_t>();
-  A.sisad = E.d_sisad.as<int32_t>();
-  A.srho = E.d_srho.as<double>();
+  A.soff = E.d_moff.as<int32_t>();  // forest rows (same layout as the saddle rows)
+  A.sisad = E.m_isad;
+  A.srho = E.m_rho;
   A.Lx = P.xlong; A.Ly = P.ylong; A.Lz = P.zlong; A.hx = P.xlongs2; A.hy = P.ylongs2; A.hz = P.zlongs2;
   A.fudge = P.fudge; A.alphap = P.alphap; A.epsilon = P.epsilon; A.nmembthresh = P.nmembthresh;
   A.node = E.d_nodes.as<NodeRec>();

@@ -136,7 +136,8 @@ int ahop_debug_compute_stages(const double* pos_in, const double* mass_in, int64
  * task, structural passes; [8..12] kNN -- query leaves, candidate leaves,
  * leaf visits, list insertions, leaves that fell back to per-query search;
  * [13..15] significance tests left undecided by the approximate sums, by
- * part: mean density, largest group mean density, densmax or radius. */
+ * part: mean density, largest group mean density, densmax or radius;
+ * [16..17] saddle forest: Boruvka rounds, forest edges. */
 int ahop_debug_tree_stats(int64_t* out, int32_t n);
 /* Per-task structure-tree profile (off by default; turning it on costs one
  * store per task).  Row k (16 int64) describes the task of node k: groups in
