@@ -339,6 +339,8 @@ int ahop_debug_tree_stats(int64_t* out, int32_t n) {
   for (int i = 13; i < n && i < 16; ++i) out[i] = (int64_t)E.tree_stats[i - 5];
   if (n > 16) out[16] = E.forest_rounds;
   if (n > 17) out[17] = E.forest_edges;
+  for (int i = 18; i < n && i < 21; ++i) out[i] = (int64_t)E.knn_stats[i - 13];
+  for (int i = 21; i < n && i < 26; ++i) out[i] = (int64_t)E.knn_phase[i - 21];
   return AHOP_OK;
 }
 

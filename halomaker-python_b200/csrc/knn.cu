@@ -208,6 +208,8 @@ struct KnnArgs {
   double* dens; // [n]
   int* err;     // error flag (stack overflow)
   unsigned long long* kstats;  // [0] query leaves [1] candidate leaves [2] leaf visits [3] insertions [4] overflows
+  int kdebug;   // extra counters: [5] leaves within the final radius, [6]/[7] cycles of overflow/other leaves,
+                // [24..28] phase cycles of the other leaves (bound, candidates + sort, seed lists, scan, density)
 };
 
 constexpr int kWarpsPerBlock = 8;
@@ -269,30 +271,30 @@ __device__ __forceinline__ bool key_less(double da, int32_t oa, double db, int32
   return da < db || (da == db && oa < ob);
 }
 
-// A query's first list: the nv smallest (distance, index) pairs among its own
-// leaf jl and the adjacent leaf jn, by a warp bitonic sort of the 64
-// candidates (two per lane, element 2*lane + slot) instead of up to 63
-// one-at-a-time insertions.  Empty candidates are (+inf, INT_MAX) and sort last.
-__device__ __forceinline__ void init_two_leaves(const KnnArgs& A, WarpList& L, int64_t jl, int64_t jn, int64_t self,
-                                                double qx, double qy, double qz, int lane, unsigned& nvis) {
-  double d0 = CUDART_INF, d1 = CUDART_INF;
-  int32_t o0 = INT_MAX, o1 = INT_MAX, s0 = -1, s1 = -1;
-  const int64_t p0 = jl * kLeaf + lane;
-  if (p0 < A.n && p0 != self) {
-    d0 = pdist2(qx, qy, qz, A.x[p0], A.y[p0], A.z[p0], A.Lx, A.Ly, A.Lz);
-    o0 = A.orig[p0];
-    s0 = (int32_t)p0;
+// A query's 64 seed candidates: lane l holds element l (own leaf jl, lane l)
+// and element 32 + l (adjacent leaf jn, lane l).  Empty ones are
+// (+inf, INT_MAX) and order last.
+__device__ __forceinline__ void seed_candidate(const KnnArgs& A, int64_t jl, int64_t jn, int64_t self, double qx,
+                                               double qy, double qz, int e, double& d, int32_t& o) {
+  const int64_t p = (e < 32) ? jl * kLeaf + e : jn * kLeaf + (e - 32);
+  d = CUDART_INF;
+  o = INT_MAX;
+  if ((e < 32 || (jn >= 0 && jn != jl)) && p < A.n && p != self) {
+    d = pdist2(qx, qy, qz, A.x[p], A.y[p], A.z[p], A.Lx, A.Ly, A.Lz);
+    o = A.orig[p];
   }
-  ++nvis;
-  if (jn >= 0 && jn != jl) {
-    const int64_t p1 = jn * kLeaf + lane;
-    if (p1 < A.n && p1 != self) {
-      d1 = pdist2(qx, qy, qz, A.x[p1], A.y[p1], A.z[p1], A.Lx, A.Ly, A.Lz);
-      o1 = A.orig[p1];
-      s1 = (int32_t)p1;
-    }
-    ++nvis;
-  }
+}
+
+// Sort a query's 64 seed candidates by (distance, index) with a warp bitonic
+// network (two per lane, element 2*lane + slot), write the element numbers of
+// the first 32 in order to list[0..31], and return the nv-th smallest
+// distance (+inf when fewer than nv exist) to every lane.
+__device__ __forceinline__ double seed_sort(const KnnArgs& A, int64_t jl, int64_t jn, int64_t self, double qx,
+                                           double qy, double qz, int lane, unsigned char* list) {
+  double d0, d1;
+  int32_t o0, o1, s0 = lane, s1 = 32 + lane;
+  seed_candidate(A, jl, jn, self, qx, qy, qz, lane, d0, o0);
+  seed_candidate(A, jl, jn, self, qx, qy, qz, 32 + lane, d1, o1);
 #pragma unroll
   for (int size = 2; size <= 64; size <<= 1) {
     const bool asc = ((2 * lane) & size) == 0;  // same for both elements of the lane
@@ -316,17 +318,33 @@ __device__ __forceinline__ void init_two_leaves(const KnnArgs& A, WarpList& L, i
       }
     }
   }
-  // sorted element e sits in lane e/2, slot e%2
-  const int src = lane >> 1;
-  const double a0 = __shfl_sync(0xffffffffu, d0, src), a1 = __shfl_sync(0xffffffffu, d1, src);
-  const int32_t b0 = __shfl_sync(0xffffffffu, o0, src), b1 = __shfl_sync(0xffffffffu, o1, src);
-  const int32_t c0 = __shfl_sync(0xffffffffu, s0, src), c1 = __shfl_sync(0xffffffffu, s1, src);
-  const bool odd = lane & 1;
-  L.ld = odd ? a1 : a0;
-  L.lo = odd ? b1 : b0;
-  L.ls = odd ? c1 : c0;
+  // sorted element 2*lane + slot; the first 32 are in lanes 0..15
+  if (lane < 16) {
+    list[2 * lane] = (unsigned char)s0;
+    list[2 * lane + 1] = (unsigned char)s1;
+  }
+  const int e = A.nv - 1;
+  const double a = __shfl_sync(0xffffffffu, d0, e >> 1), b = __shfl_sync(0xffffffffu, d1, e >> 1);
+  return (e & 1) ? b : a;
+}
+
+// A query's first list: the nv smallest (distance, index) pairs of its 64
+// seed candidates, rebuilt from the order seed_sort recorded (one distance
+// per lane, the same expression, so the same bits).
+__device__ __forceinline__ void seed_list(const KnnArgs& A, WarpList& L, int64_t jl, int64_t jn, int64_t self,
+                                          double qx, double qy, double qz, int lane, const unsigned char* list,
+                                          unsigned& nvis) {
+  const int e = list[lane];
+  double d;
+  int32_t o;
+  seed_candidate(A, jl, jn, self, qx, qy, qz, e, d, o);
+  const int64_t p = (e < 32) ? jl * kLeaf + e : jn * kLeaf + (e - 32);
+  L.ld = d;
+  L.lo = o;
+  L.ls = (d < CUDART_INF) ? (int32_t)p : -1;
   if (lane >= A.nv) { L.ld = CUDART_INF; L.ls = -1; L.lo = INT_MAX; }
   L.r2 = __shfl_sync(0xffffffffu, L.ld, A.nv - 1);
+  nvis += (jn >= 0 && jn != jl) ? 2 : 1;
 }
 
 // Per-query depth-first traversal from the root, nearest child first (used
@@ -416,59 +434,35 @@ __device__ __forceinline__ double boxbox_dist2(const double* __restrict__ a, con
   return dx * dx + dy * dy + dz * dz;
 }
 
-// k-th smallest (k = 1..64) of the 64 values held two per lane: warp bitonic
-// sort of (v0, v1) with element index 2*lane + slot; returns the value at
-// sorted position k-1 to every lane.
-__device__ __forceinline__ double warp_kth_of_64(double v0, double v1, int k, int lane) {
-#pragma unroll
-  for (int size = 2; size <= 64; size <<= 1) {
-#pragma unroll
-    for (int stride = size >> 1; stride >= 1; stride >>= 1) {
-      if (stride == 1) {
-        const int i0 = 2 * lane;  // pair (i0, i0+1) inside the lane
-        const bool asc = ((i0 & size) == 0);
-        const double lo = fmin(v0, v1), hi = fmax(v0, v1);
-        v0 = asc ? lo : hi;
-        v1 = asc ? hi : lo;
-      } else {
-        const int lstride = stride >> 1;
-        const double p0 = __shfl_xor_sync(0xffffffffu, v0, lstride);
-        const double p1 = __shfl_xor_sync(0xffffffffu, v1, lstride);
-        const int i0 = 2 * lane, i1 = 2 * lane + 1;
-        const bool lower = (lane & lstride) == 0;
-        const bool asc0 = ((i0 & size) == 0), asc1 = ((i1 & size) == 0);
-        v0 = (lower == asc0) ? fmin(v0, p0) : fmax(v0, p0);
-        v1 = (lower == asc1) ? fmin(v1, p1) : fmax(v1, p1);
-      }
-    }
-  }
-  const int e = k - 1;
-  const double a = __shfl_sync(0xffffffffu, v0, e >> 1);
-  const double b = __shfl_sync(0xffffffffu, v1, e >> 1);
-  return (e & 1) ? b : a;
-}
-
 constexpr int kMaxCand = 512;  // candidate leaves per query leaf (else per-query DFS)
 
 // One warp per query leaf (its 32 Morton-consecutive particles).
-//  A. every query's nv-th nearest distance among its own leaf and the
-//     adjacent leaf bounds its final kNN radius r_q; R = max_q r_q;
+//  A. every query sorts the 64 particles of its own and the adjacent leaf
+//     (the order is kept, 32 bytes per query); their nv-th distance bounds
+//     its final kNN radius r_q; R = max_q r_q;
 //  B. one traversal collects every leaf whose box lies within R of this
-//     leaf's box (candidates, nearest-first);
-//  C. each query builds its sorted list from the candidates (own leaves
-//     first), skipping leaves farther than its current nv-th distance.
+//     leaf's box, then sorts them by that box-to-box distance;
+//  C. each query starts from its seed order and scans the candidates
+//     nearest-first, skipping leaves farther than its current nv-th
+//     distance and stopping at the first whose box-to-box distance exceeds it.
 // The candidate leaves are shared by the 32 queries, so the traversal is
 // paid once per leaf and the leaf data mostly comes from L1.
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) knn_leaf_kernel(KnnArgs A) {
   __shared__ int32_t s_node[kWarpsPerBlock][kStack];
   __shared__ double s_bd[kWarpsPerBlock][kStack];
   __shared__ int32_t s_cand[kWarpsPerBlock][kMaxCand];
+  __shared__ unsigned char s_list[kWarpsPerBlock][kLeaf][32];  // each query's seed order
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
   const int64_t nleaf = A.lev_cnt[0];
   const int top = A.nlev - 1;
+  // candidate sort keys; s_bd is only used by the per-query fallback, which
+  // runs exactly when there is no candidate list
+  unsigned* s_key = reinterpret_cast<unsigned*>(s_bd[wib]);
+  static_assert(kStack * 2 >= kMaxCand, "sort keys must fit the fallback stack");
   for (int64_t jl = (int64_t)blockIdx.x * kWarpsPerBlock + wib; jl < nleaf; jl += nwarps) {
+    const long long t_leaf = clock64();
     const int64_t jn = (jl + 1 < nleaf) ? jl + 1 : jl - 1;  // adjacent leaf (jn >= 0 when nleaf >= 2)
     const int64_t s0 = jl * kLeaf;
     const int nq = (int)((A.n - s0) < kLeaf ? (A.n - s0) : (int64_t)kLeaf);
@@ -477,19 +471,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) knn_leaf_kernel(KnnArgs A
     bool ok = true;
     for (int q = 0; q < nq; ++q) {
       const int64_t s = s0 + q;
-      const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
-      const int64_t p0 = s0 + lane, p1 = jn * kLeaf + lane;
-      double v0 = CUDART_INF, v1 = CUDART_INF;
-      if (p0 < A.n && p0 != s) v0 = pdist2(qx, qy, qz, A.x[p0], A.y[p0], A.z[p0], A.Lx, A.Ly, A.Lz);
-      if (jn >= 0 && jn != jl && p1 < A.n && p1 != s) v1 = pdist2(qx, qy, qz, A.x[p1], A.y[p1], A.z[p1], A.Lx, A.Ly, A.Lz);
-      const double kth = warp_kth_of_64(v0, v1, A.nv, lane);
+      const double kth = seed_sort(A, jl, jn, s, A.x[s], A.y[s], A.z[s], lane, s_list[wib][q]);
       if (!(kth < CUDART_INF)) ok = false;  // fewer than nv others in the two leaves
       if (lane == q) Rq = kth;
     }
+    __syncwarp();
     double R2 = ok ? Rq : CUDART_INF;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) R2 = fmax(R2, __shfl_xor_sync(0xffffffffu, R2, o));
     if (!ok) R2 = CUDART_INF;
+    const long long t_a = clock64();
     // ---- B: candidate leaves within R of this leaf's box
     const double* myb = A.box + 6 * jl;
     int ncand = 0;
@@ -509,14 +500,23 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) knn_leaf_kernel(KnnArgs A
         const int64_t c = j * kFan + lane;
         const bool valid = c < A.lev_cnt[lvl - 1];
         bool cand = false;
-        if (valid) cand = boxbox_dist2(myb, A.box + 6 * (A.lev_off[lvl - 1] + c), A.Lx, A.Ly, A.Lz) <= lim;
+        double bbd = CUDART_INF;
+        if (valid) {
+          bbd = boxbox_dist2(myb, A.box + 6 * (A.lev_off[lvl - 1] + c), A.Lx, A.Ly, A.Lz);
+          cand = bbd <= lim;
+        }
         const unsigned mask = __ballot_sync(0xffffffffu, cand);
         const int cnt = __popc(mask);
         if (!cnt) continue;
         const int r = __popc(mask & ((1u << lane) - 1));
         if (lvl - 1 == 0) {
           if (ncand + cnt > kMaxCand) { overflow = true; break; }
-          if (cand) s_cand[wib][ncand + r] = (int32_t)c;
+          if (cand) {
+            // sort key: the leaf-to-leaf distance rounded down to 23 bits, then the slot
+            const unsigned fb = __float_as_uint(__double2float_rd(bbd));
+            s_key[ncand + r] = ((fb >> 8) << 9) | (unsigned)(ncand + r);
+            s_cand[wib][ncand + r] = (int32_t)c;
+          }
           ncand += cnt;
         } else {
           if (sp + cnt > kStack) { overflow = true; break; }
@@ -527,22 +527,47 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) knn_leaf_kernel(KnnArgs A
       }
       __syncwarp();
     }
+    if (!overflow) {
+      // candidates nearest-first: warp bitonic sort of the keys in shared memory
+      int N = 32;
+      while (N < ncand) N <<= 1;
+      for (int i = ncand + lane; i < N; i += 32) s_key[i] = 0xffffffffu;
+      __syncwarp();
+      for (int k = 2; k <= N; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+          for (int t = lane; t < (N >> 1); t += 32) {
+            const int i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+            const unsigned a = s_key[i], b = s_key[i + j];
+            if ((a > b) == ((i & k) == 0)) { s_key[i] = b; s_key[i + j] = a; }
+          }
+          __syncwarp();
+        }
+      }
+    }
+    const long long t_b = clock64();
+    long long c_init = 0, c_scan = 0, c_fin = 0;
     // ---- C: per-query kNN over the candidates
-    unsigned nvis = 0, nins = 0;
+    unsigned nvis = 0, nins = 0, nideal = 0;
     for (int q = 0; q < nq; ++q) {
       const int64_t s = s0 + q;
       const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
       WarpList L;
-      init_two_leaves(A, L, jl, jn, s, qx, qy, qz, lane, nvis);
+      const long long tq0 = clock64();
+      seed_list(A, L, jl, jn, s, qx, qy, qz, lane, s_list[wib][q], nvis);
+      const long long tq1 = clock64();
       if (overflow) {
         query_dfs(A, L, s, qx, qy, qz, lane, s_node[wib], s_bd[wib], jl, jn, nvis, nins);
       } else {
         for (int c0 = 0; c0 < ncand; c0 += 32) {
+          // every query lies in this leaf's box, so a candidate whose box is at
+          // least the current radius from that box (and all after it) is out
+          const double lb = (double)__uint_as_float((s_key[c0] >> 9) << 8);
+          if (lb * (1.0 - 1e-9) >= L.r2) break;
           const int ci = c0 + lane;
           int64_t leaf = -1;
           double bd = CUDART_INF;
           if (ci < ncand) {
-            leaf = s_cand[wib][ci];
+            leaf = s_cand[wib][s_key[ci] & 511u];
             if (leaf != jl && leaf != jn) bd = box_dist2(A.box + 6 * leaf, qx, qy, qz, A.Lx, A.Ly, A.Lz);
           }
           unsigned mask = __ballot_sync(0xffffffffu, bd < L.r2);
@@ -555,8 +580,34 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) knn_leaf_kernel(KnnArgs A
           }
         }
       }
+      const long long tq2 = clock64();
+      c_init += tq1 - tq0;
+      c_scan += tq2 - tq1;
+      if (A.kdebug && !overflow) {
+        // leaves that any search with these boxes must visit: box within the final radius
+        for (int c0 = 0; c0 < ncand; c0 += 32) {
+          const int ci = c0 + lane;
+          bool in = false;
+          if (ci < ncand) in = box_dist2(A.box + 6 * (int64_t)s_cand[wib][ci], qx, qy, qz, A.Lx, A.Ly, A.Lz) < L.r2;
+          nideal += __popc(__ballot_sync(0xffffffffu, in));
+        }
+      }
+      const long long tq3 = clock64();
       finish_query(A, L, s, lane);
       __syncwarp();
+      c_fin += clock64() - tq3;
+    }
+    if (lane == 0 && A.kstats && A.kdebug) {
+      unsigned long long* ph = A.kstats + 24;  // phase cycles of non-overflow leaves
+      if (!overflow) {
+        atomicAdd(&ph[0], (unsigned long long)(t_a - t_leaf));
+        atomicAdd(&ph[1], (unsigned long long)(t_b - t_a));
+        atomicAdd(&ph[2], (unsigned long long)c_init);
+        atomicAdd(&ph[3], (unsigned long long)c_scan);
+        atomicAdd(&ph[4], (unsigned long long)c_fin);
+      }
+      atomicAdd(&A.kstats[5], (unsigned long long)nideal);
+      atomicAdd(&A.kstats[overflow ? 6 : 7], (unsigned long long)(clock64() - t_leaf));
     }
     if (lane == 0 && A.kstats) {
       atomicAdd(&A.kstats[0], 1ULL);
@@ -588,10 +639,11 @@ int stage_knn_density(Engine& E) {
   A.nstore = E.nstore;
   A.nei = E.d_nei.as<int32_t>();
   A.dens = E.d_dens.as<double>();
-  AHOP_CUDA_TRY(E.d_flags.ensure(256));
-  AHOP_CUDA_TRY(cudaMemsetAsync(E.d_flags.p, 0, 256, E.stream));
+  AHOP_CUDA_TRY(E.d_flags.ensure(512));
+  AHOP_CUDA_TRY(cudaMemsetAsync(E.d_flags.p, 0, 512, E.stream));
   A.err = E.d_flags.as<int>();
   A.kstats = reinterpret_cast<unsigned long long*>(E.d_flags.as<char>() + 64);
+  A.kdebug = E.task_profile ? 1 : 0;
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, E.device);
   int per_sm = 0;
@@ -607,7 +659,9 @@ int stage_knn_density(Engine& E) {
   AHOP_CUDA_TRY(cudaGetLastError());
   int herr = 0;
   AHOP_CUDA_TRY(cudaMemcpyAsync(&herr, E.d_flags.p, 4, cudaMemcpyDeviceToHost, E.stream));
-  AHOP_CUDA_TRY(cudaMemcpyAsync(E.knn_stats, E.d_flags.as<char>() + 64, 5 * 8, cudaMemcpyDeviceToHost, E.stream));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(E.knn_stats, E.d_flags.as<char>() + 64, 8 * 8, cudaMemcpyDeviceToHost, E.stream));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(E.knn_phase, E.d_flags.as<char>() + 64 + 24 * 8, 5 * 8, cudaMemcpyDeviceToHost,
+                                E.stream));
   AHOP_CUDA_TRY(cudaStreamSynchronize(E.stream));
   if (herr) { set_error("kNN traversal stack overflow"); return AHOP_ELIMIT; }
   return AHOP_OK;

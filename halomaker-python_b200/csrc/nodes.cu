@@ -1353,7 +1353,7 @@ int stage_nodes(Engine& E) {
   tasks[1] = reinterpret_cast<Task*>(take((size_t)(nnodesmax + 1) * sizeof(Task)));
   AHOP_CUDA_TRY(E.d_nodes.ensure((size_t)(nnodesmax + 1) * sizeof(NodeRec)));
   AHOP_CUDA_TRY(cudaMemsetAsync(E.d_nodes.p, 0, (size_t)(nnodesmax + 1) * sizeof(NodeRec), st));
-  AHOP_CUDA_TRY(E.d_flags.ensure(256));
+  AHOP_CUDA_TRY(E.d_flags.ensure(512));
   AHOP_CUDA_TRY(cudaMemsetAsync(E.d_flags.p, 0, 256, st));
   int32_t* flags = E.d_flags.as<int32_t>();  // [0..1] err, [2] nnodes, [3] nnext
   A.stats = reinterpret_cast<unsigned long long*>(E.d_flags.as<char>() + 128);

@@ -137,7 +137,12 @@ int ahop_debug_compute_stages(const double* pos_in, const double* mass_in, int64
  * leaf visits, list insertions, leaves that fell back to per-query search;
  * [13..15] significance tests left undecided by the approximate sums, by
  * part: mean density, largest group mean density, densmax or radius;
- * [16..17] saddle forest: Boruvka rounds, forest edges. */
+ * [16..17] saddle forest: Boruvka rounds, forest edges; [18..20] kNN, only
+ * while the task profile is on: candidate leaves within each query's final
+ * radius, cycles spent in leaves that fell back to per-query search and in
+ * the other leaves (summed over warps), then [21..25] the cycles of those
+ * other leaves by phase: radius bound, candidate list and its sort, seed
+ * lists, candidate scan, density. */
 int ahop_debug_tree_stats(int64_t* out, int32_t n);
 /* Per-task structure-tree profile (off by default; turning it on costs one
  * store per task).  Row k (16 int64) describes the task of node k: groups in
