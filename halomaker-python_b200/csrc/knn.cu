@@ -227,43 +227,43 @@ __device__ __forceinline__ double box_dist2(const double* __restrict__ b, double
 // squared distance, sorted slot, original index; empty slots hold +inf.
 struct WarpList {
   double ld;
-  int32_t ls, lo;
+  int32_t ls;
   double r2;  // squared distance of the nv-th entry (acceptance bound)
 };
 
-__device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int64_t leaf, int64_t self, double qx,
+// Insert the particles of one leaf that belong in the list.  Candidates at
+// exactly the nv-th distance are taken in too: an exact distance tie is
+// settled by particle index, so one that does not precede the last entry
+// lands at position nv and drops out.  Particle indices are only read for
+// such ties.
+__device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int32_t leaf, int64_t self, double qx,
                                             double qy, double qz, int lane, unsigned& nvis, unsigned& nins) {
   ++nvis;
-  int64_t p = leaf * kLeaf + lane;
-  bool v = (p < A.n) && (p != self);
+  const int32_t p = leaf * kLeaf + lane;
+  const bool v = ((int64_t)p < A.n) && ((int64_t)p != self);
   double d = CUDART_INF;
-  int32_t o = INT_MAX;
-  if (v) {
-    d = pdist2(qx, qy, qz, A.x[p], A.y[p], A.z[p], A.Lx, A.Ly, A.Lz);
-    o = A.orig[p];
-  }
-  // accept d below the current nv-th distance, or equal to it with a smaller
-  // particle index: the list is the nv smallest (distance, index) pairs
-  int32_t lastk = __shfl_sync(0xffffffffu, L.lo, A.nv - 1);
-  unsigned mask = __ballot_sync(0xffffffffu, v && (d < L.r2 || (d == L.r2 && o < lastk)));
+  if (v) d = pdist2(qx, qy, qz, A.x[p], A.y[p], A.z[p], A.Lx, A.Ly, A.Lz);
+  unsigned mask = __ballot_sync(0xffffffffu, v && d <= L.r2);
   while (mask) {
     ++nins;
-    int src = __ffs(mask) - 1;
-    double cd = __shfl_sync(0xffffffffu, d, src);
-    int32_t co = __shfl_sync(0xffffffffu, o, src);
-    int32_t cs = (int32_t)(leaf * kLeaf + src);
-    bool prec = (lane < A.nv) && (L.ld < cd || (L.ld == cd && L.lo < co));
-    int pos = __popc(__ballot_sync(0xffffffffu, prec));
-    double ud = __shfl_up_sync(0xffffffffu, L.ld, 1);
-    int32_t us = __shfl_up_sync(0xffffffffu, L.ls, 1);
-    int32_t uo = __shfl_up_sync(0xffffffffu, L.lo, 1);
-    if (lane > pos) { L.ld = ud; L.ls = us; L.lo = uo; }
-    if (lane == pos) { L.ld = cd; L.ls = cs; L.lo = co; }
-    if (lane >= A.nv) { L.ld = CUDART_INF; L.ls = -1; L.lo = INT_MAX; }
+    const int src = __ffs(mask) - 1;
+    const double cd = __shfl_sync(0xffffffffu, d, src);
+    const int32_t cs = leaf * kLeaf + src;
+    bool prec = (lane < A.nv) && (L.ld < cd);
+    const bool tie = (lane < A.nv) && (L.ld == cd);
+    if (__any_sync(0xffffffffu, tie)) {
+      const int32_t co = A.orig[cs];
+      if (tie) prec = A.orig[L.ls] < co;
+    }
+    const int pos = __popc(__ballot_sync(0xffffffffu, prec));
+    const double ud = __shfl_up_sync(0xffffffffu, L.ld, 1);
+    const int32_t us = __shfl_up_sync(0xffffffffu, L.ls, 1);
+    if (lane > pos) { L.ld = ud; L.ls = us; }
+    if (lane == pos) { L.ld = cd; L.ls = cs; }
+    if (lane >= A.nv) { L.ld = CUDART_INF; L.ls = -1; }
     L.r2 = __shfl_sync(0xffffffffu, L.ld, A.nv - 1);
-    lastk = __shfl_sync(0xffffffffu, L.lo, A.nv - 1);
     mask &= ~(1u << src);
-    mask &= __ballot_sync(0xffffffffu, d < L.r2 || (d == L.r2 && o < lastk));
+    mask &= __ballot_sync(0xffffffffu, d <= L.r2);
   }
 }
 
@@ -340,9 +340,8 @@ __device__ __forceinline__ void seed_list(const KnnArgs& A, WarpList& L, int64_t
   seed_candidate(A, jl, jn, self, qx, qy, qz, e, d, o);
   const int64_t p = (e < 32) ? jl * kLeaf + e : jn * kLeaf + (e - 32);
   L.ld = d;
-  L.lo = o;
   L.ls = (d < CUDART_INF) ? (int32_t)p : -1;
-  if (lane >= A.nv) { L.ld = CUDART_INF; L.ls = -1; L.lo = INT_MAX; }
+  if (lane >= A.nv) { L.ld = CUDART_INF; L.ls = -1; }
   L.r2 = __shfl_sync(0xffffffffu, L.ld, A.nv - 1);
   nvis += (jn >= 0 && jn != jl) ? 2 : 1;
 }
@@ -447,7 +446,7 @@ constexpr int kMaxCand = 512;  // candidate leaves per query leaf (else per-quer
 //     distance and stopping at the first whose box-to-box distance exceeds it.
 // The candidate leaves are shared by the 32 queries, so the traversal is
 // paid once per leaf and the leaf data mostly comes from L1.
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) knn_leaf_kernel(KnnArgs A) {
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArgs A) {
   __shared__ int32_t s_node[kWarpsPerBlock][kStack];
   __shared__ double s_bd[kWarpsPerBlock][kStack];
   __shared__ int32_t s_cand[kWarpsPerBlock][kMaxCand];
@@ -564,18 +563,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) knn_leaf_kernel(KnnArgs A
           const double lb = (double)__uint_as_float((s_key[c0] >> 9) << 8);
           if (lb * (1.0 - 1e-9) >= L.r2) break;
           const int ci = c0 + lane;
-          int64_t leaf = -1;
+          int32_t leaf = -1;
           double bd = CUDART_INF;
           if (ci < ncand) {
             leaf = s_cand[wib][s_key[ci] & 511u];
-            if (leaf != jl && leaf != jn) bd = box_dist2(A.box + 6 * leaf, qx, qy, qz, A.Lx, A.Ly, A.Lz);
+            if (leaf != jl && leaf != jn) bd = box_dist2(A.box + 6 * (int64_t)leaf, qx, qy, qz, A.Lx, A.Ly, A.Lz);
           }
           unsigned mask = __ballot_sync(0xffffffffu, bd < L.r2);
           while (mask) {
             const int src = __ffs(mask) - 1;
             mask &= mask - 1;
             const double sbd = __shfl_sync(0xffffffffu, bd, src);
-            const int64_t sl = __shfl_sync(0xffffffffu, leaf, src);
+            const int32_t sl = __shfl_sync(0xffffffffu, leaf, src);
             if (sbd < L.r2) leaf_insert(A, L, sl, s, qx, qy, qz, lane, nvis, nins);
           }
         }
