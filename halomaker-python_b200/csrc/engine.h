@@ -80,6 +80,8 @@ struct Engine {
   Params prm;
   int device = -1;
   cudaStream_t stream = nullptr;  // stream of the current call
+  cudaStream_t stream2 = nullptr; // structure tree: large tasks run here beside the small ones
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev[16] = {};
   int32_t launches = 0, cub_calls = 0, waves = 0, hop_passes = 0;  // counters of the current compute
   int32_t forest_rounds = 0, forest_edges = 0;                        // saddle forest of the current compute

@@ -45,7 +45,10 @@
 
 namespace ahop {
 
-constexpr int kNT = 256;        // threads per task block
+constexpr int kNT = 256;        // threads per task block (grid-wide root kernels, small tasks)
+constexpr int kNTBig = 512;     // threads per block for tasks of more than kBigTask groups
+constexpr int kBigTask = 2048;
+constexpr int kTermWarps = 8;   // warps that sum large groups in an exact pass
 constexpr int kIPT = 4;         // items per thread in the reorder sort
 constexpr int kChunk = kNT * kIPT;
 constexpr int kBigGroup = 96;   // groups larger than this are summed by a warp
@@ -97,12 +100,19 @@ struct TreeArgs {
   NodeRec* node;          // [nnodesmax+1]
   int32_t nnodesmax;
   int32_t* nnodes;        // counter
-  Task* next;
+  Task* next;             // next wave's tasks of at most kBigTask groups
   int32_t* nnext;
+  Task* next_big;         // next wave's larger tasks (run by kNTBig-thread blocks)
+  int32_t* nnext_big;
   int32_t* err;           // [0] code, [1] detail
   unsigned long long* stats;  // [11] counters (see the end of tree_wave_kernel; [8..10] undecided tests)
   long long* tprof;       // [nnodesmax+1][16] per-task profile row by node id, or null
 };
+
+__device__ __forceinline__ void push_task(const TreeArgs& A, const Task& t) {
+  if (t.b - t.a > kBigTask) A.next_big[atomicAdd(A.nnext_big, 1)] = t;
+  else A.next[atomicAdd(A.nnext, 1)] = t;
+}
 
 __device__ __forceinline__ void set_err(const TreeArgs& A, int code, int detail) {
   if (atomicCAS(A.err, 0, code) == 0) A.err[1] = detail;
@@ -208,7 +218,7 @@ struct SharedTask {
   long long iters;
 };
 
-template <class SortT, class ScanT, class MaxScanT>
+template <int NT, class SortT, class ScanT, class MaxScanT>
 __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT::TempStorage& sort_tmp,
                                 typename ScanT::TempStorage& scan_tmp, typename MaxScanT::TempStorage& maxscan_tmp,
                                 int32_t* s_keys, int32_t* s_big, long long* ph) {
@@ -221,7 +231,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
     if (tid == 0) { const long long t = clock64(); ph[k] += t - tl; tl = t; }
   };
   if (tid == 0) { T.next_event = DBL_MAX; T.nbig = 0; }
-  for (int32_t i = a + tid; i < b; i += kNT) {
+  for (int32_t i = a + tid; i < b; i += NT) {
     A.par[i] = i;
     A.cnt[i] = 0;
     A.run[i] = 0;
@@ -234,7 +244,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   // by a whole warp afterwards.  The next event is the smallest peak density
   // or saddle still above rhot (the last edge of each prefix).
   double ev = DBL_MAX;
-  for (int32_t i = a + tid; i < b; i += kNT) {
+  for (int32_t i = a + tid; i < b; i += NT) {
     const int32_t g = A.GL[i];
     const double dg = A.densg[g];
     if (!(dg > rhot)) continue;
@@ -261,7 +271,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   {
     const int lane = tid & 31;
     const int32_t nbig = min(T.nbig, kMaxBigRows);
-    for (int32_t bi = tid >> 5; bi < nbig; bi += kNT / 32) {
+    for (int32_t bi = tid >> 5; bi < nbig; bi += NT / 32) {
       const int32_t i = s_big[bi];
       const int32_t g = A.GL[i];
       const int32_t e0 = A.soff[g - 1], e1 = e0 + A.ecur[g];
@@ -275,7 +285,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   }
   __syncthreads();
   mark(1);
-  for (int32_t i = a + tid; i < b; i += kNT) {
+  for (int32_t i = a + tid; i < b; i += NT) {
     int32_t g = A.GL[i];
     if (A.densg[g] > rhot) {
       int32_t r = uf_find(A.par, i);
@@ -289,7 +299,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   mark(2);
   // exclusive scan of component sizes over root positions -> component offsets (in cnt)
   int32_t carry = 0;
-  for (int32_t c0 = a; c0 < b; c0 += kNT) {
+  for (int32_t c0 = a; c0 < b; c0 += NT) {
     int32_t i = c0 + tid;
     int32_t v = (i < b) ? A.cnt[i] : 0;
     int32_t ex, tot;
@@ -306,7 +316,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   // head (block max-scan of head indices); run[] carries ranks across chunks
   const int32_t sent = b - a;  // key of dropped groups, above every root offset
   const int kbits = 32 - __clz(sent);
-  for (int32_t c0 = a; c0 < b; c0 += kChunk) {
+  for (int32_t c0 = a; c0 < b; c0 += (NT * kIPT)) {
     int32_t keys[kIPT], vals[kIPT];
 #pragma unroll
     for (int k = 0; k < kIPT; ++k) {
@@ -331,7 +341,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
 #pragma unroll
     for (int k = 0; k < kIPT; ++k) {
       int q = tid * kIPT + k;
-      tail[k] = (q == kChunk - 1) || (s_keys[q + 1] != keys[k]);
+      tail[k] = (q == (NT * kIPT) - 1) || (s_keys[q + 1] != keys[k]);
       if (keys[k] == sent) continue;
       int32_t r = keys[k] + a;
       int32_t np = a + A.cnt[r] + A.run[r] + (q - headq[k]);
@@ -348,7 +358,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   }
   mark(4);
   // copy back, positions, component starts
-  for (int32_t i = a + tid; i < a + nsurv; i += kNT) {
+  for (int32_t i = a + tid; i < a + nsurv; i += NT) {
     int32_t g = A.GL2[i];
     A.GL[i] = g;
     A.pos_of[g] = i;
@@ -358,7 +368,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   // component starts: root positions r (par[r] == r before reorder) map to start a + cnt[r]
   // collect them in order with a scan over root flags
   carry = 0;
-  for (int32_t c0 = a; c0 < b; c0 += kNT) {
+  for (int32_t c0 = a; c0 < b; c0 += NT) {
     int32_t i = c0 + tid;
     int32_t isroot = (i < b && A.par[i] == i) ? 1 : 0;
     int32_t ex, tot;
@@ -377,12 +387,12 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   }
   // component index of every surviving position: inclusive scan of the
   // component-start flags (run[] is free after the reorder)
-  for (int32_t i = a + tid; i < a + nsurv; i += kNT) A.run[i] = 0;
+  for (int32_t i = a + tid; i < a + nsurv; i += NT) A.run[i] = 0;
   __syncthreads();
-  for (int32_t k = tid; k < ncomp; k += kNT) A.run[A.cstart[a + k]] = 1;
+  for (int32_t k = tid; k < ncomp; k += NT) A.run[A.cstart[a + k]] = 1;
   __syncthreads();
   carry = 0;
-  for (int32_t c0 = a; c0 < a + nsurv; c0 += kNT) {
+  for (int32_t c0 = a; c0 < a + nsurv; c0 += NT) {
     const int32_t i = c0 + tid;
     const int32_t v = (i < a + nsurv) ? A.run[i] : 0;
     int32_t inc, tot;
@@ -528,11 +538,12 @@ __device__ void component_decide(const TreeArgs& A, int32_t c0, int32_t c1, doub
 // Approximate statistics of every component of the task: anchors, then the
 // groups' terms position-parallel over the whole block, then a warp per
 // component sums them and decides.
+template <int NT>
 __device__ void approx_stats(const TreeArgs& A, SharedTask& T) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const double rhot = T.rhot;
   const int32_t a = T.a, b = T.b, ncomp = T.ncomp;
-  for (int32_t k = tid; k < ncomp; k += kNT) {
+  for (int32_t k = tid; k < ncomp; k += NT) {
     const int32_t p0 = A.gpeak[A.GL[A.cstart[a + k]]];
     double* C = A.cs + 12 * (size_t)(a + k);
     C[9] = A.x[p0];
@@ -540,9 +551,9 @@ __device__ void approx_stats(const TreeArgs& A, SharedTask& T) {
     C[11] = A.z[p0];
   }
   __syncthreads();
-  for (int32_t i = a + tid; i < b; i += kNT) position_terms(A, i, rhot, A.cs + 12 * (size_t)(a + A.compidx[i]) + 9);
+  for (int32_t i = a + tid; i < b; i += NT) position_terms(A, i, rhot, A.cs + 12 * (size_t)(a + A.compidx[i]) + 9);
   __syncthreads();
-  for (int32_t k = warp; k < ncomp; k += kNT / 32)
+  for (int32_t k = warp; k < ncomp; k += NT / 32)
     component_decide(A, A.cstart[a + k], comp_end(A, T, k), rhot, A.cs + 12 * (size_t)(a + k), lane);
   __syncthreads();
 }
@@ -678,17 +689,18 @@ __device__ void colour_fold(const TreeArgs& A, int32_t c0, int32_t c1, double rh
 }
 
 // Exact sums in the reference order for the colours flagged in cs[..][10].
+template <int NT>
 __device__ void exact_stats(const TreeArgs& A, SharedTask& T, double* s_terms) {
   const int tid = threadIdx.x;
   const double rhot = T.rhot;
-  for (int32_t k = tid; k < T.ncomp; k += kNT) {
+  for (int32_t k = tid; k < T.ncomp; k += NT) {
     double* C = A.cs + 12 * (size_t)(T.a + k);
     if (C[10] == 0.0) continue;
     C[11] = (double)colour_posref(A, A.GL[A.cstart[T.a + k]], rhot);
   }
   __syncthreads();
   const int lane = tid & 31, warp = tid >> 5;
-  for (int32_t i = T.a + warp; i < T.b; i += kNT / 32) {  // large groups: a warp each
+  for (int32_t i = T.a + warp; warp < kTermWarps && i < T.b; i += kTermWarps) {  // large groups: a warp each
     const double* C = A.cs + 12 * (size_t)(T.a + A.compidx[i]);
     if (C[10] == 0.0) continue;
     const int32_t g = A.GL[i];
@@ -696,7 +708,7 @@ __device__ void exact_stats(const TreeArgs& A, SharedTask& T, double* s_terms) {
     const int32_t ref = (int32_t)C[11];
     group_sums_warp(A, g, rhot, A.x[ref], A.y[ref], A.z[ref], A.gs + 8 * (size_t)i, s_terms + warp * 32 * 6, lane);
   }
-  for (int32_t i = T.a + tid; i < T.b; i += kNT) {  // small groups: a thread each
+  for (int32_t i = T.a + tid; i < T.b; i += NT) {  // small groups: a thread each
     const double* C = A.cs + 12 * (size_t)(T.a + A.compidx[i]);
     if (C[10] == 0.0) continue;
     const int32_t g = A.GL[i];
@@ -705,7 +717,7 @@ __device__ void exact_stats(const TreeArgs& A, SharedTask& T, double* s_terms) {
     group_sums_thread(A, g, rhot, A.x[ref], A.y[ref], A.z[ref], A.gs + 8 * (size_t)i);
   }
   __syncthreads();
-  for (int32_t k = tid; k < T.ncomp; k += kNT) {
+  for (int32_t k = tid; k < T.ncomp; k += NT) {
     double* C = A.cs + 12 * (size_t)(T.a + k);
     if (C[10] == 0.0) continue;
     colour_fold(A, A.cstart[T.a + k], comp_end(A, T, k), rhot, C);
@@ -814,7 +826,7 @@ __global__ void root_okflag_kernel(const TreeArgs A, int32_t ncomp, int32_t* fla
 // level-1 nodes in colour order (reserve_nodes_block gives 1..nsisters),
 // child tasks (f90:1484-1571), deepest node per group
 __global__ void root_nodes_kernel(const TreeArgs A, int32_t ncomp, const int32_t* flag, const int32_t* rank,
-                                  int32_t nsisters, double rhot, Task* next) {
+                                  int32_t nsisters, double rhot) {
   const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= ncomp || !flag[k]) return;
   const double* C = A.cs + 12 * (size_t)k;
@@ -831,7 +843,7 @@ __global__ void root_nodes_kernel(const TreeArgs A, int32_t ncomp, const int32_t
   nd.firstchild = 0;
   if (nd.mass == 0) set_err(A, 15, io);
   const int32_t c0 = A.cstart[k], c1 = (k + 1 < ncomp) ? A.cstart[k + 1] : A.ngroups;
-  next[is] = Task{xmul(rhot, xadd(1.0, xdiv(A.fudge, xsqrt(C[1])))), io, c0, c1, 1};
+  push_task(A, Task{xmul(rhot, xadd(1.0, xdiv(A.fudge, xsqrt(C[1])))), io, c0, c1, 1});
   if (is == nsisters - 1) A.node[0].firstchild = io;  // f90:1540
 }
 
@@ -842,13 +854,16 @@ __global__ void root_deepnode_kernel(const TreeArgs A, const int32_t* flag, cons
   if (flag[k]) A.deepnode[A.GL[i]] = 1 + rank[k];
 }
 
-template <class SortT, class ScanT, class MaxScanT>
-__global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* __restrict__ tasks) {
+template <int NT>
+__global__ void __launch_bounds__(NT) tree_wave_kernel(TreeArgs A, const Task* __restrict__ tasks) {
+  using SortT = cub::BlockRadixSort<int32_t, NT, kIPT, int32_t>;
+  using ScanT = cub::BlockScan<int32_t, NT>;
+  using MaxScanT = cub::BlockScan<int32_t, NT>;
   __shared__ typename SortT::TempStorage sort_tmp;
   __shared__ typename ScanT::TempStorage scan_tmp;
   __shared__ typename MaxScanT::TempStorage maxscan_tmp;
-  __shared__ int32_t s_keys[kChunk];
-  __shared__ double s_terms[kNT / 32 * 32 * 6];
+  __shared__ int32_t s_keys[NT * kIPT];
+  __shared__ double s_terms[kTermWarps * 32 * 6];
   __shared__ SharedTask T;
   __shared__ long long s_clk[6];  // structural, approx, exact cycles; levels; structural passes; max ncomp
   __shared__ long long s_ph[8];   // cycles per phase of the structural passes
@@ -874,7 +889,7 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
     __syncthreads();
     long long c0 = clock64();
     if (restructure) {
-      structural_pass<SortT, ScanT, MaxScanT>(A, T, sort_tmp, scan_tmp, maxscan_tmp, s_keys, s_big, s_ph);
+      structural_pass<NT, SortT, ScanT, MaxScanT>(A, T, sort_tmp, scan_tmp, maxscan_tmp, s_keys, s_big, s_ph);
       if (tid == 0) { atomicAdd(&A.stats[7], 1ULL); s_clk[4] += 1; }
     }
     long long c1 = clock64();
@@ -883,7 +898,7 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
       if (tid == 0) A.node[T.inode].firstchild = 0;
       break;
     }
-    approx_stats(A, T);
+    approx_stats<NT>(A, T);
     if (tid == 0) {
       s_clk[1] += clock64() - c1;
       T.nexact = 0;
@@ -891,15 +906,15 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
       T.kk = -1;
     }
     __syncthreads();
-    for (int32_t k = tid; k < T.ncomp; k += kNT)
+    for (int32_t k = tid; k < T.ncomp; k += NT)
       if (A.cs[12 * (size_t)(T.a + k) + 10] != 0.0) atomicAdd(&T.nexact, 1);
     __syncthreads();
     if (T.nexact > 0) {  // undecided tests: exact sums in the reference order
       long long c2 = clock64();
-      exact_stats(A, T, s_terms);
+      exact_stats<NT>(A, T, s_terms);
       if (tid == 0) { s_clk[2] += clock64() - c2; atomicAdd(&A.stats[4], 1ULL); }
     }
-    for (int32_t k = tid; k < T.ncomp; k += kNT) {
+    for (int32_t k = tid; k < T.ncomp; k += NT) {
       if (A.cs[12 * (size_t)(T.a + k) + 9] == 1.0) {
         atomicAdd(&T.nsisters, 1);
         T.kk = k;  // the significant component when there is exactly one
@@ -943,7 +958,7 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
     if (T.done) break;
     {
       int32_t carry = 0;
-      for (int32_t k0 = 0; k0 < T.ncomp; k0 += kNT) {
+      for (int32_t k0 = 0; k0 < T.ncomp; k0 += NT) {
         const int32_t k = k0 + tid;
         const double* C = A.cs + 12 * (size_t)(T.a + k);
         const int sig = (k < T.ncomp && C[9] == 1.0) ? 1 : 0;
@@ -966,8 +981,7 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
           if (nd.mass == 0) set_err(A, 15, io);  // f90:1506-1510
           // child task (f90:1543-1556)
           const double rc = xmul(T.rhot, xadd(1.0, xdiv(A.fudge, xsqrt(C[1]))));
-          const int32_t slot = atomicAdd(A.nnext, 1);
-          A.next[slot] = Task{rc, io, A.cstart[T.a + k], comp_end(A, T, k), T.level + 1};
+          push_task(A, Task{rc, io, A.cstart[T.a + k], comp_end(A, T, k), T.level + 1});
         }
         carry += tot;
       }
@@ -975,7 +989,7 @@ __global__ void __launch_bounds__(kNT) tree_wave_kernel(TreeArgs A, const Task* 
     if (tid == 0) A.node[T.inode].firstchild = T.inode1 + ns - 1;  // f90:1540
     __syncthreads();
     // deepest node per group
-    for (int32_t i = T.a + tid; i < T.b; i += kNT) {
+    for (int32_t i = T.a + tid; i < T.b; i += NT) {
       const int32_t io = A.cnt[T.a + A.compidx[i]];
       if (io > 0) A.deepnode[A.GL[i]] = io;
     }
@@ -1329,7 +1343,7 @@ int stage_nodes(Engine& E) {
   // every sub-array starts on a 256-byte boundary: size the buffer with the rounding
   auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
   const size_t need = r256(bytes_i) * 12 + r256(G * 8 * 8) + r256(G * 12 * 8) +
-                      r256((size_t)(nnodesmax + 1) * sizeof(Task)) * 2;
+                      r256((size_t)(nnodesmax + 1) * sizeof(Task)) * 4;
   AHOP_CUDA_TRY(E.d_tree_scratch.ensure(need));
   char* p = static_cast<char*>(E.d_tree_scratch.p);
   auto take = [&](size_t b) { char* q = p; p += (b + 255) & ~size_t(255); return q; };
@@ -1348,14 +1362,17 @@ int stage_nodes(Engine& E) {
   A.ecur = reinterpret_cast<int32_t*>(take(bytes_i));
   A.gs = reinterpret_cast<double*>(take(G * 8 * 8));
   A.cs = reinterpret_cast<double*>(take(G * 12 * 8));
-  Task* tasks[2];
+  Task* tasks[2];   // tasks of at most kBigTask groups, by wave parity
+  Task* tasksB[2];  // larger tasks
   tasks[0] = reinterpret_cast<Task*>(take((size_t)(nnodesmax + 1) * sizeof(Task)));
   tasks[1] = reinterpret_cast<Task*>(take((size_t)(nnodesmax + 1) * sizeof(Task)));
+  tasksB[0] = reinterpret_cast<Task*>(take((size_t)(nnodesmax + 1) * sizeof(Task)));
+  tasksB[1] = reinterpret_cast<Task*>(take((size_t)(nnodesmax + 1) * sizeof(Task)));
   AHOP_CUDA_TRY(E.d_nodes.ensure((size_t)(nnodesmax + 1) * sizeof(NodeRec)));
   AHOP_CUDA_TRY(cudaMemsetAsync(E.d_nodes.p, 0, (size_t)(nnodesmax + 1) * sizeof(NodeRec), st));
   AHOP_CUDA_TRY(E.d_flags.ensure(512));
   AHOP_CUDA_TRY(cudaMemsetAsync(E.d_flags.p, 0, 256, st));
-  int32_t* flags = E.d_flags.as<int32_t>();  // [0..1] err, [2] nnodes, [3] nnext
+  int32_t* flags = E.d_flags.as<int32_t>();  // [0..1] err, [2] nnodes, [3] nnext, [4] nnext_big
   A.stats = reinterpret_cast<unsigned long long*>(E.d_flags.as<char>() + 128);
   A.tprof = nullptr;
   if (E.task_profile) {
@@ -1366,6 +1383,7 @@ int stage_nodes(Engine& E) {
   A.err = flags;
   A.nnodes = flags + 2;
   A.nnext = flags + 3;
+  A.nnext_big = flags + 4;
   A.x = E.d_x.as<double>(); A.y = E.d_y.as<double>(); A.z = E.d_z.as<double>(); A.m = E.d_m.as<double>();
   A.dens = E.d_dens.as<double>();
   A.orig = E.d_orig.as<int32_t>();
@@ -1387,14 +1405,13 @@ int stage_nodes(Engine& E) {
   init_groups_kernel<<<(unsigned)((ng + 1 + T - 1) / T), T, 0, st>>>(A);
   AHOP_CUDA_TRY(cudaGetLastError());
   // root node 0 (f90:934-943): mass and truemass stay 0, densmax = max peak density
+  int32_t nsmall = 0, nbig = 0;
   {
-    Task root{P.rho_threshold, 0, 0, ng, 0};
-    AHOP_CUDA_TRY(cudaMemcpyAsync(tasks[0], &root, sizeof(Task), cudaMemcpyHostToDevice, st));
+    const Task root{P.rho_threshold, 0, 0, ng, 0};
+    const bool big = ng > kBigTask;
+    AHOP_CUDA_TRY(cudaMemcpyAsync(big ? tasksB[0] : tasks[0], &root, sizeof(Task), cudaMemcpyHostToDevice, st));
+    (big ? nbig : nsmall) = 1;
   }
-  using SortT = cub::BlockRadixSort<int32_t, kNT, kIPT, int32_t>;
-  using ScanT = cub::BlockScan<int32_t, kNT>;
-  using MaxScanT = cub::BlockScan<int32_t, kNT>;
-  int32_t ntasks = 1;
   int cur = 0;
   int32_t* h = reinterpret_cast<int32_t*>(E.h_scalars);
   // ---- root level on the whole grid
@@ -1449,14 +1466,20 @@ int stage_nodes(Engine& E) {
     const int32_t nsis = h[4];
     if (nsis >= 2) {
       // the root branches at once (the usual case): level-1 nodes 1..nsis
+      A.next = tasks[1];
+      A.next_big = tasksB[1];
+      AHOP_CUDA_TRY(cudaMemsetAsync(A.nnext, 0, 8, st));
       E.launches++;
-      root_nodes_kernel<<<(unsigned)((ncomp + T - 1) / T), T, 0, st>>>(A, ncomp, A.cnt, A.run, nsis, rhot,
-                                                                       tasks[1]);
+      root_nodes_kernel<<<(unsigned)((ncomp + T - 1) / T), T, 0, st>>>(A, ncomp, A.cnt, A.run, nsis, rhot);
       E.launches++;
       root_deepnode_kernel<<<gb, T, 0, st>>>(A, A.cnt, A.run);
       AHOP_CUDA_TRY(cudaGetLastError());
-      AHOP_CUDA_TRY(cudaMemcpyAsync(A.nnodes, &nsis, 4, cudaMemcpyHostToDevice, st));
-      ntasks = nsis;
+      h[5] = nsis;
+      AHOP_CUDA_TRY(cudaMemcpyAsync(A.nnodes, h + 5, 4, cudaMemcpyHostToDevice, st));
+      AHOP_CUDA_TRY(cudaMemcpyAsync(h, flags, 20, cudaMemcpyDeviceToHost, st));
+      AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+      nsmall = h[3];
+      nbig = h[4];
       cur = 1;
     } else {
       // zero or one significant colour: the root task continues (f90:1577-1626)
@@ -1467,21 +1490,41 @@ int stage_nodes(Engine& E) {
     }
   }
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[12], st));
-  for (int wave = 0; ntasks > 0; ++wave) {
+  // Waves: small tasks on the compute stream, large ones (the critical path)
+  // in wider blocks on a second stream at the same time.
+  if (!E.stream2) {
+    AHOP_CUDA_TRY(cudaStreamCreateWithFlags(&E.stream2, cudaStreamNonBlocking));
+    AHOP_CUDA_TRY(cudaEventCreateWithFlags(&E.ev_fork, cudaEventDisableTiming));
+    AHOP_CUDA_TRY(cudaEventCreateWithFlags(&E.ev_join, cudaEventDisableTiming));
+  }
+  for (int wave = 0; nsmall + nbig > 0; ++wave) {
     if (wave > 100000) { set_error("structure tree: too many waves"); return AHOP_ELIMIT; }
     A.next = tasks[cur ^ 1];
-    AHOP_CUDA_TRY(cudaMemsetAsync(A.nnext, 0, 4, st));
-    E.launches++;
-    tree_wave_kernel<SortT, ScanT, MaxScanT><<<ntasks, kNT, 0, st>>>(A, tasks[cur]);
-    AHOP_CUDA_TRY(cudaGetLastError());
-    AHOP_CUDA_TRY(cudaMemcpyAsync(h, flags, 16, cudaMemcpyDeviceToHost, st));
+    A.next_big = tasksB[cur ^ 1];
+    AHOP_CUDA_TRY(cudaMemsetAsync(A.nnext, 0, 8, st));
+    if (nbig > 0) {
+      AHOP_CUDA_TRY(cudaEventRecord(E.ev_fork, st));
+      AHOP_CUDA_TRY(cudaStreamWaitEvent(E.stream2, E.ev_fork, 0));
+      E.launches++;
+      tree_wave_kernel<kNTBig><<<nbig, kNTBig, 0, E.stream2>>>(A, tasksB[cur]);
+      AHOP_CUDA_TRY(cudaGetLastError());
+      AHOP_CUDA_TRY(cudaEventRecord(E.ev_join, E.stream2));
+    }
+    if (nsmall > 0) {
+      E.launches++;
+      tree_wave_kernel<kNT><<<nsmall, kNT, 0, st>>>(A, tasks[cur]);
+      AHOP_CUDA_TRY(cudaGetLastError());
+    }
+    if (nbig > 0) AHOP_CUDA_TRY(cudaStreamWaitEvent(st, E.ev_join, 0));
+    AHOP_CUDA_TRY(cudaMemcpyAsync(h, flags, 20, cudaMemcpyDeviceToHost, st));
     AHOP_CUDA_TRY(cudaStreamSynchronize(st));
     if (h[0] != 0) {
       set_error("structure tree invariant failed (code " + std::to_string(h[0]) + ", detail " +
                 std::to_string(h[1]) + ")");
       return h[0] == 12 ? AHOP_ELIMIT : AHOP_EINVARIANT;
     }
-    ntasks = h[3];
+    nsmall = h[3];
+    nbig = h[4];
     cur ^= 1;
     E.waves = wave + 1;
   }
