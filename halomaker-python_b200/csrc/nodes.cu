@@ -46,10 +46,11 @@
 namespace ahop {
 
 constexpr int kNT = 256;        // threads per task block (grid-wide root kernels, small tasks)
-constexpr int kNTBig = 512;     // threads per block for tasks of more than kBigTask groups
+constexpr int kNTBig = 1024;    // threads per block for tasks of more than kBigTask groups
 constexpr int kBigTask = 2048;
 constexpr int kTermWarps = 8;   // warps that sum large groups in an exact pass
-constexpr int kIPT = 4;         // items per thread in the reorder sort
+constexpr int kIPT = 4;         // items per thread in the reorder sort (2 for 1024-thread blocks)
+__host__ __device__ constexpr int ipt_for(int nt) { return nt >= 1024 ? 2 : kIPT; }
 constexpr int kChunk = kNT * kIPT;
 constexpr int kBigGroup = 96;   // groups larger than this are summed by a warp
 constexpr int kRowWarp = 32;    // saddle-row prefixes longer than this are linked by a warp
@@ -222,6 +223,7 @@ template <int NT, class SortT, class ScanT, class MaxScanT>
 __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT::TempStorage& sort_tmp,
                                 typename ScanT::TempStorage& scan_tmp, typename MaxScanT::TempStorage& maxscan_tmp,
                                 int32_t* s_keys, int32_t* s_big, long long* ph) {
+  constexpr int IPT = ipt_for(NT);
   const int tid = threadIdx.x;
   const int32_t a = T.a, b = T.b;
   const double rhot = T.rhot;
@@ -316,11 +318,11 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   // head (block max-scan of head indices); run[] carries ranks across chunks
   const int32_t sent = b - a;  // key of dropped groups, above every root offset
   const int kbits = 32 - __clz(sent);
-  for (int32_t c0 = a; c0 < b; c0 += (NT * kIPT)) {
-    int32_t keys[kIPT], vals[kIPT];
+  for (int32_t c0 = a; c0 < b; c0 += (NT * IPT)) {
+    int32_t keys[IPT], vals[IPT];
 #pragma unroll
-    for (int k = 0; k < kIPT; ++k) {
-      int32_t i = c0 + tid * kIPT + k;
+    for (int k = 0; k < IPT; ++k) {
+      int32_t i = c0 + tid * IPT + k;
       int32_t r = (i < b) ? A.par[i] : -1;
       keys[k] = (r >= 0) ? (r - a) : sent;
       vals[k] = i;
@@ -328,20 +330,20 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
     SortT(sort_tmp).Sort(keys, vals, 0, kbits);
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < kIPT; ++k) s_keys[tid * kIPT + k] = keys[k];
+    for (int k = 0; k < IPT; ++k) s_keys[tid * IPT + k] = keys[k];
     __syncthreads();
-    int32_t headq[kIPT];
+    int32_t headq[IPT];
 #pragma unroll
-    for (int k = 0; k < kIPT; ++k) {
-      int q = tid * kIPT + k;
+    for (int k = 0; k < IPT; ++k) {
+      int q = tid * IPT + k;
       headq[k] = (q == 0 || s_keys[q - 1] != keys[k]) ? q : 0;
     }
     MaxScanT(maxscan_tmp).InclusiveScan(headq, headq, cub::Max());
-    bool tail[kIPT];
+    bool tail[IPT];
 #pragma unroll
-    for (int k = 0; k < kIPT; ++k) {
-      int q = tid * kIPT + k;
-      tail[k] = (q == (NT * kIPT) - 1) || (s_keys[q + 1] != keys[k]);
+    for (int k = 0; k < IPT; ++k) {
+      int q = tid * IPT + k;
+      tail[k] = (q == (NT * IPT) - 1) || (s_keys[q + 1] != keys[k]);
       if (keys[k] == sent) continue;
       int32_t r = keys[k] + a;
       int32_t np = a + A.cnt[r] + A.run[r] + (q - headq[k]);
@@ -350,8 +352,8 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < kIPT; ++k) {
-      int q = tid * kIPT + k;
+    for (int k = 0; k < IPT; ++k) {
+      int q = tid * IPT + k;
       if (tail[k] && keys[k] != sent) A.run[keys[k] + a] += q - headq[k] + 1;
     }
     __syncthreads();
@@ -854,20 +856,27 @@ __global__ void root_deepnode_kernel(const TreeArgs A, const int32_t* flag, cons
   if (flag[k]) A.deepnode[A.GL[i]] = 1 + rank[k];
 }
 
+// Dynamic shared memory of a task block: exact-sum staging (kTermWarps warps),
+// reorder keys, warp-linked row positions.
+__host__ __device__ constexpr size_t wave_dyn_smem(int nt) {
+  return (size_t)kTermWarps * 32 * 6 * 8 + (size_t)nt * ipt_for(nt) * 4 + (size_t)kMaxBigRows * 4;
+}
+
 template <int NT>
-__global__ void __launch_bounds__(NT) tree_wave_kernel(TreeArgs A, const Task* __restrict__ tasks) {
-  using SortT = cub::BlockRadixSort<int32_t, NT, kIPT, int32_t>;
+__global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeArgs A, const Task* __restrict__ tasks) {
+  using SortT = cub::BlockRadixSort<int32_t, NT, ipt_for(NT), int32_t>;
   using ScanT = cub::BlockScan<int32_t, NT>;
   using MaxScanT = cub::BlockScan<int32_t, NT>;
   __shared__ typename SortT::TempStorage sort_tmp;
   __shared__ typename ScanT::TempStorage scan_tmp;
   __shared__ typename MaxScanT::TempStorage maxscan_tmp;
-  __shared__ int32_t s_keys[NT * kIPT];
-  __shared__ double s_terms[kTermWarps * 32 * 6];
+  extern __shared__ __align__(16) unsigned char wave_dyn[];
+  double* s_terms = reinterpret_cast<double*>(wave_dyn);
+  int32_t* s_keys = reinterpret_cast<int32_t*>(wave_dyn + (size_t)kTermWarps * 32 * 6 * 8);
+  int32_t* s_big = s_keys + NT * ipt_for(NT);
   __shared__ SharedTask T;
   __shared__ long long s_clk[6];  // structural, approx, exact cycles; levels; structural passes; max ncomp
   __shared__ long long s_ph[8];   // cycles per phase of the structural passes
-  __shared__ int32_t s_big[kMaxBigRows];  // positions whose edge prefix is linked by a warp
   const int tid = threadIdx.x;
   const long long t_start = clock64();
   if (tid < 6) s_clk[tid] = 0;
@@ -1120,23 +1129,47 @@ __global__ void __launch_bounds__(256) pair_sums_warp_kernel(const TreeArgs A,
 }
 
 // fold every node's pair sums in ascending group id and write its fields
-// (f90:1407-1432, 1511-1538)
-__global__ void node_fold_kernel(const TreeArgs A, int32_t nn, const int32_t* __restrict__ nstart,
-                                 const int32_t* __restrict__ nend, const double* __restrict__ ps) {
-  const int32_t N = blockIdx.x * blockDim.x + threadIdx.x + 1;
+// (f90:1407-1432, 1511-1538).  A warp per node: the lanes stage 32 pairs at
+// a time in shared memory and lanes 0..5 each run one of the six sequential
+// sums (lane 6 the member count) -- the fold's additions in the fold's order.
+__global__ void __launch_bounds__(256) node_fold_kernel(const TreeArgs A, int32_t nn,
+                                                        const int32_t* __restrict__ nstart,
+                                                        const int32_t* __restrict__ nend,
+                                                        const double* __restrict__ ps) {
+  __shared__ double st[8][32 * 7];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int32_t N = (int32_t)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) + 1;
   if (N > nn) return;
-  double posg0 = 0, posg1 = 0, posg2 = 0, tm = 0, rsg = 0, dmg = 0;
+  // pair-sum columns of the six chains: posg(3), rsquare, truemass, densmoy
+  const int col = (lane == 0) ? 2 : (lane == 1) ? 3 : (lane == 2) ? 4 : (lane == 3) ? 5 : (lane == 4) ? 1 : 6;
+  double acc = 0.0;
   int32_t ml = 0;
-  for (int32_t p = nstart[N]; p < nend[N]; ++p) {
-    const double* G = ps + 8 * (size_t)p;
-    posg0 = xadd(posg0, G[2]);
-    posg1 = xadd(posg1, G[3]);
-    posg2 = xadd(posg2, G[4]);
-    rsg = xadd(rsg, G[5]);
-    ml += (int32_t)G[0];
-    tm = xadd(tm, G[1]);
-    dmg = xadd(dmg, G[6]);
+  const int32_t p0 = nstart[N], p1 = nend[N];
+  for (int32_t base = p0; base < p1; base += 32) {
+    const int32_t p = base + lane;
+    if (p < p1) {
+      const double* G = ps + 8 * (size_t)p;
+#pragma unroll
+      for (int c = 0; c < 7; ++c) st[wib][lane * 7 + c] = G[c];
+    }
+    __syncwarp();
+    const int cnt = min(32, p1 - base);
+    if (lane < 6) {
+#pragma unroll 8
+      for (int l = 0; l < cnt; ++l) acc = xadd(acc, st[wib][l * 7 + col]);
+    } else if (lane == 6) {
+      for (int l = 0; l < cnt; ++l) ml += (int32_t)st[wib][l * 7];
+    }
+    __syncwarp();
   }
+  const double posg0 = __shfl_sync(0xffffffffu, acc, 0);
+  const double posg1 = __shfl_sync(0xffffffffu, acc, 1);
+  const double posg2 = __shfl_sync(0xffffffffu, acc, 2);
+  const double rsg = __shfl_sync(0xffffffffu, acc, 3);
+  const double tm = __shfl_sync(0xffffffffu, acc, 4);
+  const double dmg = __shfl_sync(0xffffffffu, acc, 5);
+  ml = __shfl_sync(0xffffffffu, ml, 6);
+  if (lane != 0) return;
   NodeRec& nd = A.node[N];
   if (ml != nd.mass) set_err(A, 21, N);
   const double p2 = xadd(xadd(xmul(posg0, posg0), xmul(posg1, posg1)), xmul(posg2, posg2));
@@ -1493,6 +1526,10 @@ int stage_nodes(Engine& E) {
   // Waves: small tasks on the compute stream, large ones (the critical path)
   // in wider blocks on a second stream at the same time.
   if (!E.stream2) {
+    AHOP_CUDA_TRY(cudaFuncSetAttribute(tree_wave_kernel<kNTBig>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)wave_dyn_smem(kNTBig)));
+    AHOP_CUDA_TRY(cudaFuncSetAttribute(tree_wave_kernel<kNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)wave_dyn_smem(kNT)));
     AHOP_CUDA_TRY(cudaStreamCreateWithFlags(&E.stream2, cudaStreamNonBlocking));
     AHOP_CUDA_TRY(cudaEventCreateWithFlags(&E.ev_fork, cudaEventDisableTiming));
     AHOP_CUDA_TRY(cudaEventCreateWithFlags(&E.ev_join, cudaEventDisableTiming));
@@ -1506,13 +1543,13 @@ int stage_nodes(Engine& E) {
       AHOP_CUDA_TRY(cudaEventRecord(E.ev_fork, st));
       AHOP_CUDA_TRY(cudaStreamWaitEvent(E.stream2, E.ev_fork, 0));
       E.launches++;
-      tree_wave_kernel<kNTBig><<<nbig, kNTBig, 0, E.stream2>>>(A, tasksB[cur]);
+      tree_wave_kernel<kNTBig><<<nbig, kNTBig, wave_dyn_smem(kNTBig), E.stream2>>>(A, tasksB[cur]);
       AHOP_CUDA_TRY(cudaGetLastError());
       AHOP_CUDA_TRY(cudaEventRecord(E.ev_join, E.stream2));
     }
     if (nsmall > 0) {
       E.launches++;
-      tree_wave_kernel<kNT><<<nsmall, kNT, 0, st>>>(A, tasks[cur]);
+      tree_wave_kernel<kNT><<<nsmall, kNT, wave_dyn_smem(kNT), st>>>(A, tasks[cur]);
       AHOP_CUDA_TRY(cudaGetLastError());
     }
     if (nbig > 0) AHOP_CUDA_TRY(cudaStreamWaitEvent(st, E.ev_join, 0));
@@ -1581,7 +1618,7 @@ int stage_nodes(Engine& E) {
       E.launches++;
       pair_sums_warp_kernel<<<(unsigned)wblocks, 256, 0, st>>>(A, keys, np, posref, E.d_pair_sums.as<double>());
       E.launches++;
-      node_fold_kernel<<<(unsigned)((nn + T - 1) / T), T, 0, st>>>(A, nn, nstart, nend,
+      node_fold_kernel<<<(unsigned)(((int64_t)nn * 32 + T - 1) / T), T, 0, st>>>(A, nn, nstart, nend,
                                                                     E.d_pair_sums.as<double>());
       AHOP_CUDA_TRY(cudaGetLastError());
     }
