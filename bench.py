@@ -286,14 +286,26 @@ def main():
     alg = 168.0 * n
     achieved = alg / (knn_avg / 1e3) / 1e9
     traffic = None
+    inst = None
     try:
         prof = json.load(open(os.path.join(REPO, "profiles", "knn_density_traffic.txt")))
         traffic = prof["dram_bytes_per_particle"] * n
+        inst = prof.get("warp_instructions_per_particle")
     except Exception:
         pass
     roof = {"kernel": "knn_leaf_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "alg_bytes_per_launch": alg,
             "launch_ms": knn_avg, "peak_source": "measured" if peaks else "fallback"}
+    if inst:
+        # the kernel is bound by instruction issue, not HBM: the warp instructions
+        # ncu counted per query (profiles/) over this launch's time, against the
+        # issue peak of 4 warp schedulers per SM at the SM clock seen
+        props = torch.cuda.get_device_properties(local)
+        mhz = clk.summary().get("sm_mhz") or 1965.0
+        issue_peak = props.multi_processor_count * 4 * mhz * 1e6
+        ach = inst * n / (knn_avg / 1e3)
+        roof["issue"] = {"achieved_warp_inst_per_s": ach, "peak_warp_inst_per_s": issue_peak,
+                         "frac": ach / issue_peak, "warp_inst_per_query": inst}
     ts = (C.c_int64 * 13)()
     lib.ahop_debug_tree_stats(ts, 13)
     tree_stats = {"structural_Mcycles": ts[0] / 1e6, "level_stats_Mcycles": ts[1] / 1e6,
@@ -309,7 +321,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": spec["name"], "npart": n, "nhalo": spec["nhalo"], "seed": spec["seed"],
-                       "epsilon": eps, **PARAMS, "l2": "inputs (537 MB) larger than L2",
+                       "epsilon": eps, **PARAMS, "l2": f"inputs ({n * 32 / 1e6:.0f} MB) larger than L2",
                        "parallelism": f"replicas{world}"},
             "e2e": {"value": e2e, "unit": "Mpart/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roof, "stages_ms": mean_stage,
