@@ -358,6 +358,19 @@ int ahop_debug_task_profile(int64_t* out, int32_t maxrows) {
   return AHOP_OK;
 }
 
+int ahop_debug_set_big_task(int32_t groups) {
+  if (groups < 1) { set_error("big-task threshold must be positive"); return AHOP_EINVAL; }
+  engine().big_task = groups;
+  return AHOP_OK;
+}
+
+int ahop_debug_wave_profile(float* out, int32_t maxwaves) {
+  Engine& E = engine();
+  const int32_t n = std::min(maxwaves, E.nwave_prof);
+  for (int32_t i = 0; i < 4 * n; ++i) out[i] = E.wave_prof[i];
+  return n;
+}
+
 int ahop_debug_set_store_neighbours(int32_t k) {
   engine().req_store = k;
   return AHOP_OK;

@@ -75,6 +75,7 @@ struct NodeRec {
 constexpr int kLeaf = 32;         // particles per leaf bucket
 constexpr int kFan = 32;          // children per internal node
 constexpr int kMaxLevels = 8;
+constexpr int kMaxProfiledWaves = 64;
 
 struct Engine {
   Params prm;
@@ -82,6 +83,10 @@ struct Engine {
   cudaStream_t stream = nullptr;  // stream of the current call
   cudaStream_t stream2 = nullptr; // structure tree: large tasks run here beside the small ones
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t wave_ev[4] = {};          // per-wave timing (task profile only)
+  float wave_prof[4 * 64] = {};         // per wave: small tasks, ms, large tasks, ms
+  int32_t nwave_prof = 0;
+  int32_t big_task = 512;               // structure-tree tasks above this many groups use wide blocks
   cudaEvent_t ev[16] = {};
   int32_t launches = 0, cub_calls = 0, waves = 0, hop_passes = 0;  // counters of the current compute
   int32_t forest_rounds = 0, forest_edges = 0;                        // saddle forest of the current compute

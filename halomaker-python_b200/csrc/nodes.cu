@@ -46,8 +46,7 @@
 namespace ahop {
 
 constexpr int kNT = 256;        // threads per task block (grid-wide root kernels, small tasks)
-constexpr int kNTBig = 1024;    // threads per block for tasks of more than kBigTask groups
-constexpr int kBigTask = 2048;
+constexpr int kNTBig = 1024;    // threads per block for tasks of more than Engine::big_task groups
 constexpr int kTermWarps = 8;   // warps that sum large groups in an exact pass
 constexpr int kIPT = 4;         // items per thread in the reorder sort (2 for 1024-thread blocks)
 __host__ __device__ constexpr int ipt_for(int nt) { return nt >= 1024 ? 2 : kIPT; }
@@ -101,9 +100,10 @@ struct TreeArgs {
   NodeRec* node;          // [nnodesmax+1]
   int32_t nnodesmax;
   int32_t* nnodes;        // counter
-  Task* next;             // next wave's tasks of at most kBigTask groups
+  Task* next;             // next wave's tasks of at most big_task groups
   int32_t* nnext;
-  Task* next_big;         // next wave's larger tasks (run by kNTBig-thread blocks)
+  Task* next_big;         // next wave's tasks of more than big_task groups (kNTBig-thread blocks)
+  int32_t big_task;
   int32_t* nnext_big;
   int32_t* err;           // [0] code, [1] detail
   unsigned long long* stats;  // [11] counters (see the end of tree_wave_kernel; [8..10] undecided tests)
@@ -111,7 +111,7 @@ struct TreeArgs {
 };
 
 __device__ __forceinline__ void push_task(const TreeArgs& A, const Task& t) {
-  if (t.b - t.a > kBigTask) A.next_big[atomicAdd(A.nnext_big, 1)] = t;
+  if (t.b - t.a > A.big_task) A.next_big[atomicAdd(A.nnext_big, 1)] = t;
   else A.next[atomicAdd(A.nnext, 1)] = t;
 }
 
@@ -1395,7 +1395,8 @@ int stage_nodes(Engine& E) {
   A.ecur = reinterpret_cast<int32_t*>(take(bytes_i));
   A.gs = reinterpret_cast<double*>(take(G * 8 * 8));
   A.cs = reinterpret_cast<double*>(take(G * 12 * 8));
-  Task* tasks[2];   // tasks of at most kBigTask groups, by wave parity
+  A.big_task = E.big_task;
+  Task* tasks[2];   // tasks of at most big_task groups, by wave parity
   Task* tasksB[2];  // larger tasks
   tasks[0] = reinterpret_cast<Task*>(take((size_t)(nnodesmax + 1) * sizeof(Task)));
   tasks[1] = reinterpret_cast<Task*>(take((size_t)(nnodesmax + 1) * sizeof(Task)));
@@ -1441,7 +1442,7 @@ int stage_nodes(Engine& E) {
   int32_t nsmall = 0, nbig = 0;
   {
     const Task root{P.rho_threshold, 0, 0, ng, 0};
-    const bool big = ng > kBigTask;
+    const bool big = ng > A.big_task;
     AHOP_CUDA_TRY(cudaMemcpyAsync(big ? tasksB[0] : tasks[0], &root, sizeof(Task), cudaMemcpyHostToDevice, st));
     (big ? nbig : nsmall) = 1;
   }
@@ -1539,22 +1540,38 @@ int stage_nodes(Engine& E) {
     A.next = tasks[cur ^ 1];
     A.next_big = tasksB[cur ^ 1];
     AHOP_CUDA_TRY(cudaMemsetAsync(A.nnext, 0, 8, st));
+    const bool prof = E.task_profile && wave < kMaxProfiledWaves;
+    if (prof && !E.wave_ev[0]) {
+      for (auto& e : E.wave_ev) AHOP_CUDA_TRY(cudaEventCreate(&e));
+    }
     if (nbig > 0) {
       AHOP_CUDA_TRY(cudaEventRecord(E.ev_fork, st));
       AHOP_CUDA_TRY(cudaStreamWaitEvent(E.stream2, E.ev_fork, 0));
+      if (prof) AHOP_CUDA_TRY(cudaEventRecord(E.wave_ev[2], E.stream2));
       E.launches++;
       tree_wave_kernel<kNTBig><<<nbig, kNTBig, wave_dyn_smem(kNTBig), E.stream2>>>(A, tasksB[cur]);
       AHOP_CUDA_TRY(cudaGetLastError());
+      if (prof) AHOP_CUDA_TRY(cudaEventRecord(E.wave_ev[3], E.stream2));
       AHOP_CUDA_TRY(cudaEventRecord(E.ev_join, E.stream2));
     }
+    if (prof) AHOP_CUDA_TRY(cudaEventRecord(E.wave_ev[0], st));
     if (nsmall > 0) {
       E.launches++;
       tree_wave_kernel<kNT><<<nsmall, kNT, wave_dyn_smem(kNT), st>>>(A, tasks[cur]);
       AHOP_CUDA_TRY(cudaGetLastError());
     }
+    if (prof) AHOP_CUDA_TRY(cudaEventRecord(E.wave_ev[1], st));
     if (nbig > 0) AHOP_CUDA_TRY(cudaStreamWaitEvent(st, E.ev_join, 0));
     AHOP_CUDA_TRY(cudaMemcpyAsync(h, flags, 20, cudaMemcpyDeviceToHost, st));
     AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+    if (prof) {
+      float ms_s = 0.f, ms_b = 0.f;
+      cudaEventElapsedTime(&ms_s, E.wave_ev[0], E.wave_ev[1]);
+      if (nbig > 0) cudaEventElapsedTime(&ms_b, E.wave_ev[2], E.wave_ev[3]);
+      float* r = E.wave_prof + 4 * wave;
+      r[0] = (float)nsmall; r[1] = ms_s; r[2] = (float)nbig; r[3] = ms_b;
+      E.nwave_prof = wave + 1;
+    }
     if (h[0] != 0) {
       set_error("structure tree invariant failed (code " + std::to_string(h[0]) + ", detail " +
                 std::to_string(h[1]) + ")");

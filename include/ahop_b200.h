@@ -152,6 +152,13 @@ int ahop_debug_tree_stats(int64_t* out, int32_t n);
  * structural passes (reset, union, find, offsets, reorder, copy, starts,
  * component index).  Rows of nodes without a task stay 0. */
 int ahop_debug_set_task_profile(int32_t on);
+/* Structure-tree waves of the last compute while the task profile is on (at
+ * most 64): per wave the number of small tasks, their launch's milliseconds,
+ * the number of large tasks and theirs.  Returns the number of waves. */
+int ahop_debug_wave_profile(float* out, int32_t maxwaves);
+/* Tuning: structure-tree tasks of more than `groups` groups run in
+ * 1024-thread blocks on a second stream (default 512). */
+int ahop_debug_set_big_task(int32_t groups);
 int ahop_debug_task_profile(int64_t* out, int32_t maxrows);
 /* Ask compute to keep the first k neighbours per particle (default nhop). */
 int ahop_debug_set_store_neighbours(int32_t k);
