@@ -165,6 +165,14 @@ def halo_section(args, torch):
         halo_props.compute_device(d_off, d_pos, d_vel, d_mass, d_dens, out, 100.0, 70.0, epot=2, stream=st)
         t32.append(halo_props.timings()["epot32c"])
     tm = halo_props.timings()
+    # virial step (det_vir_1b: 1000 ellipsoidal shells per halo) on the FP64 rows
+    halo_props.compute_device(d_off, d_pos, d_vel, d_mass, d_dens, out, 100.0, 70.0, epot=1, stream=st)
+    vout = torch.zeros((nh, halo_props.NV), dtype=torch.float64, device=dev)
+    tv = []
+    for _ in range(max(1, args.steps)):
+        halo_props.virial_device(d_off, d_pos, d_vel, d_mass, out, vout, 100.0, 70.0, 430.1, 178.0, 2e-3,
+                                 stream=st)
+        tv.append(halo_props.virial_last_ms())
     pairs = float(tm["pairs"])
     m64, m32 = statistics.mean(t64), statistics.mean(t32)
     nominal_fp32 = 148 * 128 * 2 * 1.965e9 / 1e12  # TFLOP/s, non-tensor FP32 at max clock
@@ -176,7 +184,8 @@ def halo_section(args, torch):
                          "achieved": 20 * pairs / (m32 / 1e3) / 1e12, "peak": nominal_fp32, "unit": "TFLOP/s",
                          "frac": 20 * pairs / (m32 / 1e3) / 1e12 / nominal_fp32,
                          "peak_source": "nominal (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz)"},
-            "moments_ms": tm["moments"], "items": int(tm["items"])}
+            "moments_ms": tm["moments"], "items": int(tm["items"]), "virial_ms": statistics.mean(tv),
+            "virial_members_per_s": float(off[-1]) / (statistics.mean(tv) / 1e3)}
 
 
 def main():

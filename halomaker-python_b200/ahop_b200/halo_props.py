@@ -94,3 +94,63 @@ def timings() -> dict:
     t = AhopHaloTimings()
     L.check(_lib().ahop_halo_get_timings(C.byref(t)), "halo_get_timings")
     return {n: getattr(t, n) for n, _ in AhopHaloTimings._fields_}
+
+
+# ---------------------------------------------------------------- virial step
+VIR_FIELDS = ["rvir", "mvir", "cvel", "tvir", "rho_0", "r_c", "ep", "et", "amax", "bmax", "cmax"]
+NV = len(VIR_FIELDS)
+
+
+class AhopVirialParams(C.Structure):
+    _fields_ = [("Lbox", C.c_double), ("Hub_pt", C.c_double), ("gravconst", C.c_double),
+                ("vir_overdens", C.c_double), ("rho_mean", C.c_double), ("periodic", C.c_int32),
+                ("nshell", C.c_int32), ("direct_limit", C.c_int32), ("ep_field", C.c_int32)]
+
+
+def virial_params(Lbox, Hub_pt, gravconst, vir_overdens, rho_mean, periodic=True, nshell=1000, direct_limit=1000,
+                  ep="ep64"):
+    return AhopVirialParams(float(Lbox), float(Hub_pt), float(gravconst), float(vir_overdens), float(rho_mean),
+                            int(bool(periodic)), int(nshell), int(direct_limit), FIELDS.index(ep))
+
+
+def virial(off, pos, vel, mass, props, Lbox, Hub_pt, gravconst=430.1, vir_overdens=178.0, rho_mean=1.0,
+           periodic=True, nshell=1000, direct_limit=1000, ep="ep64") -> dict:
+    """det_vir_1b for every halo (ahop_halo_virial).  props: the dict returned
+    by compute() for the same halos.  Returns a dict of per-halo arrays
+    (VIR_FIELDS); ep/et are the reference's final energies."""
+    lib = _lib()
+    lib.ahop_halo_virial.argtypes = [C.POINTER(AhopVirialParams), C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_void_p]
+    off = np.ascontiguousarray(off, np.int64)
+    nh = len(off) - 1
+    pos = np.ascontiguousarray(pos, np.float64)
+    vel = np.ascontiguousarray(vel, np.float64)
+    mass = np.ascontiguousarray(mass, np.float64)
+    rows = np.ascontiguousarray(np.stack([np.asarray(props[f], np.float64) for f in FIELDS], 1)) if nh else \
+        np.zeros((1, NF))
+    out = np.zeros((max(nh, 1), NV))
+    p = virial_params(Lbox, Hub_pt, gravconst, vir_overdens, rho_mean, periodic, nshell, direct_limit, ep)
+    L.check(lib.ahop_halo_virial(C.byref(p), off.ctypes.data, nh, pos.ctypes.data, vel.ctypes.data,
+                                 mass.ctypes.data, rows.ctypes.data, out.ctypes.data), "halo_virial")
+    return {f: out[:nh, k].copy() for k, f in enumerate(VIR_FIELDS)}
+
+
+def virial_device(d_off, d_pos, d_vel, d_mass, d_props, d_out, Lbox, Hub_pt, gravconst=430.1, vir_overdens=178.0,
+                  rho_mean=1.0, periodic=True, nshell=1000, direct_limit=1000, ep="ep64", stream=None):
+    """torch CUDA tensors in (d_props: the (nhalo, NF) output of compute_device);
+    fills d_out (nhalo, NV) in place."""
+    lib = _lib()
+    lib.ahop_halo_virial_device.argtypes = [C.POINTER(AhopVirialParams), C.c_void_p, C.c_int64, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    p = virial_params(Lbox, Hub_pt, gravconst, vir_overdens, rho_mean, periodic, nshell, direct_limit, ep)
+    nh = d_off.numel() - 1
+    st = C.c_void_p(stream.cuda_stream if stream is not None else 0)
+    L.check(lib.ahop_halo_virial_device(C.byref(p), d_off.data_ptr(), nh, d_pos.data_ptr(), d_vel.data_ptr(),
+                                        d_mass.data_ptr(), d_props.data_ptr(), d_out.data_ptr(), st),
+            "halo_virial_device")
+
+
+def virial_last_ms() -> float:
+    lib = _lib()
+    lib.ahop_halo_virial_last_ms.restype = C.c_float
+    return float(lib.ahop_halo_virial_last_ms())

@@ -50,7 +50,6 @@ constexpr int kNTBig = 1024;    // threads per block for tasks of more than Engi
 constexpr int kTermWarps = 8;   // warps that sum large groups in an exact pass
 constexpr int kIPT = 4;         // items per thread in the reorder sort (2 for 1024-thread blocks)
 __host__ __device__ constexpr int ipt_for(int nt) { return nt >= 1024 ? 2 : kIPT; }
-constexpr int kChunk = kNT * kIPT;
 constexpr int kBigGroup = 96;   // groups larger than this are summed by a warp
 constexpr int kRowWarp = 32;    // saddle-row prefixes longer than this are linked by a warp
 constexpr int kMaxBigRows = 512;

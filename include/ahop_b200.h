@@ -237,6 +237,43 @@ int ahop_halo_props_noalloc(const AhopHaloParams* p, const int64_t* d_off, int64
                             const double* d_vel, const double* d_mass, const double* d_density, double* d_out,
                             void* stream);
 
+/* ---- virial properties ------------------------------------------------------
+ * Replaces det_vir_1b (CHP:1248-1262): det_main_axis_1b2 (principal axes with
+ * eigenvectors), tab_props_inside_1b40 (nshell concentric ellipsoids: mass and
+ * kinetic energy with Hubble flow), potential_profile_1b40 under the
+ * reference's default policies (shell integration, exact shell self-pair
+ * counting; halos of fewer than direct_limit members rescaled to their direct
+ * E_pot, larger ones take the profile's outer value as E_pot) and
+ * det_vir_props_1b4 (virial theorem to 20 %, else the overdensity
+ * vir_overdens * rho_mean), with the TSIS profile (rho_0, r_c).  Inputs are
+ * the members (as for ahop_halo_props) and that call's output rows; each halo
+ * gets AHOP_VIR_NFIELDS doubles indexed by VIR_*.  Halos whose axes degenerate
+ * (or that find no virial region) get NaN virial fields, as the reference. */
+enum {
+  VIR_RVIR = 0, VIR_MVIR, VIR_CVEL, VIR_TVIR, VIR_RHO0, VIR_RC, VIR_EP, VIR_ET, VIR_AMAX, VIR_BMAX, VIR_CMAX,
+  AHOP_VIR_NFIELDS
+};
+
+typedef struct {
+  double Lbox, Hub_pt, gravconst; /* as AhopHaloParams */
+  double vir_overdens, rho_mean;  /* H.vir_overdens, H.rho_mean (CHP:1330-1331) */
+  int32_t periodic;
+  int32_t nshell;       /* ttab, 1000 in the reference; at most 1024 */
+  int32_t direct_limit; /* full_PE / virial_direct_pe_nmax, 1000 in the reference */
+  int32_t ep_field;     /* HP_EP64 or HP_EP32C: which direct E_pot to rescale to */
+} AhopVirialParams;
+
+/* Host buffers: off[nhalo+1], pos[n][3], vel[n][3], mass[n],
+ * props[nhalo][AHOP_HALO_NFIELDS] (ahop_halo_props output); out[nhalo][AHOP_VIR_NFIELDS]. */
+int ahop_halo_virial(const AhopVirialParams* p, const int64_t* off, int64_t nhalo, const double* pos,
+                     const double* vel, const double* mass, const double* props, double* out);
+/* Same on device buffers, on `stream`. */
+int ahop_halo_virial_device(const AhopVirialParams* p, const int64_t* d_off, int64_t nhalo, const double* d_pos,
+                            const double* d_vel, const double* d_mass, const double* d_props, double* d_out,
+                            void* stream);
+/* Milliseconds of the last virial launch (CUDA events). */
+float ahop_halo_virial_last_ms(void);
+
 /* ---- differentiation -----------------------------------------------------------
  * SPH density with FIXED neighbour lists (nei[n][nvoisins], 0-based particle
  * indices sorted by distance at the lists' reference configuration) and its

@@ -87,3 +87,127 @@ def props(off, pos, vel, mass, dens, L, hub, G=430.1, periodic=True, epot=True, 
         hl = np.sqrt(res["Lx"] ** 2 + res["Ly"] ** 2 + res["Lz"] ** 2)
         res["spin64"] = hl * np.sqrt(np.abs(res["ek"] + res["ep64"])) / res["m"] ** 2.5 / G
     return res
+
+
+VIR_FIELDS = ["rvir", "mvir", "cvel", "tvir", "rho_0", "r_c", "ep", "et", "amax", "bmax", "cmax"]
+
+
+def virial(off, pos, vel, mass, dens, L, hub, G=430.1, vir_overdens=178.0, rho_mean=1.0, nshell=1000,
+           periodic=True, direct_limit=1000, nthreads=None):
+    """Virial properties per halo, restating det_vir_1b's chain (CHP:1248-1262):
+    det_main_axis_1b2 (1954-1967, scipy eigh), tab_props_inside_1b40 (969-1032),
+    potential_profile_1b40 under its default policies -- shell integration,
+    exact shell self-pair counting, profile outer energy for halos of at least
+    direct_limit members (1065-1123) -- and det_vir_props_1b4 (1127-1229)
+    with the TSIS profile of compute_halo_profile_1b41 (1232-1239).
+    Centre, bulk velocity, E_kin and the direct potential come from props()."""
+    from scipy.linalg import eigh
+    base = props(off, pos, vel, mass, dens, L, hub, G, periodic, True, nthreads)
+    nh = len(off) - 1
+    out = {f: np.full(nh, np.nan) for f in VIR_FIELDS}
+    nr = int(nshell)
+    for h in range(nh):
+        a, b = off[h], off[h + 1]
+        count = b - a
+        p, v, m = pos[a:b], vel[a:b], mass[a:b]
+        mt = base["m"][h]
+        c = np.array([base["px"][h], base["py"][h], base["pz"][h]])
+        vb = np.array([base["vx"][h], base["vy"][h], base["vz"][h]])
+        drx, dry, drz = [_wrap(p[:, k] - c[k], L) if periodic else p[:, k] - c[k] for k in range(3)]
+        mat = np.zeros((3, 3))
+        mat[0, 0] = np.sum(m * drx * drx); mat[0, 1] = np.sum(m * drx * dry); mat[0, 2] = np.sum(m * drx * drz)
+        mat[1, 0] = np.sum(m * drx * dry); mat[1, 1] = np.sum(m * dry * dry); mat[1, 2] = np.sum(m * dry * drz)
+        mat[2, 0] = np.sum(m * drx * drz); mat[2, 1] = np.sum(m * dry * drz); mat[2, 2] = np.sum(m * drz * drz)
+        d, V = eigh(mat)
+        d = np.sqrt(d / mt)
+        sha, shb, shc = d
+        ek = base["ek"][h]
+        ep = base["ep64"][h]
+        # tab_props_inside_1b40
+        eps = 1e-2
+        dra = drx * V[0, 0] + dry * V[1, 0] + drz * V[2, 0]
+        drb = drx * V[0, 1] + dry * V[1, 1] + drz * V[2, 1]
+        drc = drx * V[0, 2] + dry * V[1, 2] + drz * V[2, 2]
+        with np.errstate(divide="ignore", invalid="ignore"):
+            rmax = np.max(np.sqrt((dra / sha) ** 2 + (drb / shb) ** 2 + (drc / shc) ** 2))
+            amax, bmax, cmax = rmax * sha * (1.0 + eps), rmax * shb * (1.0 + eps), rmax * shc * (1.0 + eps)
+            vtx = v[:, 0] - vb[0] + drx * hub
+            vty = v[:, 1] - vb[1] + dry * hub
+            vtz = v[:, 2] - vb[2] + drz * hub
+            v2 = vtx ** 2 + vty ** 2 + vtz ** 2
+            r_ells = np.sqrt((dra / amax) ** 2 + (drb / bmax) ** 2 + (drc / cmax) ** 2)
+        if not np.all(np.isfinite(r_ells)):
+            continue  # degenerate axes: the reference cannot bin this halo either
+        i_ells = (r_ells * nr).astype(int)
+        valid = i_ells < nr
+        tabm = np.zeros(nr); tabk = np.zeros(nr)
+        np.add.at(tabm, i_ells[valid], m[valid])
+        np.add.at(tabk, i_ells[valid], 0.5 * m[valid] * v2[valid])
+        np.cumsum(tabm, out=tabm); np.cumsum(tabk, out=tabk)
+        counts = np.bincount(i_ells[valid], minlength=nr).astype(np.float64)
+        # potential_profile_1b40 (shell, count, profile_outer_for_large)
+        dm = np.diff(tabm, prepend=0.0)
+        before = tabm - dm
+        self_factor = np.zeros(nr)
+        occ = counts > 0
+        self_factor[occ] = 0.5 * (counts[occ] - 1.0) / counts[occ]
+        scale = np.arange(nr, dtype=np.float64) / np.float64(nr - 1)
+        scale[0] = 0.5 / np.float64(nr - 1)
+        r_eff = scale * (amax * bmax * cmax) ** (1.0 / 3.0)
+        tabp = -G * np.cumsum((before + self_factor * dm) * dm / r_eff)
+        outer = tabp[nr - 1]
+        if count < direct_limit:
+            if ep != outer and outer != 0.0:
+                tabp = tabp / outer * ep
+        else:
+            ep = outer
+        et = ek + ep
+        # det_vir_props_1b4
+        ttab = nr
+        mvir = tabm[ttab - 1]
+        i1 = 1
+        for i1 in range(ttab - 1, 0, -1):
+            if tabm[i1 - 1] < tabm[i1]:
+                break
+        avir = i1 / (ttab - 1) * amax
+        bvir = i1 / (ttab - 1) * bmax
+        cvir = i1 / (ttab - 1) * cmax
+        rvir = (avir * bvir * cvir) ** (1. / 3.)
+        virth_old = 1.0
+        virth = 100.0
+        for i0 in range(ttab - 1, -1, -1):
+            if (tabk[i0] + tabp[i0]) >= 0.0:
+                continue
+            virth = abs((2.0 * tabk[i0] + tabp[i0]) / (tabk[i0] + tabp[i0]))
+            if virth < virth_old:
+                mvir = tabm[i0]
+                avir = min(avir, i0 / (ttab - 1) * amax)
+                bvir = min(bvir, i0 / (ttab - 1) * bmax)
+                cvir = min(cvir, i0 / (ttab - 1) * cmax)
+                rvir = (avir * bvir * cvir) ** (1. / 3.)
+                virth_old = virth
+                if virth <= 0.20:
+                    break
+        volmin = 4. / 3. * np.pi * (amax / (ttab - 1)) * (bmax / (ttab - 1)) * (cmax / (ttab - 1))
+        if (virth > 0.20) or (mvir < vir_overdens * rho_mean * 4. / 3. * np.pi * avir * bvir * cvir):
+            ii1 = 1
+            for ii1 in range(ttab - 1, 0, -1):
+                mvir = vir_overdens * rho_mean * volmin * ii1 ** 3
+                if (tabm[ii1] >= mvir) and (tabm[ii1 - 1] < tabm[ttab - 1]):
+                    break
+            mvir = tabm[ii1]
+            avir = ii1 / (ttab - 1) * amax
+            bvir = ii1 / (ttab - 1) * bmax
+            cvir = ii1 / (ttab - 1) * cmax
+            rvir = (avir * bvir * cvir) ** (1. / 3.)
+        out["ep"][h], out["et"][h] = ep, et
+        out["amax"][h], out["bmax"][h], out["cmax"][h] = amax, bmax, cmax
+        if mvir > 0.0 and rvir > 0.0:
+            rv = min(rvir, base["r"][h])
+            out["rvir"][h] = rv
+            out["mvir"][h] = mvir
+            out["cvel"][h] = np.sqrt(G * mvir / rv)
+            out["tvir"][h] = 35.9 * G * mvir / rv
+            out["rho_0"][h] = mvir / (4.0 * np.pi * rv ** 3)
+            out["r_c"][h] = rv
+    return out

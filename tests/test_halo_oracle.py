@@ -31,3 +31,21 @@ def test_oracle_matches_reference_halo_functions():
     small = n < 1000
     np.testing.assert_allclose(r["ep64"][small], col("ep")[small], rtol=1e-12)
     np.testing.assert_allclose(r["spin64"][small], col("spin")[small], rtol=1e-10)
+
+
+VIR = os.path.join(os.path.dirname(__file__), "golden", "virial_case.npz")
+
+
+def test_virial_oracle_matches_reference():
+    """det_vir_1b's chain (tests/golden/make_virial_golden.py) vs the restatement:
+    the same NumPy/SciPy operations, so the discrete shell choices agree and the
+    values agree to rounding (the direct potential enters through the oracle's
+    own pair sum, 1e-12)."""
+    g = np.load(VIR)
+    f = list(g["fields"])
+    ref = g["out"]
+    r = halo_oracle.virial(g["off"], g["pos"], g["vel"], g["mass"], g["dens"], float(g["Lbox"]), float(g["Hub_pt"]),
+                           float(g["gravconst"]), float(g["vir_overdens"]), float(g["rho_mean"]), int(g["nshell"]),
+                           nthreads=2)
+    for name in ["rvir", "mvir", "cvel", "tvir", "rho_0", "r_c", "ep", "et", "amax", "bmax", "cmax"]:
+        np.testing.assert_allclose(r[name], ref[:, f.index(name)], rtol=1e-10, err_msg=name)
