@@ -21,7 +21,8 @@ NF = len(FIELDS)
 
 class AhopHaloParams(C.Structure):
     _fields_ = [("Lbox", C.c_double), ("Hub_pt", C.c_double), ("gravconst", C.c_double),
-                ("periodic", C.c_int32), ("epot", C.c_int32)]
+                ("periodic", C.c_int32), ("epot", C.c_int32), ("sc", C.c_int32), ("pad", C.c_int32),
+                ("dcell_min", C.c_double), ("eps_sc", C.c_double)]
 
 
 class AhopHaloTimings(C.Structure):
@@ -45,11 +46,15 @@ def _lib():
     return lib
 
 
-def params(Lbox, Hub_pt, gravconst=430.1, periodic=True, epot=3):
-    return AhopHaloParams(float(Lbox), float(Hub_pt), float(gravconst), int(bool(periodic)), int(epot))
+def params(Lbox, Hub_pt, gravconst=430.1, periodic=True, epot=3, sc=None):
+    """sc: None (centre = densest member) or (dcell_min, eps_SC) for the
+    shrinking-sphere centre of refine_centers_1b."""
+    on = sc is not None
+    return AhopHaloParams(float(Lbox), float(Hub_pt), float(gravconst), int(bool(periodic)), int(epot), int(on), 0,
+                          float(sc[0]) if on else 0.0, float(sc[1]) if on else 0.0)
 
 
-def compute(off, pos, vel, mass, dens, Lbox, Hub_pt, gravconst=430.1, periodic=True, epot=3) -> dict:
+def compute(off, pos, vel, mass, dens, Lbox, Hub_pt, gravconst=430.1, periodic=True, epot=3, sc=None) -> dict:
     """Host arrays in, dict of per-halo arrays out (FIELDS)."""
     off = np.ascontiguousarray(off, np.int64)
     nh = len(off) - 1
@@ -58,7 +63,7 @@ def compute(off, pos, vel, mass, dens, Lbox, Hub_pt, gravconst=430.1, periodic=T
     mass = np.ascontiguousarray(mass, np.float64)
     dens = np.ascontiguousarray(dens, np.float64)
     out = np.zeros((max(nh, 1), NF))
-    p = params(Lbox, Hub_pt, gravconst, periodic, epot)
+    p = params(Lbox, Hub_pt, gravconst, periodic, epot, sc)
     L.check(_lib().ahop_halo_props(C.byref(p), off.ctypes.data, nh, pos.ctypes.data, vel.ctypes.data,
                                    mass.ctypes.data, dens.ctypes.data, out.ctypes.data), "halo_props")
     return {f: out[:nh, k].copy() for k, f in enumerate(FIELDS)}

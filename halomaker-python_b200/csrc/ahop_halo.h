@@ -17,6 +17,9 @@ struct HaloArgs {
   double* out;            // [nhalo][kHaloFields]
   double L, h, hub, G;    // period, half period, Hubble constant, gravitational constant
   int periodic;
+  int sc;                 // shrinking-sphere centre (H.SC)
+  double dcell_min, eps_sc;
+  int* err;               // set when a bounded device loop hits its cap
 };
 
 }  // namespace ahop

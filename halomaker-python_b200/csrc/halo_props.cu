@@ -41,6 +41,7 @@
 namespace ahop {
 
 constexpr int kPB = 256;  // threads per block (and i-tile size of the pair kernel)
+constexpr long long kMaxShrinkSteps = 1000000;  // shrinking-sphere steps per halo (error past this)
 
 __device__ __forceinline__ double wrap_chp(double d, double L, double h, int periodic) {
   // correct_for_periodicity_1d (CHP:854-863): strict comparisons
@@ -69,6 +70,93 @@ __device__ __forceinline__ T block_sum(T v, T* sh) {
   r = sh[0];
   __syncthreads();
   return r;
+}
+
+// Shrinking-sphere centre (refine_centers_1b with SC, CHP:1555-1596 ->
+// det_halo_center_sphere_1b1, 1498-1541): from the densest member and the
+// radius of the farthest member, repeatedly take the centre of mass of the
+// members within r (min-image offsets) and shrink r by (1 - eps_SC), while
+// r > dcell_min and the sphere holds mass; the centre becomes the member
+// closest to the last centre of mass (first such member).  s_c[0..2] and
+// s_c[6] (centre and its member index) are updated in place.
+__device__ void shrink_sphere_centre(const HaloArgs& A, int64_t b0, int64_t b1, double* s_c, double* sh,
+                                     double* s_best_d, long long* s_best_i) {
+  __shared__ double s_sc[5];  // x0, y0, z0, r0, continue
+  const int tid = threadIdx.x;
+  double x0 = s_c[0], y0 = s_c[1], z0 = s_c[2];
+  auto dist2 = [&](int64_t i, double ax, double ay, double az, double& dx, double& dy, double& dz) {
+    dx = wrap_chp(A.pos[3 * i] - ax, A.L, A.h, A.periodic);
+    dy = wrap_chp(A.pos[3 * i + 1] - ay, A.L, A.h, A.periodic);
+    dz = wrap_chp(A.pos[3 * i + 2] - az, A.L, A.h, A.periodic);
+    return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+  };
+  // r0: farthest member from the densest one (_radius_from_center)
+  double r2 = 0.0;
+  for (int64_t i = b0 + tid; i < b1; i += kPB) {
+    double dx, dy, dz;
+    r2 = fmax(r2, dist2(i, x0, y0, z0, dx, dy, dz));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
+  if ((tid & 31) == 0) s_best_d[tid >> 5] = r2;
+  __syncthreads();
+  double r0 = s_best_d[0];
+  for (int w = 1; w < kPB / 32; ++w) r0 = fmax(r0, s_best_d[w]);
+  r0 = sqrt(r0);
+  __syncthreads();
+  if (!(r0 > 0.0) || !isfinite(r0)) return;
+  double xc = x0, yc = y0, zc = z0;
+  for (long long it = 0;; ++it) {
+    const double r02 = r0 * r0;
+    double pcx = 0, pcy = 0, pcz = 0, mt = 0;
+    for (int64_t i = b0 + tid; i < b1; i += kPB) {
+      double dx, dy, dz;
+      if (dist2(i, x0, y0, z0, dx, dy, dz) <= r02) {
+        const double w = A.mass[i];
+        pcx += w * dx; pcy += w * dy; pcz += w * dz; mt += w;
+      }
+    }
+    pcx = block_sum(pcx, sh); pcy = block_sum(pcy, sh); pcz = block_sum(pcz, sh); mt = block_sum(mt, sh);
+    if (tid == 0) {
+      if (mt > 0) { xc = pcx / mt + x0; yc = pcy / mt + y0; zc = pcz / mt + z0; }
+      else { xc = x0; yc = y0; zc = z0; }
+      bool cont = r0 > A.dcell_min && mt > 0;
+      if (cont && it >= kMaxShrinkSteps) { atomicExch(A.err, 1); cont = false; }
+      s_sc[0] = xc; s_sc[1] = yc; s_sc[2] = zc; s_sc[3] = (1.0 - A.eps_sc) * r0; s_sc[4] = cont ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    xc = s_sc[0]; yc = s_sc[1]; zc = s_sc[2];
+    const bool cont = s_sc[4] != 0.0;
+    r0 = s_sc[3];
+    __syncthreads();
+    if (!cont) break;
+    x0 = xc; y0 = yc; z0 = zc;
+  }
+  // the member closest to the last centre of mass (np.argmin: first minimum)
+  double bd = DBL_MAX;
+  long long bi = LLONG_MAX;
+  for (int64_t i = b0 + tid; i < b1; i += kPB) {
+    double dx, dy, dz;
+    const double d = dist2(i, xc, yc, zc, dx, dy, dz);
+    if (d < bd || (d == bd && i < bi)) { bd = d; bi = i; }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double od = __shfl_xor_sync(0xffffffffu, bd, o);
+    const long long oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (od < bd || (od == bd && oi < bi)) { bd = od; bi = oi; }
+  }
+  if ((tid & 31) == 0) { s_best_d[tid >> 5] = bd; s_best_i[tid >> 5] = bi; }
+  __syncthreads();
+  if (tid == 0) {
+    double d = s_best_d[0];
+    long long ii = s_best_i[0];
+    for (int w = 1; w < kPB / 32; ++w)
+      if (s_best_d[w] < d || (s_best_d[w] == d && s_best_i[w] < ii)) { d = s_best_d[w]; ii = s_best_i[w]; }
+    s_c[0] = A.pos[3 * ii]; s_c[1] = A.pos[3 * ii + 1]; s_c[2] = A.pos[3 * ii + 2];
+    s_c[6] = (double)(ii - b0);
+  }
+  __syncthreads();
 }
 
 // One block per halo: pass 1 (mass, momentum, densest member), pass 2
@@ -114,6 +202,7 @@ __global__ void __launch_bounds__(kPB) halo_moments_kernel(HaloArgs A) {
     s_c[6] = (double)(ii - b0);
   }
   __syncthreads();
+  if (A.sc) shrink_sphere_centre(A, b0, b1, s_c, sh, s_best_d, s_best_i);
   const double cx = s_c[0], cy = s_c[1], cz = s_c[2], vx = s_c[3], vy = s_c[4], vz = s_c[5];
   // pass 2
   double Lx = 0, Ly = 0, Lz = 0, r2max = 0, Ixx = 0, Ixy = 0, Ixz = 0, Iyy = 0, Iyz = 0, Izz = 0, ek = 0, sg = 0;
@@ -313,7 +402,7 @@ namespace ahop {
 
 struct HaloEngine {
   DevBuf d_off, d_pos, d_vel, d_mass, d_dens, d_out;  // staging for host inputs
-  DevBuf d_item_h, d_item_i, d_part64, d_part32, d_counter, d_hoff, d_order;
+  DevBuf d_item_h, d_item_i, d_part64, d_part32, d_counter, d_hoff, d_order, d_err;
   cudaEvent_t ev[5] = {};
   bool ready = false;
   cudaStream_t own = nullptr;
@@ -375,6 +464,10 @@ static int halo_run(HaloEngine& H, const AhopHaloParams* p, const int64_t* d_off
   HaloArgs A;
   A.off = d_off; A.pos = d_pos; A.vel = d_vel; A.mass = d_mass; A.dens = d_dens; A.out = d_out;
   A.L = p->Lbox; A.h = 0.5 * p->Lbox; A.hub = p->Hub_pt; A.G = p->gravconst; A.periodic = p->periodic != 0;
+  A.sc = p->sc != 0; A.dcell_min = p->dcell_min; A.eps_sc = p->eps_sc;
+  AHOP_CUDA_TRY(H.d_err.ensure(16));
+  AHOP_CUDA_TRY(cudaMemsetAsync(H.d_err.p, 0, 4, st));
+  A.err = H.d_err.as<int>();
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -416,7 +509,10 @@ static int halo_run(HaloEngine& H, const AhopHaloParams* p, const int64_t* d_off
     AHOP_CUDA_TRY(cudaGetLastError());
   }
   AHOP_CUDA_TRY(cudaEventRecord(H.ev[4], st));
+  int herr = 0;
+  AHOP_CUDA_TRY(cudaMemcpyAsync(&herr, H.d_err.p, 4, cudaMemcpyDeviceToHost, st));
   AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+  if (herr) { set_error("shrinking-sphere centre: step limit reached"); return AHOP_ELIMIT; }
   auto el = [&](int a, int b) { float ms = 0; cudaEventElapsedTime(&ms, H.ev[a], H.ev[b]); return ms; };
   H.t.moments = el(0, 1);
   H.t.epot64 = el(1, 2);
@@ -433,6 +529,11 @@ static int halo_validate(const AhopHaloParams* p, int64_t nhalo) {
   if (!p) { set_error("null params"); return AHOP_EINVAL; }
   if (nhalo < 0) { set_error("nhalo must be >= 0"); return AHOP_EINVAL; }
   if (p->periodic && !(p->Lbox > 0)) { set_error("Lbox must be positive for periodic boxes"); return AHOP_EINVAL; }
+  if (p->sc && !(p->eps_sc > 0.0 && p->eps_sc < 1.0)) {
+    // the reference's recursion never ends with eps_SC <= 0
+    set_error("eps_SC must be in (0, 1) when the shrinking-sphere centre is on");
+    return AHOP_EINVAL;
+  }
   return AHOP_OK;
 }
 
@@ -608,11 +709,15 @@ extern "C" int ahop_halo_props_noalloc(const AhopHaloParams* p, const int64_t* d
   }
   noalloc_items_kernel<<<(unsigned)((nhalo + 255) / 256), 256, 0, st>>>(d_off, nhalo, S);
   AHOP_CUDA_TRY(cudaGetLastError());
-  // the work counters must start at zero: the array keeps the last call's contents
+  // the work counters and the error flag must start at zero: the array keeps
+  // the last call's contents
   AHOP_CUDA_TRY(cudaMemsetAsync(S->counter, 0, 2 * sizeof(int32_t), st));
+  AHOP_CUDA_TRY(cudaMemsetAsync(&S->counter[3], 0, sizeof(int32_t), st));
   HaloArgs A;
   A.off = d_off; A.pos = d_pos; A.vel = d_vel; A.mass = d_mass; A.dens = d_density; A.out = d_out;
   A.L = p->Lbox; A.h = 0.5 * p->Lbox; A.hub = p->Hub_pt; A.G = p->gravconst; A.periodic = p->periodic != 0;
+  A.sc = p->sc != 0; A.dcell_min = p->dcell_min; A.eps_sc = p->eps_sc;
+  A.err = &S->counter[3];
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -635,6 +740,9 @@ extern "C" int ahop_halo_props_noalloc(const AhopHaloParams* p, const int64_t* d
   epot_finalize_kernel<<<(unsigned)((nhalo + 127) / 128), 128, 0, st>>>(
       A, S->hoff, S->order, (p->epot & 1) ? S->part64 : nullptr, (p->epot & 2) ? S->part32 : nullptr, nhalo);
   AHOP_CUDA_TRY(cudaGetLastError());
+  int32_t herr = 0;
+  AHOP_CUDA_TRY(cudaMemcpyAsync(&herr, &S->counter[3], 4, cudaMemcpyDeviceToHost, st));
   AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+  if (herr) { set_error("shrinking-sphere centre: step limit reached"); return AHOP_ELIMIT; }
   return AHOP_OK;
 }

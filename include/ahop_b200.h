@@ -204,6 +204,10 @@ typedef struct {
   double gravconst; /* G (H.gravconst = 430.1) */
   int32_t periodic; /* H.FlagPeriod != 0 */
   int32_t epot;     /* bit 0: FP64 direct sum, bit 1: FP32-compensated direct sum */
+  int32_t sc;       /* H.SC: shrinking-sphere centre (refine_centers_1b, CHP:1555-1596), off by default */
+  int32_t pad;
+  double dcell_min; /* H.dcell_min: smallest sphere radius */
+  double eps_sc;    /* H.eps_SC: radius shrink factor per step, in (0, 1) when sc is on */
 } AhopHaloParams;
 
 typedef struct {

@@ -51,8 +51,35 @@ def _wrap(d, L):
     return d
 
 
-def props(off, pos, vel, mass, dens, L, hub, G=430.1, periodic=True, epot=True, nthreads=None):
-    """Per-halo fields as a dict of arrays (names as in FIELDS, ep = FP64 pair sum)."""
+def shrink_sphere(p, m, c, L, periodic, dcell_min, eps_sc):
+    """refine_centers_1b with SC (CHP:1555-1596) -> det_halo_center_sphere_1b1
+    (1498-1541), recursion unrolled: returns the index of the new centre member."""
+    def offs(x0, y0, z0):
+        dx = _wrap(p[:, 0] - x0, L) if periodic else p[:, 0] - x0
+        dy = _wrap(p[:, 1] - y0, L) if periodic else p[:, 1] - y0
+        dz = _wrap(p[:, 2] - z0, L) if periodic else p[:, 2] - z0
+        return dx, dy, dz, dx ** 2 + dy ** 2 + dz ** 2
+    x0, y0, z0 = c
+    r0 = np.sqrt(np.max(offs(x0, y0, z0)[3]))
+    if not (np.isfinite(r0) and r0 > 0):
+        return None
+    while True:
+        dx, dy, dz, dr2 = offs(x0, y0, z0)
+        k = dr2 <= r0 * r0
+        pcx, pcy, pcz, mt = np.sum(m[k] * dx[k]), np.sum(m[k] * dy[k]), np.sum(m[k] * dz[k]), np.sum(m[k])
+        if mt > 0:
+            xc, yc, zc = pcx / mt + x0, pcy / mt + y0, pcz / mt + z0
+        else:
+            xc, yc, zc = x0, y0, z0
+        if r0 > dcell_min and mt > 0:
+            x0, y0, z0, r0 = xc, yc, zc, (1 - eps_sc) * r0
+            continue
+        return int(np.argmin(offs(xc, yc, zc)[3]))
+
+
+def props(off, pos, vel, mass, dens, L, hub, G=430.1, periodic=True, epot=True, nthreads=None, sc=None):
+    """Per-halo fields as a dict of arrays (names as in FIELDS, ep = FP64 pair sum).
+    sc = (dcell_min, eps_SC) refines the centre with the shrinking sphere."""
     nh = len(off) - 1
     res = {f: np.zeros(nh) for f in FIELDS}
     for h in range(nh):
@@ -60,6 +87,10 @@ def props(off, pos, vel, mass, dens, L, hub, G=430.1, periodic=True, epot=True, 
         p, v, m, d = pos[a:b], vel[a:b], mass[a:b], dens[a:b]
         mt = np.sum(m)
         ic = int(np.argmax(d))
+        if sc is not None:
+            j = shrink_sphere(p, m, p[ic], L, periodic, sc[0], sc[1])
+            if j is not None:
+                ic = j
         c = p[ic]
         vb = np.array([np.sum(m * v[:, 0]), np.sum(m * v[:, 1]), np.sum(m * v[:, 2])]) / mt
         dr = np.stack([_wrap(p[:, k] - c[k], L) if periodic else p[:, k] - c[k] for k in range(3)], 1)

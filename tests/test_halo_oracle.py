@@ -49,3 +49,23 @@ def test_virial_oracle_matches_reference():
                            nthreads=2)
     for name in ["rvir", "mvir", "cvel", "tvir", "rho_0", "r_c", "ep", "et", "amax", "bmax", "cmax"]:
         np.testing.assert_allclose(r[name], ref[:, f.index(name)], rtol=1e-10, err_msg=name)
+
+
+SC = os.path.join(os.path.dirname(__file__), "golden", "sc_case.npz")
+
+
+def test_shrinking_sphere_oracle_matches_reference():
+    """refine_centers_1b with SC on (tests/golden/make_sc_golden.py): the same
+    centre member, and the fields about it, as the reference."""
+    g = np.load(SC)
+    f = list(g["fields"])
+    ref = g["out"]
+    r = halo_oracle.props(g["off"], g["pos"], g["vel"], g["mass"], g["dens"], float(g["Lbox"]), float(g["Hub_pt"]),
+                          float(g["gravconst"]), epot=False, sc=(float(g["dcell_min"]), float(g["eps_sc"])))
+    for name in ["px", "py", "pz"]:
+        assert np.array_equal(r[name], ref[:, f.index(name)]), name
+    for name in ["r", "sha", "shb", "shc"]:
+        np.testing.assert_allclose(r[name], ref[:, f.index(name)], rtol=1e-10, err_msg=name)
+    for name in ["Lx", "Ly", "Lz"]:
+        col = ref[:, f.index(name)]
+        np.testing.assert_allclose(r[name], col, rtol=1e-10, atol=1e-12 * np.abs(col).max(), err_msg=name)
