@@ -19,11 +19,11 @@
 // one persistent launch over a work list of (halo, i-tile) items sorted by
 // decreasing cost; each item sums m_j / r_ij for its 256 i-particles over all
 // j > i.  Two forms share the schedule:
-//   * FP64: relative positions and 1/sqrt in double;
+//   * FP64: relative positions, 1/r from the double reciprocal square root;
 //   * FP32-compensated: positions relative to the halo centre split into
-//     hi = float(r) and lo = float(r - hi); a pair separation is
-//     (hi_j - hi_i) + (lo_j - lo_i) in FP32, 1/r from rsqrtf plus one Newton
-//     step, partial sums Kahan-compensated in FP32 and folded into FP64 per
+//     hi = float(r) and lo = float(r - hi) (float4 tiles in shared memory);
+//     a pair separation is (hi_j - hi_i) + (lo_j - lo_i) in FP32, 1/r from
+//     rsqrtf, partial sums Kahan-compensated in FP32 and folded into FP64 per
 //     item.
 // Per-item partials are reduced per halo in item order (deterministic).
 #include <cuda_runtime.h>
@@ -252,7 +252,7 @@ template <bool FP32C>
 __global__ void __launch_bounds__(kPB) epot_pairs_kernel(HaloArgs A, const int32_t* __restrict__ item_h,
                                                          const int32_t* __restrict__ item_i, int32_t nitems,
                                                          int32_t* __restrict__ counter, double* __restrict__ part) {
-  __shared__ float s_hx[kPB], s_hy[kPB], s_hz[kPB], s_lx[kPB], s_ly[kPB], s_lz[kPB], s_m[kPB];
+  __shared__ float4 s_h[kPB], s_l[kPB];  // FP32 form: (hi x, hi y, hi z, mass), (lo x, lo y, lo z, -)
   __shared__ double s_dx[kPB], s_dy[kPB], s_dz[kPB], s_dm[kPB];
   __shared__ double sh[kPB / 32];
   __shared__ int32_t s_item;
@@ -289,15 +289,13 @@ __global__ void __launch_bounds__(kPB) epot_pairs_kernel(HaloArgs A, const int32
         const double rz = wrap_chp(A.pos[3 * (base + j) + 2] - cz, A.L, A.h, A.periodic);
         if (FP32C) {
           const float hx = (float)rx, hy = (float)ry, hz = (float)rz;
-          s_hx[tid] = hx; s_hy[tid] = hy; s_hz[tid] = hz;
-          s_lx[tid] = (float)(rx - (double)hx); s_ly[tid] = (float)(ry - (double)hy);
-          s_lz[tid] = (float)(rz - (double)hz);
-          s_m[tid] = (float)A.mass[base + j];
+          s_h[tid] = make_float4(hx, hy, hz, (float)A.mass[base + j]);
+          s_l[tid] = make_float4((float)(rx - (double)hx), (float)(ry - (double)hy), (float)(rz - (double)hz), 0.f);
         } else {
           s_dx[tid] = rx; s_dy[tid] = ry; s_dz[tid] = rz; s_dm[tid] = A.mass[base + j];
         }
       } else {
-        if (FP32C) { s_m[tid] = 0.f; s_hx[tid] = s_hy[tid] = s_hz[tid] = 3.0e30f; s_lx[tid] = s_ly[tid] = s_lz[tid] = 0.f; }
+        if (FP32C) { s_h[tid] = make_float4(3.0e30f, 3.0e30f, 3.0e30f, 0.f); s_l[tid] = make_float4(0.f, 0.f, 0.f, 0.f); }
         else { s_dm[tid] = 0.0; s_dx[tid] = s_dy[tid] = s_dz[tid] = 3.0e30; }
       }
       __syncthreads();
@@ -307,13 +305,14 @@ __global__ void __launch_bounds__(kPB) epot_pairs_kernel(HaloArgs A, const int32
         if (FP32C) {
 #pragma unroll 8
           for (int jj = jstart; jj < jend; ++jj) {
-            const float dx = (s_hx[jj] - hxi) + (s_lx[jj] - lxi);
-            const float dy = (s_hy[jj] - hyi) + (s_ly[jj] - lyi);
-            const float dz = (s_hz[jj] - hzi) + (s_lz[jj] - lzi);
+            const float4 hj = s_h[jj], lj = s_l[jj];
+            const float dx = (hj.x - hxi) + (lj.x - lxi);
+            const float dy = (hj.y - hyi) + (lj.y - lyi);
+            const float dz = (hj.z - hzi) + (lj.z - lzi);
             const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            float inv = rsqrtf(r2);
-            inv = inv * (1.5f - 0.5f * r2 * inv * inv);  // one Newton step
-            const float t = (r2 > 0.f) ? s_m[jj] * inv : 0.f;
+            // hardware reciprocal square root (a few ulp): per-halo sums stay
+            // within the 1e-6 bound of the FP64 form (checked by the tests)
+            const float t = (r2 > 0.f) ? hj.w * rsqrtf(r2) : 0.f;
             const float y = t - kc;
             const float s2 = ks + y;
             kc = (s2 - ks) - y;
@@ -324,7 +323,7 @@ __global__ void __launch_bounds__(kPB) epot_pairs_kernel(HaloArgs A, const int32
           for (int jj = jstart; jj < jend; ++jj) {
             const double dx = s_dx[jj] - rxi, dy = s_dy[jj] - ryi, dz = s_dz[jj] - rzi;
             const double r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 > 0.0) ds += s_dm[jj] / sqrt(r2);
+            if (r2 > 0.0) ds += s_dm[jj] * rsqrt(r2);
           }
         }
       }
