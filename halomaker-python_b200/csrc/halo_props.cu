@@ -339,6 +339,138 @@ __global__ void __launch_bounds__(kPB) epot_pairs_kernel(HaloArgs A, const int32
   }
 }
 
+// FP32-compensated pair sums with two i-rows per thread: 128 threads cover
+// an item's 256 rows (rows tid and tid + 128), so every float4 pair of
+// shared-memory loads serves two pairs.  Same schedule, same per-item partial
+// and the same arithmetic per pair as epot_pairs_kernel<true>.
+constexpr int kPB2 = kPB / 2;
+
+__device__ __forceinline__ float pair_term(const float4& hj, const float4& lj, float hx, float hy, float hz,
+                                           float lx, float ly, float lz) {
+  const float dx = (hj.x - hx) + (lj.x - lx);
+  const float dy = (hj.y - hy) + (lj.y - ly);
+  const float dz = (hj.z - hz) + (lj.z - lz);
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  return (r2 > 0.f) ? hj.w * rsqrtf(r2) : 0.f;
+}
+
+__device__ __forceinline__ void kahan_add(float t, float& ks, float& kc) {
+  const float y = t - kc;
+  const float s2 = ks + y;
+  kc = (s2 - ks) - y;
+  ks = s2;
+}
+
+__device__ __forceinline__ void kahan_pair(const float4& hj, const float4& lj, float hx, float hy, float hz,
+                                           float lx, float ly, float lz, float& ks, float& kc) {
+  kahan_add(pair_term(hj, lj, hx, hy, hz, lx, ly, lz), ks, kc);
+}
+
+__global__ void __launch_bounds__(kPB2) epot_pairs32_kernel(HaloArgs A, const int32_t* __restrict__ item_h,
+                                                            const int32_t* __restrict__ item_i, int32_t nitems,
+                                                            int32_t* __restrict__ counter,
+                                                            double* __restrict__ part) {
+  __shared__ float4 s_h[kPB], s_l[kPB];
+  __shared__ double sh[kPB2 / 32];
+  __shared__ int32_t s_item;
+  const int tid = threadIdx.x;
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int32_t w = s_item;
+    __syncthreads();
+    if (w >= nitems) break;
+    const int32_t h = item_h[w];
+    const int64_t base = A.off[h];
+    const int32_t n = (int32_t)(A.off[h + 1] - base);
+    const int32_t i0 = item_i[w];
+    const double* c = A.out + (size_t)kHaloFields * h;
+    const double cx = c[HP_PX], cy = c[HP_PY], cz = c[HP_PZ];
+    float hx[2], hy[2], hz[2], lx[2], ly[2], lz[2], ks[2] = {0.f, 0.f}, kc[2] = {0.f, 0.f};
+    bool vi[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int32_t i = i0 + tid + r * kPB2;
+      vi[r] = i < n;
+      double rx = 0, ry = 0, rz = 0;
+      if (vi[r]) {
+        rx = wrap_chp(A.pos[3 * (base + i)] - cx, A.L, A.h, A.periodic);
+        ry = wrap_chp(A.pos[3 * (base + i) + 1] - cy, A.L, A.h, A.periodic);
+        rz = wrap_chp(A.pos[3 * (base + i) + 2] - cz, A.L, A.h, A.periodic);
+      }
+      hx[r] = (float)rx; hy[r] = (float)ry; hz[r] = (float)rz;
+      lx[r] = (float)(rx - (double)hx[r]); ly[r] = (float)(ry - (double)hy[r]); lz[r] = (float)(rz - (double)hz[r]);
+    }
+    for (int32_t j0 = i0; j0 < n; j0 += kPB) {
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int32_t t = tid + r * kPB2;
+        const int32_t j = j0 + t;
+        if (j < n) {
+          const double rx = wrap_chp(A.pos[3 * (base + j)] - cx, A.L, A.h, A.periodic);
+          const double ry = wrap_chp(A.pos[3 * (base + j) + 1] - cy, A.L, A.h, A.periodic);
+          const double rz = wrap_chp(A.pos[3 * (base + j) + 2] - cz, A.L, A.h, A.periodic);
+          const float fx = (float)rx, fy = (float)ry, fz = (float)rz;
+          s_h[t] = make_float4(fx, fy, fz, (float)A.mass[base + j]);
+          s_l[t] = make_float4((float)(rx - (double)fx), (float)(ry - (double)fy), (float)(rz - (double)fz), 0.f);
+        } else {
+          s_h[t] = make_float4(3.0e30f, 3.0e30f, 3.0e30f, 0.f);
+          s_l[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+      __syncthreads();
+      const int jend = min(kPB, n - j0);
+      if (j0 == i0) {
+        // diagonal tile: j > i for each row (row 0 is tile row tid, row 1 is tid + kPB2)
+        for (int jj = tid + 1; jj < jend; ++jj) {
+          const float4 hj = s_h[jj], lj = s_l[jj];
+          if (vi[0]) kahan_pair(hj, lj, hx[0], hy[0], hz[0], lx[0], ly[0], lz[0], ks[0], kc[0]);
+          if (vi[1] && jj > tid + kPB2) kahan_pair(hj, lj, hx[1], hy[1], hz[1], lx[1], ly[1], lz[1], ks[1], kc[1]);
+        }
+      } else if (vi[0]) {
+        // groups of four partners: the four terms of a row are added as a
+        // small tree (independent work), then the group enters the
+        // compensated sum once -- one dependent chain per four pairs
+        int jj = 0;
+        for (; jj + 4 <= jend; jj += 4) {
+          float g[2];
+#pragma unroll
+          for (int r = 0; r < 2; ++r) {
+            const float t0 = pair_term(s_h[jj], s_l[jj], hx[r], hy[r], hz[r], lx[r], ly[r], lz[r]);
+            const float t1 = pair_term(s_h[jj + 1], s_l[jj + 1], hx[r], hy[r], hz[r], lx[r], ly[r], lz[r]);
+            const float t2 = pair_term(s_h[jj + 2], s_l[jj + 2], hx[r], hy[r], hz[r], lx[r], ly[r], lz[r]);
+            const float t3 = pair_term(s_h[jj + 3], s_l[jj + 3], hx[r], hy[r], hz[r], lx[r], ly[r], lz[r]);
+            g[r] = (t0 + t1) + (t2 + t3);
+          }
+          kahan_add(g[0], ks[0], kc[0]);
+          kahan_add(g[1], ks[1], kc[1]);
+        }
+        for (; jj < jend; ++jj) {
+          const float4 hj = s_h[jj], lj = s_l[jj];
+          kahan_pair(hj, lj, hx[0], hy[0], hz[0], lx[0], ly[0], lz[0], ks[0], kc[0]);
+          kahan_pair(hj, lj, hx[1], hy[1], hz[1], lx[1], ly[1], lz[1], ks[1], kc[1]);
+        }
+      }
+      __syncthreads();
+    }
+    double mine = 0.0;
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+      if (vi[r]) mine += A.mass[base + i0 + tid + r * kPB2] * ((double)ks[r] - (double)kc[r]);
+    // block sum over kPB2 threads
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+    if ((tid & 31) == 0) sh[tid >> 5] = mine;
+    __syncthreads();
+    if (tid == 0) {
+      double tot = 0.0;
+      for (int k = 0; k < kPB2 / 32; ++k) tot += sh[k];
+      part[w] = tot;
+    }
+    __syncthreads();
+  }
+}
+
 // per-halo reduction of item partials (items of a halo are contiguous in the
 // halo-ordered list hitem_off), then E_pot, totals and spin
 __global__ void epot_finalize_kernel(HaloArgs A, const int64_t* __restrict__ hitem_off,
@@ -491,9 +623,9 @@ static int halo_run(HaloEngine& H, const AhopHaloParams* p, const int64_t* d_off
   AHOP_CUDA_TRY(cudaEventRecord(H.ev[2], st));
   if ((p->epot & 2) && nitems > 0) {
     int per = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, epot_pairs_kernel<true>, kPB, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, epot_pairs32_kernel, kPB2, 0);
     AHOP_CUDA_TRY(cudaMemsetAsync(H.d_counter.as<int32_t>() + 1, 0, 4, st));
-    epot_pairs_kernel<true><<<nsm * (per > 0 ? per : 1), kPB, 0, st>>>(
+    epot_pairs32_kernel<<<nsm * (per > 0 ? per : 1), kPB2, 0, st>>>(
         A, H.d_item_h.as<int32_t>(), H.d_item_i.as<int32_t>(), nitems, H.d_counter.as<int32_t>() + 1,
         H.d_part32.as<double>());
     ++launches;
@@ -731,8 +863,8 @@ extern "C" int ahop_halo_props_noalloc(const AhopHaloParams* p, const int64_t* d
   }
   if ((p->epot & 2) && total > 0) {
     int per = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, epot_pairs_kernel<true>, kPB, 0);
-    epot_pairs_kernel<true><<<nsm * (per > 0 ? per : 1), kPB, 0, st>>>(A, S->item_h, S->item_i, total,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, epot_pairs32_kernel, kPB2, 0);
+    epot_pairs32_kernel<<<nsm * (per > 0 ? per : 1), kPB2, 0, st>>>(A, S->item_h, S->item_i, total,
                                                                        &S->counter[1], S->part32);
     AHOP_CUDA_TRY(cudaGetLastError());
   }
