@@ -282,7 +282,7 @@ static void release_device(Engine& E) {
                     &E.d_sad_val2, &E.d_sad_cnt, &E.d_sad_keep, &E.d_sad_kpos, &E.d_flags, &E.d_soff,
                     &E.d_sisad, &E.d_srho, &E.d_nodes, &E.d_tree_scratch, &E.d_liste, &E.d_dens_orig,
                     &E.d_rtab, &E.d_itab, &E.d_tprof, &E.d_pairs, &E.d_pair_sums, &E.d_node_aux,
-                    &E.d_forest, &E.d_moff, &E.d_misad, &E.d_mrho};
+                    &E.d_forest, &E.d_moff, &E.d_misad, &E.d_mrho, &E.d_kspill};
   if (E.device >= 0) cudaSetDevice(E.device);
   for (DevBuf* b : bufs) b->release();
   E.h_liste.release(); E.h_dens.release(); E.h_rtab.release(); E.h_itab.release();

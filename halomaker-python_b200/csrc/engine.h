@@ -116,6 +116,7 @@ struct Engine {
 
   // kNN / density
   DevBuf d_nei;                          // [n][nstore] sorted-slot neighbour ids
+  DevBuf d_kspill;                       // kNN candidate spill buffers (per resident warp)
   DevBuf d_dens;                         // density in sorted order
   // hop / groups
   DevBuf d_hop, d_root, d_group;         // per sorted slot

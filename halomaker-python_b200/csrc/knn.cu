@@ -208,6 +208,7 @@ struct KnnArgs {
   double* dens; // [n]
   int* err;     // error flag (stack overflow)
   unsigned long long* kstats;  // [0] query leaves [1] candidate leaves [2] leaf visits [3] insertions [4] overflows
+  unsigned* kspill;             // per-warp candidate spill buffers [grid warps][2 * kMaxCandSpill], or null
   int kdebug;   // extra counters: [5] leaves within the final radius, [6]/[7] cycles of overflow/other leaves,
                 // [24..28] phase cycles of the other leaves (bound, candidates + sort, seed lists, scan, density)
 };
@@ -433,7 +434,8 @@ __device__ __forceinline__ double boxbox_dist2(const double* __restrict__ a, con
   return dx * dx + dy * dy + dz * dz;
 }
 
-constexpr int kMaxCand = 512;  // candidate leaves per query leaf (else per-query DFS)
+constexpr int kMaxCand = 512;        // candidate leaves per query leaf held in shared memory
+constexpr int kMaxCandSpill = 4096;  // ... in the warp's global spill buffer (else per-query DFS)
 
 // One warp per query leaf (its 32 Morton-consecutive particles).
 //  A. every query sorts the 64 particles of its own and the adjacent leaf
@@ -480,9 +482,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
     for (int o = 16; o > 0; o >>= 1) R2 = fmax(R2, __shfl_xor_sync(0xffffffffu, R2, o));
     if (!ok) R2 = CUDART_INF;
     const long long t_a = clock64();
-    // ---- B: candidate leaves within R of this leaf's box
+    // ---- B: candidate leaves within R of this leaf's box; the list lives in
+    // shared memory and moves to the warp's global spill buffer past kMaxCand
     const double* myb = A.box + 6 * jl;
     int ncand = 0;
+    unsigned* kb = s_key;
+    int32_t* cb = s_cand[wib];
+    int cap = kMaxCand;
     bool overflow = !(R2 < CUDART_INF);
     if (!overflow) {
       const double lim = R2 * (1.0 + 1e-12);
@@ -509,12 +515,23 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
         if (!cnt) continue;
         const int r = __popc(mask & ((1u << lane) - 1));
         if (lvl - 1 == 0) {
-          if (ncand + cnt > kMaxCand) { overflow = true; break; }
+          if (ncand + cnt > cap) {
+            if (cap == kMaxCand && A.kspill) {
+              unsigned* gk = A.kspill + (size_t)(blockIdx.x * kWarpsPerBlock + wib) * (2 * kMaxCandSpill);
+              int32_t* gc = reinterpret_cast<int32_t*>(gk + kMaxCandSpill);
+              for (int i = lane; i < ncand; i += 32) { gk[i] = kb[i]; gc[i] = cb[i]; }
+              __syncwarp();
+              kb = gk;
+              cb = gc;
+              cap = kMaxCandSpill;
+            }
+            if (ncand + cnt > cap) { overflow = true; break; }
+          }
           if (cand) {
-            // sort key: the leaf-to-leaf distance rounded down to 23 bits, then the slot
+            // sort key: the leaf-to-leaf distance rounded down to 20 bits, then the slot
             const unsigned fb = __float_as_uint(__double2float_rd(bbd));
-            s_key[ncand + r] = ((fb >> 8) << 9) | (unsigned)(ncand + r);
-            s_cand[wib][ncand + r] = (int32_t)c;
+            kb[ncand + r] = ((fb >> 11) << 12) | (unsigned)(ncand + r);
+            cb[ncand + r] = (int32_t)c;
           }
           ncand += cnt;
         } else {
@@ -530,14 +547,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
       // candidates nearest-first: warp bitonic sort of the keys in shared memory
       int N = 32;
       while (N < ncand) N <<= 1;
-      for (int i = ncand + lane; i < N; i += 32) s_key[i] = 0xffffffffu;
+      for (int i = ncand + lane; i < N; i += 32) kb[i] = 0xffffffffu;
       __syncwarp();
       for (int k = 2; k <= N; k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
           for (int t = lane; t < (N >> 1); t += 32) {
             const int i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
-            const unsigned a = s_key[i], b = s_key[i + j];
-            if ((a > b) == ((i & k) == 0)) { s_key[i] = b; s_key[i + j] = a; }
+            const unsigned a = kb[i], b = kb[i + j];
+            if ((a > b) == ((i & k) == 0)) { kb[i] = b; kb[i + j] = a; }
           }
           __syncwarp();
         }
@@ -560,13 +577,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
         for (int c0 = 0; c0 < ncand; c0 += 32) {
           // every query lies in this leaf's box, so a candidate whose box is at
           // least the current radius from that box (and all after it) is out
-          const double lb = (double)__uint_as_float((s_key[c0] >> 9) << 8);
+          const double lb = (double)__uint_as_float((kb[c0] >> 12) << 11);
           if (lb * (1.0 - 1e-9) >= L.r2) break;
           const int ci = c0 + lane;
           int32_t leaf = -1;
           double bd = CUDART_INF;
           if (ci < ncand) {
-            leaf = s_cand[wib][s_key[ci] & 511u];
+            leaf = cb[kb[ci] & 4095u];
             if (leaf != jl && leaf != jn) bd = box_dist2(A.box + 6 * (int64_t)leaf, qx, qy, qz, A.Lx, A.Ly, A.Lz);
           }
           unsigned mask = __ballot_sync(0xffffffffu, bd < L.r2);
@@ -587,7 +604,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
         for (int c0 = 0; c0 < ncand; c0 += 32) {
           const int ci = c0 + lane;
           bool in = false;
-          if (ci < ncand) in = box_dist2(A.box + 6 * (int64_t)s_cand[wib][ci], qx, qy, qz, A.Lx, A.Ly, A.Lz) < L.r2;
+          if (ci < ncand) in = box_dist2(A.box + 6 * (int64_t)cb[ci], qx, qy, qz, A.Lx, A.Ly, A.Lz) < L.r2;
           nideal += __popc(__ballot_sync(0xffffffffu, in));
         }
       }
@@ -649,8 +666,10 @@ int stage_knn_density(Engine& E) {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, knn_leaf_kernel, kWarpsPerBlock * 32, 0);
   if (per_sm < 1) per_sm = 1;
   int64_t want = (E.lev_cnt[0] + kWarpsPerBlock - 1) / kWarpsPerBlock;
-  int64_t grid = (int64_t)nsm * per_sm * 4;
+  int64_t grid = (int64_t)nsm * per_sm * 2;
   if (grid > want) grid = want;
+  AHOP_CUDA_TRY(E.d_kspill.ensure((size_t)grid * kWarpsPerBlock * 2 * kMaxCandSpill * 4));
+  A.kspill = E.d_kspill.as<unsigned>();
   E.launches++;
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[9], E.stream));
   knn_leaf_kernel<<<(unsigned)grid, kWarpsPerBlock * 32, 0, E.stream>>>(A);
