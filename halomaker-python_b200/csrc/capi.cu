@@ -69,7 +69,10 @@ static int validate(const Engine& E, int64_t n) {
   return AHOP_OK;
 }
 
-static int run_pipeline(Engine& E, const double* d_pos, const double* d_mass, int last_stage = 99) {
+// h_dens_early: pinned host buffer that receives the density (caller order)
+// on a copy stream while the later stages run, or null.
+static int run_pipeline(Engine& E, const double* d_pos, const double* d_mass, int last_stage = 99,
+                        double* h_dens_early = nullptr) {
   int rc;
   E.launches = E.cub_calls = E.waves = E.hop_passes = 0;
   cudaStream_t st = E.stream;
@@ -78,6 +81,24 @@ static int run_pipeline(Engine& E, const double* d_pos, const double* d_mass, in
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[2], st));
   if (last_stage < 2) return AHOP_OK;
   if ((rc = stage_knn_density(E))) return rc;
+  // the density is final here: back to caller order now
+  AHOP_CUDA_TRY(E.d_dens_orig.ensure(E.n * 8));
+  E.launches++;
+  dens_to_orig_kernel<<<(unsigned)((E.n + 255) / 256), 256, 0, st>>>(E.d_dens.as<double>(),
+                                                                     E.d_orig.as<int32_t>(), E.n,
+                                                                     E.d_dens_orig.as<double>());
+  AHOP_CUDA_TRY(cudaGetLastError());
+  if (h_dens_early) {
+    if (!E.stream_copy) {
+      AHOP_CUDA_TRY(cudaStreamCreateWithFlags(&E.stream_copy, cudaStreamNonBlocking));
+      AHOP_CUDA_TRY(cudaEventCreateWithFlags(&E.ev_dens, cudaEventDisableTiming));
+      AHOP_CUDA_TRY(cudaEventCreateWithFlags(&E.ev_copied, cudaEventDisableTiming));
+    }
+    AHOP_CUDA_TRY(cudaEventRecord(E.ev_dens, st));
+    AHOP_CUDA_TRY(cudaStreamWaitEvent(E.stream_copy, E.ev_dens, 0));
+    AHOP_CUDA_TRY(cudaMemcpyAsync(h_dens_early, E.d_dens_orig.p, E.n * 8, cudaMemcpyDeviceToHost, E.stream_copy));
+    AHOP_CUDA_TRY(cudaEventRecord(E.ev_copied, E.stream_copy));
+  }
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[3], st));
   if (last_stage < 3) return AHOP_OK;
   if ((rc = stage_hop_groups(E))) return rc;
@@ -88,13 +109,6 @@ static int run_pipeline(Engine& E, const double* d_pos, const double* d_mass, in
   if (last_stage < 5) return AHOP_OK;
   if ((rc = stage_nodes(E))) return rc;
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[6], st));
-  // density back to caller order
-  AHOP_CUDA_TRY(E.d_dens_orig.ensure(E.n * 8));
-  E.launches++;
-  dens_to_orig_kernel<<<(unsigned)((E.n + 255) / 256), 256, 0, st>>>(E.d_dens.as<double>(),
-                                                                     E.d_orig.as<int32_t>(), E.n,
-                                                                     E.d_dens_orig.as<double>());
-  AHOP_CUDA_TRY(cudaGetLastError());
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[7], st));
   return AHOP_OK;
 }
@@ -212,17 +226,19 @@ int ahop_compute_adaptahop(const double* pos_in, const double* mass_in, int64_t 
   cudaStream_t st = E.stream;
   AHOP_CUDA_TRY(E.d_pos_in.ensure(npart * 24));
   AHOP_CUDA_TRY(E.d_mass_in.ensure(npart * 8));
+  AHOP_CUDA_TRY(E.h_dens.ensure(npart * 8));
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[0], st));
   AHOP_CUDA_TRY(cudaMemcpyAsync(E.d_pos_in.p, pos_in, npart * 24, cudaMemcpyHostToDevice, st));
   AHOP_CUDA_TRY(cudaMemcpyAsync(E.d_mass_in.p, mass_in, npart * 8, cudaMemcpyHostToDevice, st));
-  if ((rc = run_pipeline(E, E.d_pos_in.as<double>(), E.d_mass_in.as<double>()))) return rc;
+  // the density goes back to the host on a copy stream during the later stages
+  if ((rc = run_pipeline(E, E.d_pos_in.as<double>(), E.d_mass_in.as<double>(), 99, E.h_dens.as<double>())))
+    return rc;
   // module outputs to host (pinned, reused across calls)
   const int64_t nused = E.prm.nusedpart > 0 ? std::min<int64_t>(E.prm.nusedpart, npart) : npart;
-  AHOP_CUDA_TRY(E.h_dens.ensure(npart * 8));
   AHOP_CUDA_TRY(E.h_liste.ensure(nused * 4));
   AHOP_CUDA_TRY(E.h_rtab.ensure((size_t)(E.nnodes > 0 ? E.nnodes : 1) * 64));
   AHOP_CUDA_TRY(E.h_itab.ensure((size_t)(E.nnodes > 0 ? E.nnodes : 1) * 24));
-  AHOP_CUDA_TRY(cudaMemcpyAsync(E.h_dens.p, E.d_dens_orig.p, npart * 8, cudaMemcpyDeviceToHost, st));
+  AHOP_CUDA_TRY(cudaStreamWaitEvent(st, E.ev_copied, 0));
   AHOP_CUDA_TRY(cudaMemcpyAsync(E.h_liste.p, E.d_liste.p, nused * 4, cudaMemcpyDeviceToHost, st));
   if (E.nnodes > 0) {
     AHOP_CUDA_TRY(cudaMemcpyAsync(E.h_rtab.p, E.d_rtab.p, (size_t)E.nnodes * 64, cudaMemcpyDeviceToHost, st));
@@ -282,7 +298,7 @@ static void release_device(Engine& E) {
                     &E.d_sad_val2, &E.d_sad_cnt, &E.d_sad_keep, &E.d_sad_kpos, &E.d_flags, &E.d_soff,
                     &E.d_sisad, &E.d_srho, &E.d_nodes, &E.d_tree_scratch, &E.d_liste, &E.d_dens_orig,
                     &E.d_rtab, &E.d_itab, &E.d_tprof, &E.d_pairs, &E.d_pair_sums, &E.d_node_aux,
-                    &E.d_forest, &E.d_moff, &E.d_misad, &E.d_mrho, &E.d_kspill};
+                    &E.d_forest, &E.d_moff, &E.d_misad, &E.d_mrho, &E.d_kspill, &E.d_task_sort};
   if (E.device >= 0) cudaSetDevice(E.device);
   for (DevBuf* b : bufs) b->release();
   E.h_liste.release(); E.h_dens.release(); E.h_rtab.release(); E.h_itab.release();

@@ -83,6 +83,8 @@ struct Engine {
   cudaStream_t stream = nullptr;  // stream of the current call
   cudaStream_t stream2 = nullptr; // structure tree: large tasks run here beside the small ones
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t stream_copy = nullptr;   // host path: density copy-out during the later stages
+  cudaEvent_t ev_dens = nullptr, ev_copied = nullptr;
   cudaEvent_t wave_ev[4] = {};          // per-wave timing (task profile only)
   float wave_prof[4 * 64] = {};         // per wave: small tasks, ms, large tasks, ms
   int32_t nwave_prof = 0;
@@ -137,6 +139,7 @@ struct Engine {
   // nodes
   DevBuf d_nodes;                        // NodeRec[nnodesmax+1]
   DevBuf d_tree_scratch;
+  DevBuf d_task_sort;                    // wave task ordering scratch
   DevBuf d_tprof;                        // per-task profile rows (debug)
   DevBuf d_forest;                       // saddle-forest scratch
   DevBuf d_moff, d_misad, d_mrho;        // saddle forest CSR (rows by decreasing saddle)

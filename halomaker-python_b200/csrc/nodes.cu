@@ -855,6 +855,21 @@ __global__ void root_deepnode_kernel(const TreeArgs A, const int32_t* flag, cons
   if (flag[k]) A.deepnode[A.GL[i]] = 1 + rank[k];
 }
 
+// order a wave's small tasks by decreasing size (long tasks start first, so
+// the wave does not end on one late long task)
+__global__ void task_keys_kernel(const Task* __restrict__ t, int32_t n, uint32_t* keys, int32_t* vals) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  keys[i] = ~(uint32_t)(t[i].b - t[i].a);
+  vals[i] = i;
+}
+
+__global__ void task_gather_kernel(const Task* __restrict__ in, const int32_t* __restrict__ idx, int32_t n,
+                                   Task* __restrict__ out) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[idx[i]];
+}
+
 // Dynamic shared memory of a task block: exact-sum staging (kTermWarps warps),
 // reorder keys, warp-linked row positions.
 __host__ __device__ constexpr size_t wave_dyn_smem(int nt) {
@@ -1539,6 +1554,27 @@ int stage_nodes(Engine& E) {
     A.next = tasks[cur ^ 1];
     A.next_big = tasksB[cur ^ 1];
     AHOP_CUDA_TRY(cudaMemsetAsync(A.nnext, 0, 8, st));
+    if (nsmall > 2048) {
+      const size_t nb = (size_t)nsmall;
+      AHOP_CUDA_TRY(E.d_task_sort.ensure(nb * 16 + nb * sizeof(Task) + 256));
+      uint32_t* k0 = E.d_task_sort.as<uint32_t>();
+      uint32_t* k1 = k0 + nb;
+      int32_t* v0 = reinterpret_cast<int32_t*>(k1 + nb);
+      int32_t* v1 = v0 + nb;
+      Task* tmp = reinterpret_cast<Task*>(reinterpret_cast<char*>(E.d_task_sort.p) + ((nb * 16 + 255) & ~size_t(255)));
+      E.launches += 2;
+      task_keys_kernel<<<(unsigned)((nb + T - 1) / T), T, 0, st>>>(tasks[cur], nsmall, k0, v0);
+      cub::DoubleBuffer<uint32_t> kb(k0, k1);
+      cub::DoubleBuffer<int32_t> vb(v0, v1);
+      size_t t1 = 0;
+      cub::DeviceRadixSort::SortPairs(nullptr, t1, kb, vb, nsmall, 0, 32, st);
+      AHOP_CUDA_TRY(E.d_cub.ensure(t1));
+      E.cub_calls++;
+      AHOP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(E.d_cub.p, t1, kb, vb, nsmall, 0, 32, st));
+      task_gather_kernel<<<(unsigned)((nb + T - 1) / T), T, 0, st>>>(tasks[cur], vb.Current(), nsmall, tmp);
+      AHOP_CUDA_TRY(cudaMemcpyAsync(tasks[cur], tmp, nb * sizeof(Task), cudaMemcpyDeviceToDevice, st));
+      AHOP_CUDA_TRY(cudaGetLastError());
+    }
     const bool prof = E.task_profile && wave < kMaxProfiledWaves;
     if (prof && !E.wave_ev[0]) {
       for (auto& e : E.wave_ev) AHOP_CUDA_TRY(cudaEventCreate(&e));
