@@ -48,8 +48,11 @@ namespace ahop {
 constexpr int kNT = 256;        // threads per task block (grid-wide root kernels, small tasks)
 constexpr int kNTBig = 1024;    // threads per block for tasks of more than Engine::big_task groups
 constexpr int kTermWarps = 8;   // warps that sum large groups in an exact pass
+constexpr int kSmallComp = 4;   // components of at most this many groups are decided by one thread
 constexpr int kIPT = 4;         // items per thread in the reorder sort (2 for 1024-thread blocks)
 __host__ __device__ constexpr int ipt_for(int nt) { return nt >= 1024 ? 2 : kIPT; }
+// groups whose union-find parents a task block keeps in shared memory
+__host__ __device__ constexpr int par_cap(int nt) { return nt >= 1024 ? 32768 : 1024; }
 constexpr int kBigGroup = 96;   // groups larger than this are summed by a warp
 constexpr int kRowWarp = 32;    // saddle-row prefixes longer than this are linked by a warp
 constexpr int kMaxBigRows = 512;
@@ -221,10 +224,15 @@ struct SharedTask {
 template <int NT, class SortT, class ScanT, class MaxScanT>
 __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT::TempStorage& sort_tmp,
                                 typename ScanT::TempStorage& scan_tmp, typename MaxScanT::TempStorage& maxscan_tmp,
-                                int32_t* s_keys, int32_t* s_big, long long* ph) {
+                                int32_t* s_keys, int32_t* s_big, int32_t* s_par, long long* ph) {
   constexpr int IPT = ipt_for(NT);
   const int tid = threadIdx.x;
   const int32_t a = T.a, b = T.b;
+  // union-find parents: in shared memory when the task fits (entries relative
+  // to a), else the global array (absolute positions)
+  const bool local = (b - a) <= par_cap(NT);
+  int32_t* par = local ? s_par : A.par;
+  const int32_t poff = local ? a : 0;
   const double rhot = T.rhot;
   long long tl = clock64();
   // thread 0 charges the cycles since the last mark to phase k
@@ -233,7 +241,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   };
   if (tid == 0) { T.next_event = DBL_MAX; T.nbig = 0; }
   for (int32_t i = a + tid; i < b; i += NT) {
-    A.par[i] = i;
+    par[i - poff] = i - poff;
     A.cnt[i] = 0;
     A.run[i] = 0;
   }
@@ -262,7 +270,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
       const int32_t h = A.sisad[e];
       const int32_t j = A.pos_of[h];
       if (j < a || j >= b) { set_err(A, 11, g); continue; }  // f90:1229-1233
-      if (h > g) uf_union(A.par, i, j);
+      if (h > g) uf_union(par, i - poff, j - poff);
     }
   }
 #pragma unroll
@@ -280,7 +288,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
         const int32_t h = A.sisad[e];
         const int32_t j = A.pos_of[h];
         if (j < a || j >= b) { set_err(A, 11, g); continue; }
-        if (h > g) uf_union(A.par, i, j);
+        if (h > g) uf_union(par, i - poff, j - poff);
       }
     }
   }
@@ -289,11 +297,11 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   for (int32_t i = a + tid; i < b; i += NT) {
     int32_t g = A.GL[i];
     if (A.densg[g] > rhot) {
-      int32_t r = uf_find(A.par, i);
-      A.par[i] = r;
-      atomicAdd(&A.cnt[r], 1);
+      const int32_t r = uf_find(par, i - poff);
+      par[i - poff] = r;
+      atomicAdd(&A.cnt[r + poff], 1);
     } else {
-      A.par[i] = -1;
+      par[i - poff] = -1;
     }
   }
   __syncthreads();
@@ -322,8 +330,8 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
       int32_t i = c0 + tid * IPT + k;
-      int32_t r = (i < b) ? A.par[i] : -1;
-      keys[k] = (r >= 0) ? (r - a) : sent;
+      int32_t r = (i < b) ? par[i - poff] : -1;
+      keys[k] = (r >= 0) ? (r + poff - a) : sent;
       vals[k] = i;
     }
     SortT(sort_tmp).Sort(keys, vals, 0, kbits);
@@ -371,7 +379,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   carry = 0;
   for (int32_t c0 = a; c0 < b; c0 += NT) {
     int32_t i = c0 + tid;
-    int32_t isroot = (i < b && A.par[i] == i) ? 1 : 0;
+    int32_t isroot = (i < b && par[i - poff] == i - poff) ? 1 : 0;
     int32_t ex, tot;
     ScanT(scan_tmp).ExclusiveSum(isroot, ex, tot);
     __syncthreads();
@@ -464,41 +472,11 @@ __device__ __forceinline__ void position_terms(const TreeArgs& A, int32_t i, dou
 // Sum the gs rows of positions [c0, c1) over one warp and decide the
 // significance test (f90:1459-1463) in three states from the rigorous
 // rounding bounds; lane 0 writes cs row C.
-__device__ void component_decide(const TreeArgs& A, int32_t c0, int32_t c1, double rhot, double* C, int lane) {
+// The three-state significance test (f90:1459-1463) from a component's
+// approximate sums; writes cs row C.
+__device__ void decide_from_sums(const TreeArgs& A, double rhot, long long nl, int32_t nmax, double dmax, double S,
+                                 double M, double Sx, double Sy, double Sz, double Q, int triB, double* C) {
   const double u = 1.1102230246251565e-16;
-  long long nl = 0;
-  int32_t nmax = 0;
-  double dmax = -1.0, S = 0, M = 0, Sx = 0, Sy = 0, Sz = 0, Q = 0;
-  int triB = kFalse;  // densmoy_comp_max > rhot
-#pragma unroll 4
-  for (int32_t i = c0 + lane; i < c1; i += 32) {
-    const double* G = A.gs + 8 * (size_t)i;
-    const int32_t ng = A.gn[i];
-    nl += ng;
-    nmax = max(nmax, ng);
-    dmax = fmax(dmax, G[0]);
-    S += G[1];
-    M += G[2];
-    Sx += G[3];
-    Sy += G[4];
-    Sz += G[5];
-    Q += G[6];
-    triB = tri_or(triB, (int)G[7]);
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    nl += __shfl_xor_sync(0xffffffffu, nl, o);
-    nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
-    dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
-    S += __shfl_xor_sync(0xffffffffu, S, o);
-    M += __shfl_xor_sync(0xffffffffu, M, o);
-    Sx += __shfl_xor_sync(0xffffffffu, Sx, o);
-    Sy += __shfl_xor_sync(0xffffffffu, Sy, o);
-    Sz += __shfl_xor_sync(0xffffffffu, Sz, o);
-    Q += __shfl_xor_sync(0xffffffffu, Q, o);
-    triB = tri_or(triB, __shfl_xor_sync(0xffffffffu, triB, o));
-  }
-  if (lane != 0) return;
   const double n = (double)nl;
   C[0] = n; C[1] = (double)nmax; C[2] = dmax; C[3] = S;
   C[4] = M; C[5] = Sx; C[6] = Sy; C[7] = Sz; C[8] = Q;
@@ -536,6 +514,66 @@ __device__ void component_decide(const TreeArgs& A, int32_t c0, int32_t c1, doub
   C[10] = (dec == 2) ? 1.0 : 0.0;  // undecided: recompute exactly
 }
 
+// component_decide for a small component on one thread (no shuffles)
+__device__ void component_decide_thread(const TreeArgs& A, int32_t c0, int32_t c1, double rhot, double* C) {
+  long long nl = 0;
+  int32_t nmax = 0;
+  double dmax = -1.0, S = 0, M = 0, Sx = 0, Sy = 0, Sz = 0, Q = 0;
+  int triB = kFalse;
+  for (int32_t i = c0; i < c1; ++i) {
+    const double* G = A.gs + 8 * (size_t)i;
+    const int32_t ng = A.gn[i];
+    nl += ng;
+    nmax = max(nmax, ng);
+    dmax = fmax(dmax, G[0]);
+    S += G[1];
+    M += G[2];
+    Sx += G[3];
+    Sy += G[4];
+    Sz += G[5];
+    Q += G[6];
+    triB = tri_or(triB, (int)G[7]);
+  }
+  decide_from_sums(A, rhot, nl, nmax, dmax, S, M, Sx, Sy, Sz, Q, triB, C);
+}
+
+__device__ void component_decide(const TreeArgs& A, int32_t c0, int32_t c1, double rhot, double* C, int lane) {
+  long long nl = 0;
+  int32_t nmax = 0;
+  double dmax = -1.0, S = 0, M = 0, Sx = 0, Sy = 0, Sz = 0, Q = 0;
+  int triB = kFalse;  // densmoy_comp_max > rhot
+#pragma unroll 4
+  for (int32_t i = c0 + lane; i < c1; i += 32) {
+    const double* G = A.gs + 8 * (size_t)i;
+    const int32_t ng = A.gn[i];
+    nl += ng;
+    nmax = max(nmax, ng);
+    dmax = fmax(dmax, G[0]);
+    S += G[1];
+    M += G[2];
+    Sx += G[3];
+    Sy += G[4];
+    Sz += G[5];
+    Q += G[6];
+    triB = tri_or(triB, (int)G[7]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    nl += __shfl_xor_sync(0xffffffffu, nl, o);
+    nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+    dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    S += __shfl_xor_sync(0xffffffffu, S, o);
+    M += __shfl_xor_sync(0xffffffffu, M, o);
+    Sx += __shfl_xor_sync(0xffffffffu, Sx, o);
+    Sy += __shfl_xor_sync(0xffffffffu, Sy, o);
+    Sz += __shfl_xor_sync(0xffffffffu, Sz, o);
+    Q += __shfl_xor_sync(0xffffffffu, Q, o);
+    triB = tri_or(triB, __shfl_xor_sync(0xffffffffu, triB, o));
+  }
+  if (lane != 0) return;
+  decide_from_sums(A, rhot, nl, nmax, dmax, S, M, Sx, Sy, Sz, Q, triB, C);
+}
+
 // Approximate statistics of every component of the task: anchors, then the
 // groups' terms position-parallel over the whole block, then a warp per
 // component sums them and decides.
@@ -554,8 +592,15 @@ __device__ void approx_stats(const TreeArgs& A, SharedTask& T) {
   __syncthreads();
   for (int32_t i = a + tid; i < b; i += NT) position_terms(A, i, rhot, A.cs + 12 * (size_t)(a + A.compidx[i]) + 9);
   __syncthreads();
-  for (int32_t k = warp; k < ncomp; k += NT / 32)
-    component_decide(A, A.cstart[a + k], comp_end(A, T, k), rhot, A.cs + 12 * (size_t)(a + k), lane);
+  // components of a few groups on one thread each, larger ones a warp each
+  for (int32_t k = tid; k < ncomp; k += NT) {
+    const int32_t c0 = A.cstart[a + k], c1 = comp_end(A, T, k);
+    if (c1 - c0 <= kSmallComp) component_decide_thread(A, c0, c1, rhot, A.cs + 12 * (size_t)(a + k));
+  }
+  for (int32_t k = warp; k < ncomp; k += NT / 32) {
+    const int32_t c0 = A.cstart[a + k], c1 = comp_end(A, T, k);
+    if (c1 - c0 > kSmallComp) component_decide(A, c0, c1, rhot, A.cs + 12 * (size_t)(a + k), lane);
+  }
   __syncthreads();
 }
 
@@ -871,9 +916,11 @@ __global__ void task_gather_kernel(const Task* __restrict__ in, const int32_t* _
 }
 
 // Dynamic shared memory of a task block: exact-sum staging (kTermWarps warps),
-// reorder keys, warp-linked row positions.
+// reorder keys, warp-linked row positions, union-find parents of tasks of at
+// most par_cap groups.
 __host__ __device__ constexpr size_t wave_dyn_smem(int nt) {
-  return (size_t)kTermWarps * 32 * 6 * 8 + (size_t)nt * ipt_for(nt) * 4 + (size_t)kMaxBigRows * 4;
+  return (size_t)kTermWarps * 32 * 6 * 8 + (size_t)nt * ipt_for(nt) * 4 + (size_t)kMaxBigRows * 4 +
+         (size_t)par_cap(nt) * 4;
 }
 
 template <int NT>
@@ -888,6 +935,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
   double* s_terms = reinterpret_cast<double*>(wave_dyn);
   int32_t* s_keys = reinterpret_cast<int32_t*>(wave_dyn + (size_t)kTermWarps * 32 * 6 * 8);
   int32_t* s_big = s_keys + NT * ipt_for(NT);
+  int32_t* s_par = s_big + kMaxBigRows;
   __shared__ SharedTask T;
   __shared__ long long s_clk[6];  // structural, approx, exact cycles; levels; structural passes; max ncomp
   __shared__ long long s_ph[8];   // cycles per phase of the structural passes
@@ -912,7 +960,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
     __syncthreads();
     long long c0 = clock64();
     if (restructure) {
-      structural_pass<NT, SortT, ScanT, MaxScanT>(A, T, sort_tmp, scan_tmp, maxscan_tmp, s_keys, s_big, s_ph);
+      structural_pass<NT, SortT, ScanT, MaxScanT>(A, T, sort_tmp, scan_tmp, maxscan_tmp, s_keys, s_big, s_par, s_ph);
       if (tid == 0) { atomicAdd(&A.stats[7], 1ULL); s_clk[4] += 1; }
     }
     long long c1 = clock64();
