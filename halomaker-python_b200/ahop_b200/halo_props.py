@@ -27,7 +27,11 @@ class AhopHaloParams(C.Structure):
 
 class AhopHaloTimings(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("moments", "epot64", "epot32c", "finalize", "total")] + [
-        ("pairs", C.c_double), ("items", C.c_int32), ("kernel_launches", C.c_int32)]
+        ("pairs", C.c_double), ("items", C.c_int32), ("kernel_launches", C.c_int32), ("tune_ms", C.c_float),
+        ("graph_replays", C.c_int32)]
+
+
+BUCKETS = 5  # halo-size buckets of the FP32 pair kernel's tile shape: n < 512, 4096, 32768, 262144, larger
 
 
 _bound = False
@@ -42,6 +46,9 @@ def _lib():
         lib.ahop_halo_props_device.argtypes = [C.POINTER(AhopHaloParams), C.c_void_p, C.c_int64, C.c_void_p,
                                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.ahop_halo_get_timings.argtypes = [C.POINTER(AhopHaloTimings)]
+        lib.ahop_halo_get_tiles.argtypes = [C.c_void_p, C.c_void_p]
+        lib.ahop_halo_set_tiles.argtypes = [C.c_void_p]
+        lib.ahop_halo_set_graph.argtypes = [C.c_int32]
         _bound = True
     return lib
 
@@ -99,6 +106,32 @@ def timings() -> dict:
     t = AhopHaloTimings()
     L.check(_lib().ahop_halo_get_timings(C.byref(t)), "halo_get_timings")
     return {n: getattr(t, n) for n, _ in AhopHaloTimings._fields_}
+
+
+def tiles() -> dict:
+    """Rows per work item of the FP32-compensated pair kernel per halo-size
+    bucket (0 = not tuned yet) and the autotuner's times (ms) per shape."""
+    rows = np.zeros(BUCKETS, np.int32)
+    ms = np.zeros(BUCKETS * 3, np.float32)
+    L.check(_lib().ahop_halo_get_tiles(rows.ctypes.data, ms.ctypes.data), "halo_get_tiles")
+    return {"rows": rows.tolist(), "tune_ms": ms.reshape(BUCKETS, 3).tolist()}
+
+
+def set_tiles(rows=None) -> None:
+    """Pin rows per item (128, 256 or 512; 0 = autotune) per bucket; None
+    forgets every pin and every tuned shape."""
+    if rows is None:
+        L.check(_lib().ahop_halo_set_tiles(None), "halo_set_tiles")
+        return
+    r = np.ascontiguousarray(rows, np.int32)
+    if r.shape != (BUCKETS,):
+        raise ValueError(f"rows must have {BUCKETS} entries")
+    L.check(_lib().ahop_halo_set_tiles(r.ctypes.data), "halo_set_tiles")
+
+
+def set_graph(on: bool) -> None:
+    """Capture and replay the launch sequence as a CUDA graph (default on)."""
+    L.check(_lib().ahop_halo_set_graph(int(bool(on))), "halo_set_graph")
 
 
 # ---------------------------------------------------------------- virial step

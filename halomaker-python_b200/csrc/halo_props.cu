@@ -33,6 +33,8 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <chrono>
+#include <cstring>
 #include <cub/cub.cuh>
 
 #include "ahop_halo.h"
@@ -51,7 +53,7 @@ __device__ __forceinline__ double wrap_chp(double d, double L, double h, int per
   return d;
 }
 
-template <class T>
+template <class T, int NT = kPB>
 __device__ __forceinline__ T block_sum(T v, T* sh) {
   const int tid = threadIdx.x;
 #pragma unroll
@@ -60,7 +62,7 @@ __device__ __forceinline__ T block_sum(T v, T* sh) {
   __syncthreads();
   T r = 0;
   if (tid < 32) {
-    r = (tid < kPB / 32) ? sh[tid] : T(0);
+    r = (tid < NT / 32) ? sh[tid] : T(0);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
   }
@@ -247,14 +249,33 @@ __global__ void __launch_bounds__(kPB) halo_moments_kernel(HaloArgs A) {
   }
 }
 
-// Potential pair sums.  Work item w: halo item_h[w], i-tile start item_i[w].
-template <bool FP32C>
-__global__ void __launch_bounds__(kPB) epot_pairs_kernel(HaloArgs A, const int32_t* __restrict__ item_h,
-                                                         const int32_t* __restrict__ item_i, int32_t nitems,
-                                                         int32_t* __restrict__ counter, double* __restrict__ part) {
-  __shared__ float4 s_h[kPB], s_l[kPB];  // FP32 form: (hi x, hi y, hi z, mass), (lo x, lo y, lo z, -)
-  __shared__ double s_dx[kPB], s_dy[kPB], s_dz[kPB], s_dm[kPB];
-  __shared__ double sh[kPB / 32];
+// ---------------------------------------------------------------- pair sums
+// Work item: member rows [i0, i0 + rows) of halo h against partners
+// j in [j0, j1), j > i.  j0 is either i0 (the item holds the diagonal tile) or
+// i0 plus a multiple of the row count, so partner tiles line up with the row
+// tile.  A halo's items cover every pair once; item partials are folded per
+// halo in halo order by epot_finalize_kernel, so the result does not depend on
+// the schedule.
+struct PairItem {
+  int32_t h, i0, j0, j1;
+};
+
+constexpr int kT64 = 256;  // FP64 form: rows per item = threads per block = partner tile
+
+__device__ __forceinline__ void rel_pos(const HaloArgs& A, int64_t k, double cx, double cy, double cz,
+                                        double& rx, double& ry, double& rz) {
+  rx = wrap_chp(A.pos[3 * k] - cx, A.L, A.h, A.periodic);
+  ry = wrap_chp(A.pos[3 * k + 1] - cy, A.L, A.h, A.periodic);
+  rz = wrap_chp(A.pos[3 * k + 2] - cz, A.L, A.h, A.periodic);
+}
+
+// Plain FP64 form: relative positions, 1/r from the double reciprocal square
+// root, one row per thread, partner tiles of 256 in shared memory.
+__global__ void __launch_bounds__(kT64) epot64_kernel(HaloArgs A, const PairItem* __restrict__ items,
+                                                      int32_t nitems, int32_t* __restrict__ counter,
+                                                      double* __restrict__ part) {
+  __shared__ double s_dx[kT64], s_dy[kT64], s_dz[kT64], s_dm[kT64];
+  __shared__ double sh[kT64 / 32];
   __shared__ int32_t s_item;
   const int tid = threadIdx.x;
   for (;;) {
@@ -263,95 +284,142 @@ __global__ void __launch_bounds__(kPB) epot_pairs_kernel(HaloArgs A, const int32
     const int32_t w = s_item;
     __syncthreads();
     if (w >= nitems) break;
-    const int32_t h = item_h[w];
-    const int64_t base = A.off[h];
-    const int32_t n = (int32_t)(A.off[h + 1] - base);
-    const int32_t i0 = item_i[w];
-    const double* c = A.out + (size_t)kHaloFields * h;
+    const PairItem it = items[w];
+    const int64_t base = A.off[it.h];
+    const int32_t n = (int32_t)(A.off[it.h + 1] - base);
+    const double* c = A.out + (size_t)kHaloFields * it.h;
     const double cx = c[HP_PX], cy = c[HP_PY], cz = c[HP_PZ];
-    const int32_t i = i0 + tid;
+    const int32_t i = it.i0 + tid;
     const bool vi = i < n;
     double rxi = 0, ryi = 0, rzi = 0;
-    if (vi) {
-      rxi = wrap_chp(A.pos[3 * (base + i)] - cx, A.L, A.h, A.periodic);
-      ryi = wrap_chp(A.pos[3 * (base + i) + 1] - cy, A.L, A.h, A.periodic);
-      rzi = wrap_chp(A.pos[3 * (base + i) + 2] - cz, A.L, A.h, A.periodic);
-    }
-    const float hxi = (float)rxi, hyi = (float)ryi, hzi = (float)rzi;
-    const float lxi = (float)(rxi - (double)hxi), lyi = (float)(ryi - (double)hyi), lzi = (float)(rzi - (double)hzi);
-    float ks = 0.f, kc = 0.f;  // Kahan sum / compensation (FP32 form)
-    double ds = 0.0;           // FP64 form
-    for (int32_t j0 = i0; j0 < n; j0 += kPB) {
+    if (vi) rel_pos(A, base + i, cx, cy, cz, rxi, ryi, rzi);
+    double ds = 0.0;
+    for (int32_t j0 = it.j0; j0 < it.j1; j0 += kT64) {
       const int32_t j = j0 + tid;
-      if (j < n) {
-        const double rx = wrap_chp(A.pos[3 * (base + j)] - cx, A.L, A.h, A.periodic);
-        const double ry = wrap_chp(A.pos[3 * (base + j) + 1] - cy, A.L, A.h, A.periodic);
-        const double rz = wrap_chp(A.pos[3 * (base + j) + 2] - cz, A.L, A.h, A.periodic);
-        if (FP32C) {
-          const float hx = (float)rx, hy = (float)ry, hz = (float)rz;
-          s_h[tid] = make_float4(hx, hy, hz, (float)A.mass[base + j]);
-          s_l[tid] = make_float4((float)(rx - (double)hx), (float)(ry - (double)hy), (float)(rz - (double)hz), 0.f);
-        } else {
-          s_dx[tid] = rx; s_dy[tid] = ry; s_dz[tid] = rz; s_dm[tid] = A.mass[base + j];
-        }
+      if (j < it.j1) {
+        double rx, ry, rz;
+        rel_pos(A, base + j, cx, cy, cz, rx, ry, rz);
+        s_dx[tid] = rx; s_dy[tid] = ry; s_dz[tid] = rz; s_dm[tid] = A.mass[base + j];
       } else {
-        if (FP32C) { s_h[tid] = make_float4(3.0e30f, 3.0e30f, 3.0e30f, 0.f); s_l[tid] = make_float4(0.f, 0.f, 0.f, 0.f); }
-        else { s_dm[tid] = 0.0; s_dx[tid] = s_dy[tid] = s_dz[tid] = 3.0e30; }
+        s_dm[tid] = 0.0; s_dx[tid] = s_dy[tid] = s_dz[tid] = 3.0e30;
       }
       __syncthreads();
       if (vi) {
-        const int jstart = (j0 == i0) ? tid + 1 : 0;  // j > i on the diagonal tile
-        const int jend = min(kPB, n - j0);
-        if (FP32C) {
-#pragma unroll 8
-          for (int jj = jstart; jj < jend; ++jj) {
-            const float4 hj = s_h[jj], lj = s_l[jj];
-            const float dx = (hj.x - hxi) + (lj.x - lxi);
-            const float dy = (hj.y - hyi) + (lj.y - lyi);
-            const float dz = (hj.z - hzi) + (lj.z - lzi);
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            // hardware reciprocal square root (a few ulp): per-halo sums stay
-            // within the 1e-6 bound of the FP64 form (checked by the tests)
-            const float t = (r2 > 0.f) ? hj.w * rsqrtf(r2) : 0.f;
-            const float y = t - kc;
-            const float s2 = ks + y;
-            kc = (s2 - ks) - y;
-            ks = s2;
-          }
-        } else {
+        const int jstart = (j0 == it.i0) ? tid + 1 : 0;  // j > i on the diagonal tile
+        const int jend = min(kT64, it.j1 - j0);
 #pragma unroll 4
-          for (int jj = jstart; jj < jend; ++jj) {
-            const double dx = s_dx[jj] - rxi, dy = s_dy[jj] - ryi, dz = s_dz[jj] - rzi;
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 > 0.0) ds += s_dm[jj] * rsqrt(r2);
-          }
+        for (int jj = jstart; jj < jend; ++jj) {
+          const double dx = s_dx[jj] - rxi, dy = s_dy[jj] - ryi, dz = s_dz[jj] - rzi;
+          const double r2 = dx * dx + dy * dy + dz * dz;
+          if (r2 > 0.0) ds += s_dm[jj] * rsqrt(r2);
         }
       }
       __syncthreads();
     }
-    double mine = 0.0;
-    if (vi) {
-      const double mi = A.mass[base + i];
-      mine = FP32C ? mi * ((double)ks - (double)kc) : mi * ds;
-    }
-    const double tot = block_sum(mine, sh);
+    const double tot = block_sum(vi ? A.mass[base + i] * ds : 0.0, sh);
     if (tid == 0) part[w] = tot;
   }
 }
 
-// FP32-compensated pair sums with two i-rows per thread: 128 threads cover
-// an item's 256 rows (rows tid and tid + 128), so every float4 pair of
-// shared-memory loads serves two pairs.  Same schedule, same per-item partial
-// and the same arithmetic per pair as epot_pairs_kernel<true>.
-constexpr int kPB2 = kPB / 2;
+// FP32-compensated form on packed FP32 pairs (the sm_100 f32x2 add/sub/mul/fma
+// instructions: two lanes per 64-bit register, one instruction).  Positions
+// relative to the halo centre are split into hi = float(r) and
+// lo = float(r - hi); a separation is (hi_j - hi_i) + (lo_j - lo_i).  The two
+// lanes of every packed register hold two partners j, 2q and 2q+1, of the same
+// row i, so a row's own coordinates are loop-invariant (hi_i, hi_i) pairs.
+// Each thread owns kR32 rows (rows tid + 128 r); partner tiles are 128 * R
+// wide, shared memory holds them as packed pairs.  For every row, eight
+// partner pairs (16 terms) are accumulated by a fused multiply-add chain per
+// lane, then enter a Kahan-compensated FP32 sum; rows fold into FP64 per item.
+// Separations of exactly zero (coincident members) are excluded like in the
+// FP64 form: the fast path does not test for them -- rsqrt(0) = inf makes the
+// row's sum non-finite, and the block then recomputes the item with a
+// per-pair test.  The tile shape (R = 1, 2 or 4 rows per thread) is chosen
+// per halo-size bucket by the host-side autotuner and read per item.
+typedef unsigned long long f2_t;
 
-__device__ __forceinline__ float pair_term(const float4& hj, const float4& lj, float hx, float hy, float hz,
-                                           float lx, float ly, float lz) {
-  const float dx = (hj.x - hx) + (lj.x - lx);
-  const float dy = (hj.y - hy) + (lj.y - ly);
-  const float dz = (hj.z - hz) + (lj.z - lz);
-  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  return (r2 > 0.f) ? hj.w * rsqrtf(r2) : 0.f;
+__device__ __forceinline__ f2_t f2_pack(float a, float b) {
+  f2_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(f2_t v, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ f2_t f2_add(f2_t a, f2_t b) {
+  f2_t r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2_t f2_sub(f2_t a, f2_t b) {
+  f2_t r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2_t f2_mul(f2_t a, f2_t b) {
+  f2_t r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2_t f2_fma(f2_t a, f2_t b, f2_t c) {
+  f2_t r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+constexpr int kB32 = 128;              // threads per block of the FP32 form
+constexpr int kMaxR32 = 4;             // rows per thread, largest shape
+constexpr int kMaxT32 = kB32 * kMaxR32;
+constexpr int kGroup32 = 8;            // partner pairs per compensated fold
+constexpr int kChunkJ = 32768;         // partners per item at most (a multiple of every tile width)
+constexpr float kFar = 1.0e18f;        // padding position: its terms vanish (mass 0, finite r)
+
+struct Tile32 {
+  float4 a[kMaxT32 / 2];  // hi x(2q), x(2q+1), y(2q), y(2q+1)
+  float4 b[kMaxT32 / 2];  // hi z(2q), z(2q+1), mass(2q), mass(2q+1)
+  float4 c[kMaxT32 / 2];  // lo x, x, y, y
+  float2 d[kMaxT32 / 2];  // lo z, z
+};
+
+__device__ __forceinline__ void split_hilo(double r, float& hi, float& lo) {
+  hi = (float)r;
+  lo = (float)(r - (double)hi);
+}
+
+// Stage partners [j0, j0 + T) (T = 128 R) of one item; slots past j1 get the
+// padding (mass 0, far away).
+template <int R>
+__device__ __forceinline__ void stage_tile32(Tile32& S, const HaloArgs& A, int64_t base, int32_t j0, int32_t j1,
+                                             double cx, double cy, double cz) {
+  constexpr int P = kB32 * R / 2;
+  for (int q = threadIdx.x; q < P; q += kB32) {
+    float hx[2], hy[2], hz[2], m[2], lx[2], ly[2], lz[2];
+#pragma unroll
+    for (int l = 0; l < 2; ++l) {
+      const int32_t j = j0 + 2 * q + l;
+      if (j < j1) {
+        double rx, ry, rz;
+        rel_pos(A, base + j, cx, cy, cz, rx, ry, rz);
+        split_hilo(rx, hx[l], lx[l]);
+        split_hilo(ry, hy[l], ly[l]);
+        split_hilo(rz, hz[l], lz[l]);
+        m[l] = (float)A.mass[base + j];
+      } else {
+        hx[l] = hy[l] = hz[l] = kFar;
+        lx[l] = ly[l] = lz[l] = 0.f;
+        m[l] = 0.f;
+      }
+    }
+    S.a[q] = make_float4(hx[0], hx[1], hy[0], hy[1]);
+    S.b[q] = make_float4(hz[0], hz[1], m[0], m[1]);
+    S.c[q] = make_float4(lx[0], lx[1], ly[0], ly[1]);
+    S.d[q] = make_float2(lz[0], lz[1]);
+  }
 }
 
 __device__ __forceinline__ void kahan_add(float t, float& ks, float& kc) {
@@ -361,17 +429,125 @@ __device__ __forceinline__ void kahan_add(float t, float& ks, float& kc) {
   ks = s2;
 }
 
-__device__ __forceinline__ void kahan_pair(const float4& hj, const float4& lj, float hx, float hy, float hz,
-                                           float lx, float ly, float lz, float& ks, float& kc) {
-  kahan_add(pair_term(hj, lj, hx, hy, hz, lx, ly, lz), ks, kc);
+// One partner (tile slot jj) of one row with the zero-separation test; the
+// per-pair path of the diagonal tile and of the recomputation.
+__device__ __forceinline__ void pair_checked(const Tile32& S, int jj, float hx, float hy, float hz, float lx,
+                                             float ly, float lz, float& ks, float& kc) {
+  const int q = jj >> 1, l = jj & 1;
+  const float* a = reinterpret_cast<const float*>(&S.a[q]);
+  const float* b = reinterpret_cast<const float*>(&S.b[q]);
+  const float* c = reinterpret_cast<const float*>(&S.c[q]);
+  const float* d = reinterpret_cast<const float*>(&S.d[q]);
+  const float dx = (a[l] - hx) + (c[l] - lx);
+  const float dy = (a[2 + l] - hy) + (c[2 + l] - ly);
+  const float dz = (b[l] - hz) + (d[l] - lz);
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  if (r2 > 0.f) kahan_add(b[2 + l] * rsqrtf(r2), ks, kc);
 }
 
-__global__ void __launch_bounds__(kPB2) epot_pairs32_kernel(HaloArgs A, const int32_t* __restrict__ item_h,
-                                                            const int32_t* __restrict__ item_i, int32_t nitems,
-                                                            int32_t* __restrict__ counter,
-                                                            double* __restrict__ part) {
-  __shared__ float4 s_h[kPB], s_l[kPB];
-  __shared__ double sh[kPB2 / 32];
+template <int R>
+__device__ double epot32_item(Tile32& S, double* sh, const HaloArgs& A, const PairItem& it, bool checked) {
+  constexpr int T = kB32 * R;
+  const int tid = threadIdx.x;
+  const int64_t base = A.off[it.h];
+  const int32_t n = (int32_t)(A.off[it.h + 1] - base);
+  const double* cen = A.out + (size_t)kHaloFields * it.h;
+  const double cx = cen[HP_PX], cy = cen[HP_PY], cz = cen[HP_PZ];
+  float hx[R], hy[R], hz[R], lx[R], ly[R], lz[R];
+  f2_t HX[R], HY[R], HZ[R], LX[R], LY[R], LZ[R], ks[R], kc[R];
+  float ksd[R], kcd[R];  // per-pair path sums
+  bool vi[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int32_t i = it.i0 + tid + kB32 * r;
+    vi[r] = i < n;
+    if (vi[r]) {
+      double rx, ry, rz;
+      rel_pos(A, base + i, cx, cy, cz, rx, ry, rz);
+      split_hilo(rx, hx[r], lx[r]);
+      split_hilo(ry, hy[r], ly[r]);
+      split_hilo(rz, hz[r], lz[r]);
+    } else {
+      // far on the other side from the padding: every separation stays finite
+      hx[r] = hy[r] = hz[r] = -kFar;
+      lx[r] = ly[r] = lz[r] = 0.f;
+    }
+    HX[r] = f2_pack(hx[r], hx[r]); HY[r] = f2_pack(hy[r], hy[r]); HZ[r] = f2_pack(hz[r], hz[r]);
+    LX[r] = f2_pack(lx[r], lx[r]); LY[r] = f2_pack(ly[r], ly[r]); LZ[r] = f2_pack(lz[r], lz[r]);
+    ks[r] = kc[r] = 0ull;
+    ksd[r] = kcd[r] = 0.f;
+  }
+  for (int32_t j0 = it.j0; j0 < it.j1; j0 += T) {
+    stage_tile32<R>(S, A, base, j0, it.j1, cx, cy, cz);
+    __syncthreads();
+    const int jend = min(T, it.j1 - j0);
+    if (j0 == it.i0 || checked) {
+      // per-pair path: j > i on the diagonal tile, every pair when recomputing
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        if (!vi[r]) continue;
+        const int jstart = (j0 == it.i0) ? tid + kB32 * r + 1 : 0;
+        for (int jj = jstart; jj < jend; ++jj)
+          pair_checked(S, jj, hx[r], hy[r], hz[r], lx[r], ly[r], lz[r], ksd[r], kcd[r]);
+      }
+    } else {
+      const int np = ((jend + 2 * kGroup32 - 1) / (2 * kGroup32)) * kGroup32;  // partner pairs, padded
+      const ulonglong2* Sa = reinterpret_cast<const ulonglong2*>(S.a);
+      const ulonglong2* Sb = reinterpret_cast<const ulonglong2*>(S.b);
+      const ulonglong2* Sc = reinterpret_cast<const ulonglong2*>(S.c);
+      const f2_t* Sd = reinterpret_cast<const f2_t*>(S.d);
+      for (int q0 = 0; q0 < np; q0 += kGroup32) {
+        f2_t acc[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) acc[r] = 0ull;
+#pragma unroll
+        for (int g = 0; g < kGroup32; ++g) {
+          const ulonglong2 pa = Sa[q0 + g], pb = Sb[q0 + g], pc = Sc[q0 + g];
+          const f2_t pd = Sd[q0 + g];
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const f2_t dx = f2_add(f2_sub(pa.x, HX[r]), f2_sub(pc.x, LX[r]));
+            const f2_t dy = f2_add(f2_sub(pa.y, HY[r]), f2_sub(pc.y, LY[r]));
+            const f2_t dz = f2_add(f2_sub(pb.x, HZ[r]), f2_sub(pd, LZ[r]));
+            const f2_t r2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_mul(dz, dz)));
+            float u, v;
+            f2_unpack(r2, u, v);
+            acc[r] = f2_fma(pb.y, f2_pack(rsqrt_ftz(u), rsqrt_ftz(v)), acc[r]);
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const f2_t y = f2_sub(acc[r], kc[r]);
+          const f2_t s2 = f2_add(ks[r], y);
+          kc[r] = f2_sub(f2_sub(s2, ks[r]), y);
+          ks[r] = s2;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  double mine = 0.0;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    if (!vi[r]) continue;
+    float s0, s1, c0, c1;
+    f2_unpack(ks[r], s0, s1);
+    f2_unpack(kc[r], c0, c1);
+    const double row = (((double)s0 - (double)c0) + ((double)s1 - (double)c1)) + ((double)ksd[r] - (double)kcd[r]);
+    mine += A.mass[base + it.i0 + tid + kB32 * r] * row;
+  }
+  return block_sum<double, kB32>(mine, sh);
+}
+
+// Persistent FP32-compensated pair kernel: items taken from a counter in list
+// order; the shape of an item is hshape[h] (code 0, 1, 2 = 1, 2, 4 rows per
+// thread), or fixed_code for every item when hshape is null.
+__global__ void __launch_bounds__(kB32, 4) epot32_kernel(HaloArgs A, const PairItem* __restrict__ items,
+                                                         const int8_t* __restrict__ hshape, int fixed_code,
+                                                         int32_t nitems, int32_t* __restrict__ counter,
+                                                         double* __restrict__ part) {
+  __shared__ Tile32 S;
+  __shared__ double sh[kB32 / 32];
   __shared__ int32_t s_item;
   const int tid = threadIdx.x;
   for (;;) {
@@ -380,110 +556,47 @@ __global__ void __launch_bounds__(kPB2) epot_pairs32_kernel(HaloArgs A, const in
     const int32_t w = s_item;
     __syncthreads();
     if (w >= nitems) break;
-    const int32_t h = item_h[w];
-    const int64_t base = A.off[h];
-    const int32_t n = (int32_t)(A.off[h + 1] - base);
-    const int32_t i0 = item_i[w];
-    const double* c = A.out + (size_t)kHaloFields * h;
-    const double cx = c[HP_PX], cy = c[HP_PY], cz = c[HP_PZ];
-    float hx[2], hy[2], hz[2], lx[2], ly[2], lz[2], ks[2] = {0.f, 0.f}, kc[2] = {0.f, 0.f};
-    bool vi[2];
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      const int32_t i = i0 + tid + r * kPB2;
-      vi[r] = i < n;
-      double rx = 0, ry = 0, rz = 0;
-      if (vi[r]) {
-        rx = wrap_chp(A.pos[3 * (base + i)] - cx, A.L, A.h, A.periodic);
-        ry = wrap_chp(A.pos[3 * (base + i) + 1] - cy, A.L, A.h, A.periodic);
-        rz = wrap_chp(A.pos[3 * (base + i) + 2] - cz, A.L, A.h, A.periodic);
-      }
-      hx[r] = (float)rx; hy[r] = (float)ry; hz[r] = (float)rz;
-      lx[r] = (float)(rx - (double)hx[r]); ly[r] = (float)(ry - (double)hy[r]); lz[r] = (float)(rz - (double)hz[r]);
+    const PairItem it = items[w];
+    const int code = hshape ? (int)hshape[it.h] : fixed_code;
+    double tot;
+    if (code == 2) tot = epot32_item<4>(S, sh, A, it, false);
+    else if (code == 1) tot = epot32_item<2>(S, sh, A, it, false);
+    else tot = epot32_item<1>(S, sh, A, it, false);
+    // a zero separation in the fast path shows as a non-finite sum: recompute
+    // the item with the per-pair test (block-uniform decision)
+    if (__syncthreads_or(tid == 0 && !isfinite(tot))) {
+      if (code == 2) tot = epot32_item<4>(S, sh, A, it, true);
+      else if (code == 1) tot = epot32_item<2>(S, sh, A, it, true);
+      else tot = epot32_item<1>(S, sh, A, it, true);
     }
-    for (int32_t j0 = i0; j0 < n; j0 += kPB) {
-#pragma unroll
-      for (int r = 0; r < 2; ++r) {
-        const int32_t t = tid + r * kPB2;
-        const int32_t j = j0 + t;
-        if (j < n) {
-          const double rx = wrap_chp(A.pos[3 * (base + j)] - cx, A.L, A.h, A.periodic);
-          const double ry = wrap_chp(A.pos[3 * (base + j) + 1] - cy, A.L, A.h, A.periodic);
-          const double rz = wrap_chp(A.pos[3 * (base + j) + 2] - cz, A.L, A.h, A.periodic);
-          const float fx = (float)rx, fy = (float)ry, fz = (float)rz;
-          s_h[t] = make_float4(fx, fy, fz, (float)A.mass[base + j]);
-          s_l[t] = make_float4((float)(rx - (double)fx), (float)(ry - (double)fy), (float)(rz - (double)fz), 0.f);
-        } else {
-          s_h[t] = make_float4(3.0e30f, 3.0e30f, 3.0e30f, 0.f);
-          s_l[t] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-      }
-      __syncthreads();
-      const int jend = min(kPB, n - j0);
-      if (j0 == i0) {
-        // diagonal tile: j > i for each row (row 0 is tile row tid, row 1 is tid + kPB2)
-        for (int jj = tid + 1; jj < jend; ++jj) {
-          const float4 hj = s_h[jj], lj = s_l[jj];
-          if (vi[0]) kahan_pair(hj, lj, hx[0], hy[0], hz[0], lx[0], ly[0], lz[0], ks[0], kc[0]);
-          if (vi[1] && jj > tid + kPB2) kahan_pair(hj, lj, hx[1], hy[1], hz[1], lx[1], ly[1], lz[1], ks[1], kc[1]);
-        }
-      } else if (vi[0]) {
-        // groups of four partners: the four terms of a row are added as a
-        // small tree (independent work), then the group enters the
-        // compensated sum once -- one dependent chain per four pairs
-        int jj = 0;
-        for (; jj + 4 <= jend; jj += 4) {
-          float g[2];
-#pragma unroll
-          for (int r = 0; r < 2; ++r) {
-            const float t0 = pair_term(s_h[jj], s_l[jj], hx[r], hy[r], hz[r], lx[r], ly[r], lz[r]);
-            const float t1 = pair_term(s_h[jj + 1], s_l[jj + 1], hx[r], hy[r], hz[r], lx[r], ly[r], lz[r]);
-            const float t2 = pair_term(s_h[jj + 2], s_l[jj + 2], hx[r], hy[r], hz[r], lx[r], ly[r], lz[r]);
-            const float t3 = pair_term(s_h[jj + 3], s_l[jj + 3], hx[r], hy[r], hz[r], lx[r], ly[r], lz[r]);
-            g[r] = (t0 + t1) + (t2 + t3);
-          }
-          kahan_add(g[0], ks[0], kc[0]);
-          kahan_add(g[1], ks[1], kc[1]);
-        }
-        for (; jj < jend; ++jj) {
-          const float4 hj = s_h[jj], lj = s_l[jj];
-          kahan_pair(hj, lj, hx[0], hy[0], hz[0], lx[0], ly[0], lz[0], ks[0], kc[0]);
-          kahan_pair(hj, lj, hx[1], hy[1], hz[1], lx[1], ly[1], lz[1], ks[1], kc[1]);
-        }
-      }
-      __syncthreads();
-    }
-    double mine = 0.0;
-#pragma unroll
-    for (int r = 0; r < 2; ++r)
-      if (vi[r]) mine += A.mass[base + i0 + tid + r * kPB2] * ((double)ks[r] - (double)kc[r]);
-    // block sum over kPB2 threads
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
-    if ((tid & 31) == 0) sh[tid >> 5] = mine;
-    __syncthreads();
-    if (tid == 0) {
-      double tot = 0.0;
-      for (int k = 0; k < kPB2 / 32; ++k) tot += sh[k];
-      part[w] = tot;
-    }
-    __syncthreads();
+    if (tid == 0) part[w] = tot;
   }
 }
 
-// per-halo reduction of item partials (items of a halo are contiguous in the
-// halo-ordered list hitem_off), then E_pot, totals and spin
-__global__ void epot_finalize_kernel(HaloArgs A, const int64_t* __restrict__ hitem_off,
-                                     const int32_t* __restrict__ order, const double* __restrict__ part64,
-                                     const double* __restrict__ part32, int64_t nhalo) {
+// Rows per item of shape code c.
+__host__ __device__ constexpr int rows32_of(int code) { return kB32 << code; }
+
+// Item partials of one work list, folded per halo in halo order: the items
+// of halo h are entries [hoff[h], hoff[h+1]) of the halo-ordered list, and
+// order[k] is where entry k ran in the schedule.
+struct ItemFold {
+  const int64_t* hoff;
+  const int32_t* order;
+  const double* part;  // null: this form was not computed
+};
+
+__device__ __forceinline__ double fold_items(const ItemFold& F, int64_t h) {
+  double s = 0.0;
+  if (!F.part) return s;
+  for (int64_t k = F.hoff[h]; k < F.hoff[h + 1]; ++k) s += F.part[F.order[k]];
+  return s;
+}
+
+// per-halo reduction of item partials, then E_pot, totals and spin
+__global__ void epot_finalize_kernel(HaloArgs A, ItemFold f64, ItemFold f32, int64_t nhalo) {
   int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (h >= nhalo) return;
-  double s64 = 0, s32 = 0;
-  for (int64_t k = hitem_off[h]; k < hitem_off[h + 1]; ++k) {
-    const int32_t w = order[k];
-    if (part64) s64 += part64[w];
-    if (part32) s32 += part32[w];
-  }
+  const double s64 = fold_items(f64, h), s32 = fold_items(f32, h);
   double* o = A.out + (size_t)kHaloFields * h;
   o[HP_EP64] = -A.G * s64;
   o[HP_EP32C] = -A.G * s32;
@@ -531,14 +644,88 @@ __global__ void epot_finalize_kernel(HaloArgs A, const int64_t* __restrict__ hit
 // ------------------------------------------------------------------ host side
 namespace ahop {
 
+// Halo-size buckets of the FP32-compensated pair kernel's tile shape:
+// n < 512, < 4096, < 32768, < 262144, >= 262144 members.
+constexpr int kBuckets = AHOP_HALO_BUCKETS;
+constexpr int kShapes = 3;                       // 1, 2 or 4 rows per thread (128, 256, 512 rows per item)
+constexpr int kDefaultShape = 1;
+constexpr double kTunePairs = 3.0e9;             // pairs timed per bucket and shape by the autotuner
+
+static int bucket_of(int64_t n) {
+  return n < 512 ? 0 : n < 4096 ? 1 : n < 32768 ? 2 : n < 262144 ? 3 : 4;
+}
+
+// One work list in halo order plus its schedule (items by decreasing cost).
+struct ItemList {
+  std::vector<PairItem> items;   // halo order
+  std::vector<int64_t> cost;
+  std::vector<int64_t> hoff;     // [nhalo+1]
+  std::vector<PairItem> sched;   // run order
+  std::vector<int32_t> order;    // halo-order entry k ran as sched[order[k]]
+  void clear() { items.clear(); cost.clear(); hoff.clear(); }
+};
+
+// Items of halo h (n members) with `rows` rows per item over rows [0, row_limit),
+// partners in chunks of kChunkJ.
+static void add_halo_items(ItemList& L, int32_t h, int64_t n, int rows, int64_t row_limit) {
+  const int64_t rl = std::min(n, row_limit);
+  for (int64_t i0 = 0; i0 < rl; i0 += rows) {
+    const int64_t r = std::min<int64_t>(rows, n - i0);
+    for (int64_t j0 = i0; j0 < n; j0 += kChunkJ) {
+      const int64_t j1 = std::min<int64_t>(n, j0 + kChunkJ);
+      L.items.push_back(PairItem{h, (int32_t)i0, (int32_t)j0, (int32_t)j1});
+      L.cost.push_back(j0 == i0 ? r * (j1 - j0) - r * r / 2 : r * (j1 - j0));
+    }
+  }
+}
+
+static void schedule(ItemList& L) {
+  const int32_t ni = (int32_t)L.items.size();
+  std::vector<int32_t> idx(ni);
+  for (int32_t k = 0; k < ni; ++k) idx[k] = k;
+  std::stable_sort(idx.begin(), idx.end(), [&](int32_t a, int32_t b) { return L.cost[a] > L.cost[b]; });
+  L.sched.resize(ni);
+  L.order.resize(ni);
+  for (int32_t k = 0; k < ni; ++k) {
+    L.sched[k] = L.items[idx[k]];
+    L.order[idx[k]] = k;
+  }
+}
+
+struct ListBufs {
+  DevBuf items, order, hoff, part;
+  int32_t n = 0;
+};
+
+struct GraphSig {
+  HaloArgs A;
+  const void* ptr[10];
+  int64_t nhalo;
+  int32_t n64, n32, grid64, grid32, epot, pad;
+};
+
 struct HaloEngine {
   DevBuf d_off, d_pos, d_vel, d_mass, d_dens, d_out;  // staging for host inputs
-  DevBuf d_item_h, d_item_i, d_part64, d_part32, d_counter, d_hoff, d_order, d_err;
+  ListBufs l64, l32, tune;
+  DevBuf d_hshape, d_counter, d_err;
   cudaEvent_t ev[5] = {};
+  cudaEvent_t ev_in = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
   bool ready = false;
-  cudaStream_t own = nullptr;
+  cudaStream_t own = nullptr;  // host-buffer entry point
+  cudaStream_t gs = nullptr;   // launches and graph replays
   AhopHaloTimings t{};
   std::vector<int64_t> h_off;
+  ItemList L64, L32;
+  // autotuner: tuned shape per bucket (-1 = not yet), pinned shapes, timings
+  int8_t code[kBuckets] = {-1, -1, -1, -1, -1};
+  int8_t pinned[kBuckets] = {-1, -1, -1, -1, -1};
+  float tune_ms[kBuckets][kShapes] = {};
+  double tune_pairs[kBuckets] = {};
+  // CUDA graph of the launch sequence, replayed while its arguments match
+  bool use_graph = true;
+  cudaGraphExec_t gexec = nullptr;
+  GraphSig gsig{};
+  int32_t graph_replays = 0;
 };
 
 static HaloEngine& halo_engine() {
@@ -546,103 +733,250 @@ static HaloEngine& halo_engine() {
   return *e;
 }
 
+template <class T>
+static int upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
+  AHOP_CUDA_TRY(b.ensure(std::max<size_t>(v.size() * sizeof(T), 16)));
+  if (!v.empty()) AHOP_CUDA_TRY(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  return AHOP_OK;
+}
+
+static int upload_list(ListBufs& B, const ItemList& L, cudaStream_t st) {
+  int rc;
+  if ((rc = upload(B.items, L.sched, st))) return rc;
+  if ((rc = upload(B.order, L.order, st))) return rc;
+  if ((rc = upload(B.hoff, L.hoff, st))) return rc;
+  AHOP_CUDA_TRY(B.part.ensure(std::max<size_t>(L.sched.size() * 8, 16)));
+  B.n = (int32_t)L.sched.size();
+  return AHOP_OK;
+}
+
+static int grid_for(const void* fn, int threads) {
+  int dev = 0, nsm = 148, per = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, 0);
+  return nsm * (per > 0 ? per : 1);
+}
+
+// Autotuner: for every bucket present in this call whose shape is neither
+// tuned nor pinned, time each shape on the same sample of that bucket's pairs
+// (its halos in order, rows cut at a multiple of 512 so every shape sees the
+// same pairs, about kTunePairs pairs in all) and keep the fastest.  Needs the
+// halo centres (moments) in A.out.
+static int tune_buckets(HaloEngine& H, const HaloArgs& A, const int64_t* h_off, int64_t nhalo, cudaStream_t st) {
+  bool need[kBuckets] = {};
+  bool any = false;
+  for (int64_t h = 0; h < nhalo; ++h) {
+    const int b = bucket_of(h_off[h + 1] - h_off[h]);
+    if (H.code[b] < 0 && H.pinned[b] < 0 && h_off[h + 1] - h_off[h] > 1) need[b] = any = true;
+  }
+  if (!any) return AHOP_OK;
+  if (!H.ev_t0) {
+    AHOP_CUDA_TRY(cudaEventCreate(&H.ev_t0));
+    AHOP_CUDA_TRY(cudaEventCreate(&H.ev_t1));
+  }
+  const int grid = grid_for((const void*)epot32_kernel, kB32);
+  for (int b = 0; b < kBuckets; ++b) {
+    if (!need[b]) continue;
+    std::vector<std::pair<int32_t, int64_t>> sample;  // (halo, row limit)
+    double acc = 0;
+    for (int64_t h = 0; h < nhalo && acc < kTunePairs; ++h) {
+      const int64_t n = h_off[h + 1] - h_off[h];
+      if (bucket_of(n) != b || n < 2) continue;
+      const double all = 0.5 * (double)n * (double)(n - 1);
+      int64_t rl = n;
+      if (acc + all > kTunePairs) {
+        rl = (int64_t)((kTunePairs - acc) / (double)n) + 1;
+        rl = ((rl + kMaxT32 - 1) / kMaxT32) * kMaxT32;
+        rl = std::min(rl, n);
+      }
+      sample.emplace_back((int32_t)h, rl);
+      acc += rl >= n ? all : (double)rl * (double)n - 0.5 * (double)rl * (double)rl;
+    }
+    H.tune_pairs[b] = acc;
+    float best = 0.f;
+    int best_c = kDefaultShape;
+    for (int c = 0; c < kShapes; ++c) {
+      ItemList L;
+      for (auto& s : sample) add_halo_items(L, s.first, h_off[s.first + 1] - h_off[s.first], rows32_of(c), s.second);
+      schedule(L);
+      int rc;
+      if ((rc = upload(H.tune.items, L.sched, st))) return rc;
+      AHOP_CUDA_TRY(H.tune.part.ensure(std::max<size_t>(L.sched.size() * 8, 16)));
+      float ms = 0.f;
+      for (int rep = 0; rep < 2; ++rep) {  // first run warms up, the second is timed
+        AHOP_CUDA_TRY(cudaMemsetAsync(H.d_counter.as<int32_t>() + 2, 0, 4, st));
+        AHOP_CUDA_TRY(cudaEventRecord(H.ev_t0, st));
+        epot32_kernel<<<grid, kB32, 0, st>>>(A, H.tune.items.as<PairItem>(), nullptr, c, (int32_t)L.sched.size(),
+                                             H.d_counter.as<int32_t>() + 2, H.tune.part.as<double>());
+        AHOP_CUDA_TRY(cudaGetLastError());
+        AHOP_CUDA_TRY(cudaEventRecord(H.ev_t1, st));
+      }
+      AHOP_CUDA_TRY(cudaEventSynchronize(H.ev_t1));
+      AHOP_CUDA_TRY(cudaEventElapsedTime(&ms, H.ev_t0, H.ev_t1));
+      H.tune_ms[b][c] = ms;
+      if (c == 0 || ms < best) { best = ms; best_c = c; }
+    }
+    H.code[b] = (int8_t)best_c;
+  }
+  return AHOP_OK;
+}
+
+// The device work of one call, in stream order; `capture` marks the timing
+// events as graph nodes.
+static int enqueue_props(HaloEngine& H, const HaloArgs& A, int64_t nhalo, int epot, int grid64, int grid32,
+                         cudaStream_t s, bool capture, int* launches) {
+  const unsigned flags = capture ? cudaEventRecordExternal : 0u;
+  AHOP_CUDA_TRY(cudaMemsetAsync(H.d_counter.p, 0, 8, s));
+  AHOP_CUDA_TRY(cudaMemsetAsync(H.d_err.p, 0, 4, s));
+  AHOP_CUDA_TRY(cudaEventRecordWithFlags(H.ev[0], s, flags));
+  *launches = 0;
+  if (nhalo > 0) {
+    halo_moments_kernel<<<(unsigned)nhalo, kPB, 0, s>>>(A);
+    ++*launches;
+    AHOP_CUDA_TRY(cudaGetLastError());
+  }
+  AHOP_CUDA_TRY(cudaEventRecordWithFlags(H.ev[1], s, flags));
+  if ((epot & 1) && H.l64.n > 0) {
+    epot64_kernel<<<grid64, kT64, 0, s>>>(A, H.l64.items.as<PairItem>(), H.l64.n, H.d_counter.as<int32_t>(),
+                                          H.l64.part.as<double>());
+    ++*launches;
+    AHOP_CUDA_TRY(cudaGetLastError());
+  }
+  AHOP_CUDA_TRY(cudaEventRecordWithFlags(H.ev[2], s, flags));
+  if ((epot & 2) && H.l32.n > 0) {
+    epot32_kernel<<<grid32, kB32, 0, s>>>(A, H.l32.items.as<PairItem>(), H.d_hshape.as<int8_t>(), kDefaultShape,
+                                          H.l32.n, H.d_counter.as<int32_t>() + 1, H.l32.part.as<double>());
+    ++*launches;
+    AHOP_CUDA_TRY(cudaGetLastError());
+  }
+  AHOP_CUDA_TRY(cudaEventRecordWithFlags(H.ev[3], s, flags));
+  if (nhalo > 0) {
+    const ItemFold f64{H.l64.hoff.as<int64_t>(), H.l64.order.as<int32_t>(),
+                       (epot & 1) ? H.l64.part.as<double>() : nullptr};
+    const ItemFold f32{H.l32.hoff.as<int64_t>(), H.l32.order.as<int32_t>(),
+                       (epot & 2) ? H.l32.part.as<double>() : nullptr};
+    epot_finalize_kernel<<<(unsigned)((nhalo + 127) / 128), 128, 0, s>>>(A, f64, f32, nhalo);
+    ++*launches;
+    AHOP_CUDA_TRY(cudaGetLastError());
+  }
+  AHOP_CUDA_TRY(cudaEventRecordWithFlags(H.ev[4], s, flags));
+  return AHOP_OK;
+}
+
 static int halo_run(HaloEngine& H, const AhopHaloParams* p, const int64_t* d_off, const int64_t* h_off,
                     int64_t nhalo, const double* d_pos, const double* d_vel, const double* d_mass,
                     const double* d_dens, double* d_out, cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  AHOP_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone) {
+    set_error("the stream is being captured; use ahop_halo_props_noalloc inside a stream capture");
+    return AHOP_EINVAL;
+  }
   if (!H.ready) {
     for (auto& e : H.ev) AHOP_CUDA_TRY(cudaEventCreate(&e));
+    AHOP_CUDA_TRY(cudaEventCreateWithFlags(&H.ev_in, cudaEventDisableTiming));
+    AHOP_CUDA_TRY(cudaStreamCreateWithFlags(&H.gs, cudaStreamNonBlocking));
     H.ready = true;
   }
-  // work list: (halo, i-tile) items sorted by decreasing pair cost
-  std::vector<int64_t> cost;
-  std::vector<int32_t> ih, ii;
-  std::vector<int64_t> hoff(nhalo + 1, 0);
   double pairs = 0;
   for (int64_t h = 0; h < nhalo; ++h) {
     const int64_t n = h_off[h + 1] - h_off[h];
-    if (n < 0 || n > INT32_MAX) { set_error("halo member count out of range"); return AHOP_EINVAL; }
+    if (n < 0 || n > INT32_MAX - kChunkJ) { set_error("halo member count out of range"); return AHOP_EINVAL; }
     pairs += 0.5 * (double)n * (double)(n - 1);
-    hoff[h] = (int64_t)ih.size();
-    for (int64_t i0 = 0; i0 < n; i0 += kPB) {
-      ih.push_back((int32_t)h);
-      ii.push_back((int32_t)i0);
-      cost.push_back((n - i0) * (int64_t)kPB);
-    }
   }
-  hoff[nhalo] = (int64_t)ih.size();
-  const int32_t nitems = (int32_t)ih.size();
-  std::vector<int32_t> sorted(nitems);
-  for (int32_t k = 0; k < nitems; ++k) sorted[k] = k;
-  std::stable_sort(sorted.begin(), sorted.end(), [&](int32_t a, int32_t b) { return cost[a] > cost[b]; });
-  std::vector<int32_t> sh(nitems), si(nitems), order(nitems);
-  for (int32_t k = 0; k < nitems; ++k) {
-    sh[k] = ih[sorted[k]];
-    si[k] = ii[sorted[k]];
-    order[sorted[k]] = k;  // halo-ordered item k runs as scheduled item order[k]
-  }
-  const size_t ni = (size_t)(nitems > 0 ? nitems : 1);
-  AHOP_CUDA_TRY(H.d_item_h.ensure(ni * 4));
-  AHOP_CUDA_TRY(H.d_item_i.ensure(ni * 4));
-  AHOP_CUDA_TRY(H.d_order.ensure(ni * 4));
-  AHOP_CUDA_TRY(H.d_part64.ensure(ni * 8));
-  AHOP_CUDA_TRY(H.d_part32.ensure(ni * 8));
-  AHOP_CUDA_TRY(H.d_counter.ensure(16));
-  AHOP_CUDA_TRY(H.d_hoff.ensure((size_t)(nhalo + 1) * 8));
-  AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_item_h.p, sh.data(), nitems * 4, cudaMemcpyHostToDevice, st));
-  AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_item_i.p, si.data(), nitems * 4, cudaMemcpyHostToDevice, st));
-  AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_order.p, order.data(), nitems * 4, cudaMemcpyHostToDevice, st));
-  AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_hoff.p, hoff.data(), (nhalo + 1) * 8, cudaMemcpyHostToDevice, st));
   HaloArgs A;
+  memset(&A, 0, sizeof A);  // compared bytewise for graph reuse
   A.off = d_off; A.pos = d_pos; A.vel = d_vel; A.mass = d_mass; A.dens = d_dens; A.out = d_out;
   A.L = p->Lbox; A.h = 0.5 * p->Lbox; A.hub = p->Hub_pt; A.G = p->gravconst; A.periodic = p->periodic != 0;
   A.sc = p->sc != 0; A.dcell_min = p->dcell_min; A.eps_sc = p->eps_sc;
   AHOP_CUDA_TRY(H.d_err.ensure(16));
-  AHOP_CUDA_TRY(cudaMemsetAsync(H.d_err.p, 0, 4, st));
+  AHOP_CUDA_TRY(H.d_counter.ensure(16));
   A.err = H.d_err.as<int>();
-  int dev = 0, nsm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int epot = p->epot & 3;
+  int rc;
+  float tune_total = 0.f;
+  if (epot & 2) {
+    // shapes for this call's buckets; the tuner needs the centres first
+    bool need = false;
+    for (int64_t h = 0; h < nhalo && !need; ++h) {
+      const int b = bucket_of(h_off[h + 1] - h_off[h]);
+      need = H.code[b] < 0 && H.pinned[b] < 0 && h_off[h + 1] - h_off[h] > 1;
+    }
+    if (need) {
+      auto t0 = std::chrono::steady_clock::now();
+      AHOP_CUDA_TRY(cudaMemsetAsync(H.d_err.p, 0, 4, st));
+      halo_moments_kernel<<<(unsigned)nhalo, kPB, 0, st>>>(A);
+      AHOP_CUDA_TRY(cudaGetLastError());
+      if ((rc = tune_buckets(H, A, h_off, nhalo, st))) return rc;
+      tune_total = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+  }
+  // work lists (halo order), schedules, per-halo shape codes
+  std::vector<int8_t> hshape;
+  H.L64.clear();
+  H.L32.clear();
+  H.L64.hoff.assign(nhalo + 1, 0);
+  H.L32.hoff.assign(nhalo + 1, 0);
+  if (epot & 2) hshape.resize(nhalo > 0 ? nhalo : 1, (int8_t)kDefaultShape);
+  for (int64_t h = 0; h < nhalo; ++h) {
+    const int64_t n = h_off[h + 1] - h_off[h];
+    H.L64.hoff[h] = (int64_t)H.L64.items.size();
+    H.L32.hoff[h] = (int64_t)H.L32.items.size();
+    if (epot & 1) add_halo_items(H.L64, (int32_t)h, n, kT64, n);
+    if (epot & 2) {
+      const int b = bucket_of(n);
+      const int c = H.pinned[b] >= 0 ? H.pinned[b] : H.code[b] >= 0 ? H.code[b] : kDefaultShape;
+      hshape[h] = (int8_t)c;
+      add_halo_items(H.L32, (int32_t)h, n, rows32_of(c), n);
+    }
+  }
+  H.L64.hoff[nhalo] = (int64_t)H.L64.items.size();
+  H.L32.hoff[nhalo] = (int64_t)H.L32.items.size();
+  schedule(H.L64);
+  schedule(H.L32);
+  if ((rc = upload_list(H.l64, H.L64, st))) return rc;
+  if ((rc = upload_list(H.l32, H.L32, st))) return rc;
+  if ((rc = upload(H.d_hshape, hshape, st))) return rc;
+  const int grid64 = grid_for((const void*)epot64_kernel, kT64);
+  const int grid32 = grid_for((const void*)epot32_kernel, kB32);
+  // the launches run on the engine's stream after everything queued on st
+  AHOP_CUDA_TRY(cudaEventRecord(H.ev_in, st));
+  AHOP_CUDA_TRY(cudaStreamWaitEvent(H.gs, H.ev_in, 0));
   int launches = 0;
-  AHOP_CUDA_TRY(cudaEventRecord(H.ev[0], st));
-  if (nhalo > 0) {
-    halo_moments_kernel<<<(unsigned)nhalo, kPB, 0, st>>>(A);
-    ++launches;
-    AHOP_CUDA_TRY(cudaGetLastError());
+  if (H.use_graph) {
+    GraphSig sig;
+    memset(&sig, 0, sizeof sig);
+    sig.A = A;
+    const void* ptrs[10] = {H.l64.items.p, H.l64.order.p, H.l64.hoff.p, H.l64.part.p, H.l32.items.p,
+                            H.l32.order.p, H.l32.hoff.p, H.l32.part.p, H.d_hshape.p, H.d_counter.p};
+    memcpy(sig.ptr, ptrs, sizeof ptrs);
+    sig.nhalo = nhalo; sig.n64 = H.l64.n; sig.n32 = H.l32.n; sig.grid64 = grid64; sig.grid32 = grid32;
+    sig.epot = epot;
+    if (!H.gexec || memcmp(&sig, &H.gsig, sizeof sig) != 0) {
+      if (H.gexec) { cudaGraphExecDestroy(H.gexec); H.gexec = nullptr; }
+      cudaGraph_t g = nullptr;
+      AHOP_CUDA_TRY(cudaStreamBeginCapture(H.gs, cudaStreamCaptureModeThreadLocal));
+      rc = enqueue_props(H, A, nhalo, epot, grid64, grid32, H.gs, true, &launches);
+      const cudaError_t ec = cudaStreamEndCapture(H.gs, &g);
+      if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+      AHOP_CUDA_TRY(ec);
+      const cudaError_t ei = cudaGraphInstantiate(&H.gexec, g, 0);
+      cudaGraphDestroy(g);
+      AHOP_CUDA_TRY(ei);
+      H.gsig = sig;
+      H.graph_replays = 0;
+    } else {
+      ++H.graph_replays;
+      launches = H.t.kernel_launches;
+    }
+    AHOP_CUDA_TRY(cudaGraphLaunch(H.gexec, H.gs));
+  } else {
+    if ((rc = enqueue_props(H, A, nhalo, epot, grid64, grid32, H.gs, false, &launches))) return rc;
   }
-  AHOP_CUDA_TRY(cudaEventRecord(H.ev[1], st));
-  if ((p->epot & 1) && nitems > 0) {
-    int per = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, epot_pairs_kernel<false>, kPB, 0);
-    AHOP_CUDA_TRY(cudaMemsetAsync(H.d_counter.p, 0, 4, st));
-    epot_pairs_kernel<false><<<nsm * (per > 0 ? per : 1), kPB, 0, st>>>(
-        A, H.d_item_h.as<int32_t>(), H.d_item_i.as<int32_t>(), nitems, H.d_counter.as<int32_t>(),
-        H.d_part64.as<double>());
-    ++launches;
-    AHOP_CUDA_TRY(cudaGetLastError());
-  }
-  AHOP_CUDA_TRY(cudaEventRecord(H.ev[2], st));
-  if ((p->epot & 2) && nitems > 0) {
-    int per = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, epot_pairs32_kernel, kPB2, 0);
-    AHOP_CUDA_TRY(cudaMemsetAsync(H.d_counter.as<int32_t>() + 1, 0, 4, st));
-    epot_pairs32_kernel<<<nsm * (per > 0 ? per : 1), kPB2, 0, st>>>(
-        A, H.d_item_h.as<int32_t>(), H.d_item_i.as<int32_t>(), nitems, H.d_counter.as<int32_t>() + 1,
-        H.d_part32.as<double>());
-    ++launches;
-    AHOP_CUDA_TRY(cudaGetLastError());
-  }
-  AHOP_CUDA_TRY(cudaEventRecord(H.ev[3], st));
-  if (nhalo > 0) {
-    epot_finalize_kernel<<<(unsigned)((nhalo + 127) / 128), 128, 0, st>>>(
-        A, H.d_hoff.as<int64_t>(), H.d_order.as<int32_t>(), (p->epot & 1) ? H.d_part64.as<double>() : nullptr,
-        (p->epot & 2) ? H.d_part32.as<double>() : nullptr, nhalo);
-    ++launches;
-    AHOP_CUDA_TRY(cudaGetLastError());
-  }
-  AHOP_CUDA_TRY(cudaEventRecord(H.ev[4], st));
   int herr = 0;
-  AHOP_CUDA_TRY(cudaMemcpyAsync(&herr, H.d_err.p, 4, cudaMemcpyDeviceToHost, st));
-  AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(&herr, H.d_err.p, 4, cudaMemcpyDeviceToHost, H.gs));
+  AHOP_CUDA_TRY(cudaStreamSynchronize(H.gs));
   if (herr) { set_error("shrinking-sphere centre: step limit reached"); return AHOP_ELIMIT; }
   auto el = [&](int a, int b) { float ms = 0; cudaEventElapsedTime(&ms, H.ev[a], H.ev[b]); return ms; };
   H.t.moments = el(0, 1);
@@ -651,8 +985,10 @@ static int halo_run(HaloEngine& H, const AhopHaloParams* p, const int64_t* d_off
   H.t.finalize = el(3, 4);
   H.t.total = el(0, 4);
   H.t.pairs = pairs;
-  H.t.items = nitems;
+  H.t.items = H.l64.n + H.l32.n;
   H.t.kernel_launches = launches;
+  H.t.tune_ms = tune_total;
+  H.t.graph_replays = H.use_graph ? H.graph_replays : -1;
   return AHOP_OK;
 }
 
@@ -721,6 +1057,49 @@ int ahop_halo_get_timings(AhopHaloTimings* t) {
   return AHOP_OK;
 }
 
+int ahop_halo_get_tiles(int32_t* rows, float* ms) {
+  if (!rows) { set_error("null rows"); return AHOP_EINVAL; }
+  HaloEngine& H = halo_engine();
+  for (int b = 0; b < kBuckets; ++b) {
+    const int c = H.pinned[b] >= 0 ? H.pinned[b] : H.code[b];
+    rows[b] = c >= 0 ? rows32_of(c) : 0;
+    if (ms)
+      for (int k = 0; k < kShapes; ++k) ms[b * kShapes + k] = H.tune_ms[b][k];
+  }
+  return AHOP_OK;
+}
+
+int ahop_halo_set_tiles(const int32_t* rows) {
+  HaloEngine& H = halo_engine();
+  if (!rows) {
+    for (int b = 0; b < kBuckets; ++b) {
+      H.pinned[b] = H.code[b] = -1;
+      for (int k = 0; k < kShapes; ++k) H.tune_ms[b][k] = 0.f;
+    }
+    return AHOP_OK;
+  }
+  int8_t c[kBuckets];
+  for (int b = 0; b < kBuckets; ++b) {
+    if (rows[b] == 0) c[b] = -1;
+    else if (rows[b] == rows32_of(0)) c[b] = 0;
+    else if (rows[b] == rows32_of(1)) c[b] = 1;
+    else if (rows[b] == rows32_of(2)) c[b] = 2;
+    else { set_error("tile rows must be 0, 128, 256 or 512"); return AHOP_EINVAL; }
+  }
+  for (int b = 0; b < kBuckets; ++b) H.pinned[b] = c[b];
+  return AHOP_OK;
+}
+
+int ahop_halo_set_graph(int32_t on) {
+  HaloEngine& H = halo_engine();
+  H.use_graph = on != 0;
+  if (!H.use_graph && H.gexec) {
+    cudaGraphExecDestroy(H.gexec);
+    H.gexec = nullptr;
+  }
+  return AHOP_OK;
+}
+
 }  // extern "C"
 
 // --------------------------------------------------- allocation-free variant
@@ -737,8 +1116,7 @@ constexpr int64_t kNoAllocMaxHalos = 65536;         // halos per call
 constexpr int64_t kNoAllocMaxItems = 262144;        // (halo, 256-member tile) items per call
 
 struct NoAllocScratch {
-  int32_t item_h[kNoAllocMaxItems];
-  int32_t item_i[kNoAllocMaxItems];
+  PairItem items[kNoAllocMaxItems];
   int32_t order[kNoAllocMaxItems];
   double part64[kNoAllocMaxItems];
   double part32[kNoAllocMaxItems];
@@ -746,7 +1124,7 @@ struct NoAllocScratch {
   int32_t counter[4];  // [0],[1]: work counters of the two pair kernels; [2]: item total; [3]: error
 };
 
-// ~7.9 MB; in host code this name is only a host-side stand-in, the device
+// ~10 MB; in host code this name is only a host-side stand-in, the device
 // address comes from cudaGetSymbolAddress below.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
 
@@ -761,7 +1139,7 @@ __global__ void __launch_bounds__(1024) noalloc_offsets_kernel(const int64_t* __
     int64_t nit = 0;
     if (h < nhalo) {
       const int64_t n = off[h + 1] - off[h];
-      nit = n > 0 ? (n + kPB - 1) / kPB : 0;
+      nit = n > 0 ? (n + kT64 - 1) / kT64 : 0;
     }
     int64_t ex, tot;
     Scan(tmp).ExclusiveSum(nit, ex, tot);
@@ -775,17 +1153,19 @@ __global__ void __launch_bounds__(1024) noalloc_offsets_kernel(const int64_t* __
   }
 }
 
-// Work items in halo order (no cost sort: per-item partials and the per-halo
-// fold order do not depend on the schedule, so results match the allocating
-// entry point bit for bit).
+// Work items in halo order, one per 256 rows of a halo with all of its
+// partners (no cost sort, no partner chunks).  The FP64 form and the FP32
+// form (at 2 rows per thread, also 256 rows per item) share the list.  The
+// FP64 rows equal the allocating entry point's to rounding; the
+// FP32-compensated ones are summed in other groups (that entry point chunks
+// partners and picks tile shapes per halo size) and agree to its error.
 __global__ void noalloc_items_kernel(const int64_t* __restrict__ off, int64_t nhalo, NoAllocScratch* S) {
   const int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (h >= nhalo) return;
   const int64_t n = off[h + 1] - off[h];
   int64_t k = S->hoff[h];
-  for (int64_t i0 = 0; i0 < n; i0 += kPB, ++k) {
-    S->item_h[k] = (int32_t)h;
-    S->item_i[k] = (int32_t)i0;
+  for (int64_t i0 = 0; i0 < n; i0 += kT64, ++k) {
+    S->items[k] = PairItem{(int32_t)h, (int32_t)i0, (int32_t)i0, (int32_t)n};
     S->order[k] = (int32_t)k;
   }
 }
@@ -845,31 +1225,27 @@ extern "C" int ahop_halo_props_noalloc(const AhopHaloParams* p, const int64_t* d
   AHOP_CUDA_TRY(cudaMemsetAsync(S->counter, 0, 2 * sizeof(int32_t), st));
   AHOP_CUDA_TRY(cudaMemsetAsync(&S->counter[3], 0, sizeof(int32_t), st));
   HaloArgs A;
+  memset(&A, 0, sizeof A);
   A.off = d_off; A.pos = d_pos; A.vel = d_vel; A.mass = d_mass; A.dens = d_density; A.out = d_out;
   A.L = p->Lbox; A.h = 0.5 * p->Lbox; A.hub = p->Hub_pt; A.G = p->gravconst; A.periodic = p->periodic != 0;
   A.sc = p->sc != 0; A.dcell_min = p->dcell_min; A.eps_sc = p->eps_sc;
   A.err = &S->counter[3];
-  int dev = 0, nsm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   halo_moments_kernel<<<(unsigned)nhalo, kPB, 0, st>>>(A);
   AHOP_CUDA_TRY(cudaGetLastError());
   if ((p->epot & 1) && total > 0) {
-    int per = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, epot_pairs_kernel<false>, kPB, 0);
-    epot_pairs_kernel<false><<<nsm * (per > 0 ? per : 1), kPB, 0, st>>>(A, S->item_h, S->item_i, total,
-                                                                        &S->counter[0], S->part64);
+    epot64_kernel<<<grid_for((const void*)epot64_kernel, kT64), kT64, 0, st>>>(A, S->items, total, &S->counter[0],
+                                                                               S->part64);
     AHOP_CUDA_TRY(cudaGetLastError());
   }
   if ((p->epot & 2) && total > 0) {
-    int per = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, epot_pairs32_kernel, kPB2, 0);
-    epot_pairs32_kernel<<<nsm * (per > 0 ? per : 1), kPB2, 0, st>>>(A, S->item_h, S->item_i, total,
-                                                                       &S->counter[1], S->part32);
+    static_assert(rows32_of(1) == kT64, "the FP32 form shares the 256-row list");
+    epot32_kernel<<<grid_for((const void*)epot32_kernel, kB32), kB32, 0, st>>>(A, S->items, nullptr, 1, total,
+                                                                               &S->counter[1], S->part32);
     AHOP_CUDA_TRY(cudaGetLastError());
   }
-  epot_finalize_kernel<<<(unsigned)((nhalo + 127) / 128), 128, 0, st>>>(
-      A, S->hoff, S->order, (p->epot & 1) ? S->part64 : nullptr, (p->epot & 2) ? S->part32 : nullptr, nhalo);
+  const ItemFold f64{S->hoff, S->order, (p->epot & 1) ? S->part64 : nullptr};
+  const ItemFold f32{S->hoff, S->order, (p->epot & 2) ? S->part32 : nullptr};
+  epot_finalize_kernel<<<(unsigned)((nhalo + 127) / 128), 128, 0, st>>>(A, f64, f32, nhalo);
   AHOP_CUDA_TRY(cudaGetLastError());
   int32_t herr = 0;
   AHOP_CUDA_TRY(cudaMemcpyAsync(&herr, &S->counter[3], 4, cudaMemcpyDeviceToHost, st));

@@ -214,6 +214,8 @@ typedef struct {
   float moments, epot64, epot32c, finalize, total; /* ms, CUDA events */
   double pairs;                                    /* sum over halos of n(n-1)/2 */
   int32_t items, kernel_launches;
+  float tune_ms;          /* host wall time of the tile autotuner in this call (0 when it did not run) */
+  int32_t graph_replays;  /* replays of the captured launch graph since its capture (-1: graphs off) */
 } AhopHaloTimings;
 
 /* Host buffers: off[nhalo+1], pos[n][3], vel[n][3], mass[n], density[n];
@@ -225,12 +227,31 @@ int ahop_halo_props_device(const AhopHaloParams* p, const int64_t* d_off, int64_
                            const double* d_vel, const double* d_mass, const double* d_density, double* d_out,
                            void* stream);
 int ahop_halo_get_timings(AhopHaloTimings* t);
+/* Tile shapes of the FP32-compensated pair kernel, one per halo-size bucket
+ * (members n < 512, < 4096, < 32768, < 262144, >= 262144): 128, 256 or 512
+ * rows per work item (1, 2 or 4 rows per thread).  Unless pinned, a bucket's
+ * shape is picked by timing the three shapes on the first call that holds
+ * halos of that bucket (about 3e9 pairs of that call's own halos per shape),
+ * and kept for the process.  The shape changes the FP32 summation groups, so
+ * ep32c may differ between shapes by its rounding error (well below 1e-6
+ * relative); pin the shapes for bit-reproducible FP32 results across
+ * processes.  get: rows[AHOP_HALO_BUCKETS] in use (0 = not tuned yet),
+ * ms[AHOP_HALO_BUCKETS * 3] the autotuner's times per shape (may be null).
+ * set: rows[b] in {128, 256, 512} pins bucket b, 0 lets the autotuner pick;
+ * rows == NULL forgets every pin and every tuned shape. */
+#define AHOP_HALO_BUCKETS 5
+int ahop_halo_get_tiles(int32_t* rows, float* ms);
+int ahop_halo_set_tiles(const int32_t* rows);
+/* The launch sequence of ahop_halo_props(_device) is captured once as a CUDA
+ * graph and replayed while the call's device pointers, halo count and work
+ * list sizes stay the same (on = 1, the default); on = 0 launches directly. */
+int ahop_halo_set_graph(int32_t on);
 /* Allocation-free variant of ahop_halo_props_device (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc -- code running while
  * another part of the process captures a CUDA graph, frameworks that own all
  * device memory through their own pool, callers with a fixed memory budget.
  * It allocates nothing: its scratch is a file-scope device array of about
- * 7.9 MB (held on every GPU that loads the library until exit), limiting one
+ * 10 MB (held on every GPU that loads the library until exit), limiting one
  * call to 65,536 halos and 262,144 work items (one item per 256 members of a
  * halo); larger calls are rejected with AHOP_EINVAL.  The caller passes device
  * inputs and the device output [nhalo][AHOP_HALO_NFIELDS].  Every call shares

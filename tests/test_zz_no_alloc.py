@@ -6,8 +6,10 @@ framework that owns all device memory through its own pool.  For them the
 library offers one entry point whose scratch lives in a fixed-size device
 array compiled into the library.  This test calls it through the C ABI twice
 in a row and checks it against the allocating entry point
-(ahop_halo_props_device) with the tolerance of the other halo-property tests,
-and checks that sizes beyond its stated limits are rejected.  It sits in its
+(ahop_halo_props_device) with the tolerance of the other halo-property tests
+(the FP32-compensated fields, summed in other groups by the two entry points,
+to the 1e-6 of that form), and checks that sizes beyond its stated limits are
+rejected.  It sits in its
 own file that pytest collects last and passes alone or after the other tests.
 """
 import numpy as np
@@ -18,6 +20,8 @@ from conftest import gpu_available
 pytestmark = pytest.mark.gpu
 
 FIELDS_RTOL = 1e-12
+FP32C_RTOL = 1e-6
+FP32C_FIELDS = ("ep32c", "spin32c")
 
 
 @pytest.fixture(scope="module")
@@ -47,7 +51,8 @@ def test_noalloc_matches_allocating_entry_point_twice(catalogue):
         torch.cuda.synchronize()
         o = out.cpu().numpy()
         for k, name in enumerate(halo_props.FIELDS):
-            np.testing.assert_allclose(o[:, k], r[:, k], rtol=FIELDS_RTOL, atol=0, err_msg=f"call {call}: {name}")
+            rtol = FP32C_RTOL if name in FP32C_FIELDS else FIELDS_RTOL
+            np.testing.assert_allclose(o[:, k], r[:, k], rtol=rtol, atol=0, err_msg=f"call {call}: {name}")
 
 
 def test_noalloc_rejects_sizes_beyond_its_limit(catalogue):
