@@ -327,9 +327,9 @@ __global__ void __launch_bounds__(kT64) epot64_kernel(HaloArgs A, const PairItem
 // lo = float(r - hi); a separation is (hi_j - hi_i) + (lo_j - lo_i).  The two
 // lanes of every packed register hold two partners j, 2q and 2q+1, of the same
 // row i, so a row's own coordinates are loop-invariant (hi_i, hi_i) pairs.
-// Each thread owns kR32 rows (rows tid + 128 r); partner tiles are 128 * R
-// wide, shared memory holds them as packed pairs.  For every row, eight
-// partner pairs (16 terms) are accumulated by a fused multiply-add chain per
+// Each thread owns R rows (rows tid + 128 r); partner tiles are 128 * R
+// wide, shared memory holds them as packed pairs.  For every row, sixteen
+// partner pairs (32 terms) are accumulated by a fused multiply-add chain per
 // lane, then enter a Kahan-compensated FP32 sum; rows fold into FP64 per item.
 // Separations of exactly zero (coincident members) are excluded like in the
 // FP64 form: the fast path does not test for them -- rsqrt(0) = inf makes the
@@ -375,7 +375,7 @@ __device__ __forceinline__ float rsqrt_ftz(float x) {
 constexpr int kB32 = 128;              // threads per block of the FP32 form
 constexpr int kMaxR32 = 4;             // rows per thread, largest shape
 constexpr int kMaxT32 = kB32 * kMaxR32;
-constexpr int kGroup32 = 8;            // partner pairs per compensated fold
+constexpr int kGroup32 = 16;           // partner pairs per compensated fold
 constexpr int kChunkJ = 32768;         // partners per item at most (a multiple of every tile width)
 constexpr float kFar = 1.0e18f;        // padding position: its terms vanish (mass 0, finite r)
 
@@ -649,7 +649,8 @@ namespace ahop {
 constexpr int kBuckets = AHOP_HALO_BUCKETS;
 constexpr int kShapes = 3;                       // 1, 2 or 4 rows per thread (128, 256, 512 rows per item)
 constexpr int kDefaultShape = 1;
-constexpr double kTunePairs = 3.0e9;             // pairs timed per bucket and shape by the autotuner
+constexpr double kTunePairs = 3.0e9;             // pairs timed per bucket and shape by the autotuner, at least
+constexpr int kTuneWaves = 4;                    // ... and at least this many items per resident block, largest shape
 
 static int bucket_of(int64_t n) {
   return n < 512 ? 0 : n < 4096 ? 1 : n < 32768 ? 2 : n < 262144 ? 3 : 4;
@@ -760,9 +761,12 @@ static int grid_for(const void* fn, int threads) {
 
 // Autotuner: for every bucket present in this call whose shape is neither
 // tuned nor pinned, time each shape on the same sample of that bucket's pairs
-// (its halos in order, rows cut at a multiple of 512 so every shape sees the
-// same pairs, about kTunePairs pairs in all) and keep the fastest.  Needs the
-// halo centres (moments) in A.out.
+// and keep the fastest.  The sample takes the bucket's halos in order, in
+// slabs of 512 rows (a multiple of every shape's rows, so every shape sees the
+// same pairs), until it holds kTunePairs pairs and enough items of the
+// largest shape to keep every resident block busy for kTuneWaves items (or
+// the whole bucket): a sample that leaves blocks idle would favour the small
+// shapes.  Needs the halo centres (moments) in A.out.
 static int tune_buckets(HaloEngine& H, const HaloArgs& A, const int64_t* h_off, int64_t nhalo, cudaStream_t st) {
   bool need[kBuckets] = {};
   bool any = false;
@@ -780,18 +784,20 @@ static int tune_buckets(HaloEngine& H, const HaloArgs& A, const int64_t* h_off, 
     if (!need[b]) continue;
     std::vector<std::pair<int32_t, int64_t>> sample;  // (halo, row limit)
     double acc = 0;
-    for (int64_t h = 0; h < nhalo && acc < kTunePairs; ++h) {
+    int64_t items_big = 0;
+    const int64_t want_items = (int64_t)kTuneWaves * grid;
+    auto enough = [&] { return acc >= kTunePairs && items_big >= want_items; };
+    for (int64_t h = 0; h < nhalo && !enough(); ++h) {
       const int64_t n = h_off[h + 1] - h_off[h];
       if (bucket_of(n) != b || n < 2) continue;
-      const double all = 0.5 * (double)n * (double)(n - 1);
-      int64_t rl = n;
-      if (acc + all > kTunePairs) {
-        rl = (int64_t)((kTunePairs - acc) / (double)n) + 1;
-        rl = ((rl + kMaxT32 - 1) / kMaxT32) * kMaxT32;
-        rl = std::min(rl, n);
+      int64_t rl = 0;
+      while (rl < n && !enough()) {  // one slab of kMaxT32 rows = one item row of the largest shape
+        const int64_t r = std::min<int64_t>(kMaxT32, n - rl);
+        acc += (double)r * (double)(n - rl) - 0.5 * (double)r * (double)(r + 1);
+        items_big += (n - rl + kChunkJ - 1) / kChunkJ;
+        rl += r;
       }
       sample.emplace_back((int32_t)h, rl);
-      acc += rl >= n ? all : (double)rl * (double)n - 0.5 * (double)rl * (double)rl;
     }
     H.tune_pairs[b] = acc;
     float best = 0.f;
@@ -804,7 +810,7 @@ static int tune_buckets(HaloEngine& H, const HaloArgs& A, const int64_t* h_off, 
       if ((rc = upload(H.tune.items, L.sched, st))) return rc;
       AHOP_CUDA_TRY(H.tune.part.ensure(std::max<size_t>(L.sched.size() * 8, 16)));
       float ms = 0.f;
-      for (int rep = 0; rep < 2; ++rep) {  // first run warms up, the second is timed
+      for (int rep = (c == 0 ? 0 : 1); rep < 2; ++rep) {  // the bucket's first run warms up
         AHOP_CUDA_TRY(cudaMemsetAsync(H.d_counter.as<int32_t>() + 2, 0, 4, st));
         AHOP_CUDA_TRY(cudaEventRecord(H.ev_t0, st));
         epot32_kernel<<<grid, kB32, 0, st>>>(A, H.tune.items.as<PairItem>(), nullptr, c, (int32_t)L.sched.size(),
