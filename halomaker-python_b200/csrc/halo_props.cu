@@ -585,18 +585,32 @@ struct ItemFold {
   const double* part;  // null: this form was not computed
 };
 
-__device__ __forceinline__ double fold_items(const ItemFold& F, int64_t h) {
+// One warp per halo: lane l sums entries l, l + 32, ... in order, then a
+// butterfly over the lanes (every lane ends with the same bits), so the fold
+// is deterministic and a halo with many items does not serialise on one thread.
+__device__ __forceinline__ double fold_items(const ItemFold& F, int64_t h, int lane) {
   double s = 0.0;
   if (!F.part) return s;
-  for (int64_t k = F.hoff[h]; k < F.hoff[h + 1]; ++k) s += F.part[F.order[k]];
+  for (int64_t k = F.hoff[h] + lane; k < F.hoff[h + 1]; k += 32) s += F.part[F.order[k]];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   return s;
 }
 
+constexpr int kFinBlock = 128;  // four halos per block
+
+static inline unsigned finalize_blocks(int64_t nhalo) {
+  return (unsigned)((nhalo * 32 + kFinBlock - 1) / kFinBlock);
+}
+
 // per-halo reduction of item partials, then E_pot, totals and spin
-__global__ void epot_finalize_kernel(HaloArgs A, ItemFold f64, ItemFold f32, int64_t nhalo) {
-  int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kFinBlock) epot_finalize_kernel(HaloArgs A, ItemFold f64, ItemFold f32,
+                                                                  int64_t nhalo) {
+  const int64_t h = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;  // uniform per warp
+  const int lane = threadIdx.x & 31;
   if (h >= nhalo) return;
-  const double s64 = fold_items(f64, h), s32 = fold_items(f32, h);
+  const double s64 = fold_items(f64, h, lane), s32 = fold_items(f32, h, lane);
+  if (lane != 0) return;
   double* o = A.out + (size_t)kHaloFields * h;
   o[HP_EP64] = -A.G * s64;
   o[HP_EP32C] = -A.G * s32;
@@ -862,7 +876,7 @@ static int enqueue_props(HaloEngine& H, const HaloArgs& A, int64_t nhalo, int ep
                        (epot & 1) ? H.l64.part.as<double>() : nullptr};
     const ItemFold f32{H.l32.hoff.as<int64_t>(), H.l32.order.as<int32_t>(),
                        (epot & 2) ? H.l32.part.as<double>() : nullptr};
-    epot_finalize_kernel<<<(unsigned)((nhalo + 127) / 128), 128, 0, s>>>(A, f64, f32, nhalo);
+    epot_finalize_kernel<<<finalize_blocks(nhalo), kFinBlock, 0, s>>>(A, f64, f32, nhalo);
     ++*launches;
     AHOP_CUDA_TRY(cudaGetLastError());
   }
@@ -1251,7 +1265,7 @@ extern "C" int ahop_halo_props_noalloc(const AhopHaloParams* p, const int64_t* d
   }
   const ItemFold f64{S->hoff, S->order, (p->epot & 1) ? S->part64 : nullptr};
   const ItemFold f32{S->hoff, S->order, (p->epot & 2) ? S->part32 : nullptr};
-  epot_finalize_kernel<<<(unsigned)((nhalo + 127) / 128), 128, 0, st>>>(A, f64, f32, nhalo);
+  epot_finalize_kernel<<<finalize_blocks(nhalo), kFinBlock, 0, st>>>(A, f64, f32, nhalo);
   AHOP_CUDA_TRY(cudaGetLastError());
   int32_t herr = 0;
   AHOP_CUDA_TRY(cudaMemcpyAsync(&herr, &S->counter[3], 4, cudaMemcpyDeviceToHost, st));
