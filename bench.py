@@ -228,6 +228,36 @@ def halo_section(args, torch, dist=None):
             "virial_members_per_s": float(off[-1]) * world / (statistics.mean(tv) / 1e3)}
 
 
+def pipeline_section(args):
+    """Whole snapshots on one GPU: W untimed + K timed runs of
+    pipeline.run_snapshot; per-stage times of the last run and the mean
+    particles/s over the timed runs (host clock around the synchronised call,
+    pinned host arrays in, property rows out)."""
+    import numpy as np
+    from ahop_b200 import build, halo_props, pipeline, synthetic
+    build.build()
+    t0 = time.perf_counter()
+    ps = synthetic.workload(args.pipeline)
+    gen_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        pipeline.run_snapshot(ps.pos, ps.vel, ps.mass, box=ps.box, epot=2)
+    walls = []
+    res = None
+    for _ in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        res = pipeline.run_snapshot(ps.pos, ps.vel, ps.mass, box=ps.box, epot=2)
+        walls.append(time.perf_counter() - t0)
+    t = res["timings"]
+    stars = int(np.count_nonzero(ps.mass < ps.mass.max() * 0.5)) if ps.n else 0
+    return {"mode": "pipeline", "workload": args.pipeline, "npart": ps.n, "stars": stars, "generate_s": gen_s,
+            "steps": len(walls), "warmup": args.warmup, "wall_s": walls, "Mpart_per_s": ps.n / min(walls) / 1e6,
+            "nstruct": int(res["nstruct"]), "nb_of_halos": int(res["nb_of_halos"]),
+            "structures_with_members": int(len(res["ids"])), "members": int(res["members"]),
+            "stage_ms": {k: v for k, v in t.items() if not isinstance(v, dict)},
+            "finder_stages_ms": {k: v for k, v in t["finder_stages"].items()},
+            "props_stages": t["props_stages"], "tile_rows_per_bucket": halo_props.tiles()["rows"]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -244,6 +274,9 @@ def main():
                     help="pin the FP32 pair kernel's rows per item in every bucket (0: autotune)")
     ap.add_argument("--halo-only", action="store_true",
                     help="run only the batched halo section and print its JSON (profiling; not the bench line)")
+    ap.add_argument("--pipeline", default="", metavar="WORKLOAD",
+                    help="run whole snapshots (finder, MSM, member gather, FP32-compensated properties) on a named "
+                         "synthetic workload (e.g. c5_512cubed) and print per-stage times (not the bench line)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -261,6 +294,9 @@ def main():
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if args.pipeline:
+        print(json.dumps(pipeline_section(args)))
+        return
     if args.halo_only:
         from ahop_b200 import build
         build.build()

@@ -40,3 +40,28 @@ def select() -> dict:
                 first_sister=_arr(o.first_sister, ns), first_daughter=_arr(o.first_daughter, ns),
                 level=_arr(o.level, ns), pids_groupsorted=_arr(o.pids_groupsorted, n),
                 run_ids=_arr(o.run_ids, nr), run_idxs=_arr(o.run_idxs, nr), run_counts=_arr(o.run_counts, nr))
+
+
+def gather_device(d_pos, d_vel, d_mass, stream=None):
+    """Members of every structure (id >= 1) gathered on the device in structure
+    order, after ``select()``: returns (off int64[ns+1], ids int32[ns], pos,
+    vel, mass, density) as torch CUDA tensors."""
+    import torch
+    lib = L.lib()
+    lib.ahop_structure_members.argtypes = [C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
+    lib.ahop_gather_members_device.argtypes = [C.c_void_p] * 10
+    ns, nm = C.c_int32(), C.c_int64()
+    L.check(lib.ahop_structure_members(C.byref(ns), C.byref(nm)), "structure_members")
+    dev = d_pos.device
+    off = torch.empty(ns.value + 1, dtype=torch.int64, device=dev)
+    ids = torch.empty(max(ns.value, 1), dtype=torch.int32, device=dev)
+    m = nm.value
+    pos = torch.empty((max(m, 1), 3), dtype=torch.float64, device=dev)
+    vel = torch.empty((max(m, 1), 3), dtype=torch.float64, device=dev) if d_vel is not None else None
+    mass = torch.empty(max(m, 1), dtype=torch.float64, device=dev)
+    dens = torch.empty(max(m, 1), dtype=torch.float64, device=dev)
+    st = stream.cuda_stream if stream is not None else 0
+    ptr = lambda t: t.data_ptr() if t is not None else None
+    L.check(lib.ahop_gather_members_device(ptr(d_pos), ptr(d_vel), ptr(d_mass), ptr(off), ptr(ids), ptr(pos),
+                                           ptr(vel), ptr(mass), ptr(dens), st), "gather_members_device")
+    return off, ids[:ns.value], pos[:m], (vel[:m] if vel is not None else None), mass[:m], dens[:m]

@@ -158,7 +158,43 @@ struct MsmState {
   DevBuf d_scr, d_wp, d_key, d_key2, d_val, d_val2, d_struct, d_runs;
   HostBuf h_wp, h_struct, h_sorted, h_runs;
   AhopStructs out{};
+  bool have = false;       // a selection is held (device grouping below)
+  int32_t nruns = 0;       // runs of the sorted structure ids (id 0 first when present)
+  int32_t skip = 0;        // runs of id 0 (unassigned particles): 0 or 1
+  int64_t nmembers = 0;    // particles in structures (id >= 1)
+  int64_t n = 0;
+  int32_t ns = 0;          // structures of the selection (sizes the run arrays)
 };
+
+// Gather of the members of every structure (id >= 1) into structure order:
+// member k of the grouping is particle src = sorted[first + k]; per-structure
+// offsets from the run offsets.
+__global__ void gather_members_kernel(const int32_t* __restrict__ sorted, int64_t first, int64_t nmem,
+                                      const double* __restrict__ pos, const double* __restrict__ vel,
+                                      const double* __restrict__ mass, const double* __restrict__ dens,
+                                      double* __restrict__ gpos, double* __restrict__ gvel,
+                                      double* __restrict__ gmass, double* __restrict__ gdens) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= nmem) return;
+  const int64_t i = sorted[first + k];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    gpos[3 * k + c] = pos[3 * i + c];
+    if (gvel) gvel[3 * k + c] = vel[3 * i + c];
+  }
+  gmass[k] = mass[i];
+  if (gdens) gdens[k] = dens[i];
+}
+
+__global__ void member_offsets_kernel(const int32_t* __restrict__ idxs, int32_t skip, int32_t nr1, int64_t n,
+                                      int64_t* __restrict__ off, int32_t* __restrict__ ids,
+                                      const uint32_t* __restrict__ uids) {
+  const int32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r > nr1) return;
+  const int64_t base = idxs[skip];
+  off[r] = (r < nr1 ? (int64_t)idxs[skip + r] : n) - base;
+  if (r < nr1 && ids) ids[r] = (int32_t)uids[skip + r];
+}
 MsmState& msm_state() {
   static MsmState* s = new MsmState();
   return *s;
@@ -310,6 +346,19 @@ extern "C" int ahop_select_msm(AhopStructs* out) {
     AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
     AHOP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(E.d_cub.p, tmp, cnts, idxs, nr, st));
   }
+  // first run of a structure (id 0 = unassigned particles sorts first)
+  {
+    uint32_t first_id = 1;
+    if (nr > 0) AHOP_CUDA_TRY(cudaMemcpyAsync(&first_id, uids, 4, cudaMemcpyDeviceToHost, st));
+    int32_t first_idx = 0;
+    if (nr > 1) AHOP_CUDA_TRY(cudaMemcpyAsync(&first_idx, idxs + 1, 4, cudaMemcpyDeviceToHost, st));
+    AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+    S.nruns = nr;
+    S.skip = (nr > 0 && first_id == 0) ? 1 : 0;
+    S.nmembers = S.skip ? (nr > 1 ? n - first_idx : 0) : n;
+    S.n = n;
+    S.ns = ns;
+  }
   // host copies
   AHOP_CUDA_TRY(S.h_wp.ensure(n * 4 + 4));
   AHOP_CUDA_TRY(S.h_sorted.ensure(n * 4 + 4));
@@ -339,5 +388,46 @@ extern "C" int ahop_select_msm(AhopStructs* out) {
   out->run_ids = hr;
   out->run_idxs = hr + nr;
   out->run_counts = hr + 2 * nr;
+  S.have = true;
+  return AHOP_OK;
+}
+
+extern "C" int ahop_structure_members(int32_t* nstructs, int64_t* nmembers) {
+  MsmState& S = msm_state();
+  if (!nstructs || !nmembers) { set_error("null out"); return AHOP_EINVAL; }
+  if (!S.have) { set_error("no selection (call ahop_select_msm first)"); return AHOP_ESTATE; }
+  *nstructs = S.nruns - S.skip;
+  *nmembers = S.nmembers;
+  return AHOP_OK;
+}
+
+extern "C" int ahop_gather_members_device(const double* d_pos, const double* d_vel, const double* d_mass,
+                                          int64_t* d_off, int32_t* d_ids, double* d_gpos, double* d_gvel,
+                                          double* d_gmass, double* d_gdens, void* stream) {
+  Engine& E = engine();
+  MsmState& S = msm_state();
+  if (!S.have || !E.have_result) { set_error("no selection (call ahop_select_msm first)"); return AHOP_ESTATE; }
+  if (!d_pos || !d_mass || !d_off || !d_gpos || !d_gmass) { set_error("null device buffer"); return AHOP_EINVAL; }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // the selection's arrays were written on the engine stream
+  AHOP_CUDA_TRY(cudaStreamSynchronize(E.stream));
+  const int32_t nr1 = S.nruns - S.skip;
+  const int T = 256;
+  uint32_t* uids = S.d_runs.as<uint32_t>();
+  const int32_t ns2 = S.ns + 2;  // run arrays: uids, counts, offsets, each ns + 2 long
+  const int32_t* idxs = reinterpret_cast<const int32_t*>(uids + ns2) + ns2;
+  if (nr1 > 0) {
+    member_offsets_kernel<<<(nr1 + 1 + T - 1) / T, T, 0, st>>>(idxs, S.skip, nr1, S.n, d_off, d_ids, uids);
+    AHOP_CUDA_TRY(cudaGetLastError());
+  } else {
+    AHOP_CUDA_TRY(cudaMemsetAsync(d_off, 0, 8, st));
+  }
+  if (S.nmembers > 0) {
+    const int64_t first = S.n - S.nmembers;
+    gather_members_kernel<<<(unsigned)((S.nmembers + T - 1) / T), T, 0, st>>>(
+        S.d_val2.as<int32_t>(), first, S.nmembers, d_pos, d_vel, d_mass, E.d_dens_orig.as<double>(), d_gpos,
+        (d_vel && d_gvel) ? d_gvel : nullptr, d_gmass, d_gdens);
+    AHOP_CUDA_TRY(cudaGetLastError());
+  }
   return AHOP_OK;
 }

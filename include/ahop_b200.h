@@ -183,6 +183,18 @@ typedef struct {
   const int32_t *run_ids, *run_idxs, *run_counts;
 } AhopStructs;
 int ahop_select_msm(AhopStructs* out);
+/* The per-halo member gather of the reference's property loop (CHP:497-506:
+ * members of structure s are pids0_groupsorted[whereIam_idxs[s] ...]) on the
+ * device, after ahop_select_msm.  nstructs = structures with at least one
+ * member (ascending id), nmembers = particles in them.  The gather writes, in
+ * structure order: d_off[nstructs+1] member offsets, d_ids[nstructs] structure
+ * ids (may be NULL), and each member's d_pos/d_vel ((n,3), caller's particle
+ * order; d_vel/d_gvel may be NULL), d_mass and finder density (d_gdens may be
+ * NULL), on `stream`. */
+int ahop_structure_members(int32_t* nstructs, int64_t* nmembers);
+int ahop_gather_members_device(const double* d_pos, const double* d_vel, const double* d_mass, int64_t* d_off,
+                               int32_t* d_ids, double* d_gpos, double* d_gvel, double* d_gmass, double* d_gdens,
+                               void* stream);
 
 /* ---- batched halo properties ------------------------------------------------
  * Replaces the per-halo reductions of src/compute_halo_props.py run by
