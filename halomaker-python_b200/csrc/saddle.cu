@@ -12,6 +12,8 @@
 // The reference's row order among exactly equal saddle values follows its
 // unstable quicksort; nothing downstream depends on that order (the colouring
 // uses the row only up to the first value <= the threshold).
+#include <climits>
+#include <string>
 #include <cub/cub.cuh>
 
 #include "engine.h"
@@ -19,19 +21,24 @@
 
 namespace ahop {
 
+// Cross-group links per particle; the 64-bit total guards the 32-bit offsets.
 __global__ void link_count_kernel(const int32_t* __restrict__ group, const int32_t* __restrict__ nei, int nstore,
-                                  int nhop, int64_t n, int32_t* __restrict__ cnt) {
-  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  int32_t g1 = group[s];
+                                  int nhop, int64_t n, int32_t* __restrict__ cnt,
+                                  unsigned long long* __restrict__ total) {
+  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   int c = 0;
-  if (g1 > 0) {
-    for (int i = 0; i < nhop; ++i) {
-      int32_t g2 = group[nei[s * nstore + i]];
-      c += (g2 > 0 && g2 != g1);
+  if (s < n) {
+    const int32_t g1 = group[s];
+    if (g1 > 0) {
+      for (int i = 0; i < nhop; ++i) {
+        const int32_t g2 = group[nei[s * nstore + i]];
+        c += (g2 > 0 && g2 != g1);
+      }
     }
+    cnt[s] = c;
   }
-  cnt[s] = c;
+  const unsigned w = __reduce_add_sync(0xffffffffu, (unsigned)c);
+  if ((threadIdx.x & 31) == 0 && w) atomicAdd(total, (unsigned long long)w);
 }
 
 __global__ void link_emit_kernel(const int32_t* __restrict__ group, const int32_t* __restrict__ nei, int nstore,
@@ -107,8 +114,12 @@ int stage_saddles(Engine& E) {
   AHOP_CUDA_TRY(E.d_idx.ensure((n + 1) * 4));
   int32_t* cnt = E.d_idx2.as<int32_t>();
   int32_t* off = E.d_idx.as<int32_t>();
+  AHOP_CUDA_TRY(E.d_flags.ensure(512));
+  unsigned long long* d_total = reinterpret_cast<unsigned long long*>(E.d_flags.as<char>() + 448);
+  AHOP_CUDA_TRY(cudaMemsetAsync(d_total, 0, 8, st));
   E.launches++;
-  link_count_kernel<<<grid, T, 0, st>>>(E.d_group.as<int32_t>(), E.d_nei.as<int32_t>(), E.nstore, P.nhop, n, cnt);
+  link_count_kernel<<<grid, T, 0, st>>>(E.d_group.as<int32_t>(), E.d_nei.as<int32_t>(), E.nstore, P.nhop, n, cnt,
+                                        d_total);
   AHOP_CUDA_TRY(cudaGetLastError());
   AHOP_CUDA_TRY(cudaMemsetAsync(cnt + n, 0, 4, st));
   size_t tmp = 0;
@@ -117,8 +128,14 @@ int stage_saddles(Engine& E) {
   E.cub_calls++;
   AHOP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(E.d_cub.p, tmp, cnt, off, (int)(n + 1), st));
   int32_t nlink = 0;
+  unsigned long long total = 0;
   AHOP_CUDA_TRY(cudaMemcpyAsync(&nlink, off + n, 4, cudaMemcpyDeviceToHost, st));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(&total, d_total, 8, cudaMemcpyDeviceToHost, st));
   AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+  if (total > (unsigned long long)INT32_MAX) {
+    set_error("saddles: " + std::to_string(total) + " cross-group links exceed 32-bit offsets");
+    return AHOP_ELIMIT;
+  }
   const size_t nl = (size_t)(nlink > 0 ? nlink : 1);
   AHOP_CUDA_TRY(E.d_sad_key.ensure(nl * 8));
   AHOP_CUDA_TRY(E.d_sad_key2.ensure(nl * 8));
