@@ -425,6 +425,7 @@ def main():
                        "parallelism": f"replicas{world}"},
             "e2e": {"value": e2e, "unit": "Mpart/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roof, "stages_ms": mean_stage,
+            "stages_mpart_per_s": {k: (n / (v / 1e3) / 1e6 if v > 0 else None) for k, v in mean_stage.items()},
             "gpu_launches": int(stage[-1]["kernel_launches"]) * args.steps,
             "cub_calls_per_step": int(stage[-1]["cub_calls"]), "tree_waves": int(stage[-1]["tree_waves"]),
             "nnodes": nnodes, "tree_stats": tree_stats, "knn_stats": knn_stats, "clocks": clk.summary()}

@@ -29,16 +29,21 @@ def _arr(p, n):
     return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_int32)), (n,)).copy()
 
 
-def select() -> dict:
+def select(particle_views: bool = True) -> dict:
+    """particle_views=False skips the per-particle host arrays (whereIam_parts,
+    pids_groupsorted: None) -- for callers that gather members on the device."""
     lib = L.lib()
     lib.ahop_select_msm.argtypes = [C.POINTER(AhopStructs)]
+    lib.ahop_msm_set_particle_views.argtypes = [C.c_int32]
+    L.check(lib.ahop_msm_set_particle_views(int(bool(particle_views))), "msm_set_particle_views")
     o = AhopStructs()
     L.check(lib.ahop_select_msm(C.byref(o)), "select_msm")
     n, ns, nr = int(o.nusedpart), int(o.nstruct), int(o.ngroupruns)
+    pv = lambda p: _arr(p, n) if particle_views else None
     return dict(nstruct=ns, nb_of_halos=int(o.nb_of_halos), nb_of_subhalos=int(o.nb_of_subhalos),
-                whereIam_parts=_arr(o.whereIam_parts, n), mother=_arr(o.mother, ns),
+                whereIam_parts=pv(o.whereIam_parts), mother=_arr(o.mother, ns),
                 first_sister=_arr(o.first_sister, ns), first_daughter=_arr(o.first_daughter, ns),
-                level=_arr(o.level, ns), pids_groupsorted=_arr(o.pids_groupsorted, n),
+                level=_arr(o.level, ns), pids_groupsorted=pv(o.pids_groupsorted),
                 run_ids=_arr(o.run_ids, nr), run_idxs=_arr(o.run_idxs, nr), run_counts=_arr(o.run_counts, nr))
 
 

@@ -22,13 +22,15 @@ from . import finder, halo_props, msm
 
 
 def run_snapshot(pos: np.ndarray, vel: np.ndarray, mass: np.ndarray, box: float = 1.0, hub: float = 70.0,
-                 gravconst: float = 430.1, epot: int = 2, finder_params: dict | None = None) -> dict:
+                 gravconst: float = 430.1, epot: int = 2, finder_params: dict | None = None,
+                 particle_views: bool = False) -> dict:
     """Host arrays pos (N,3), vel (N,3), mass (N,) in box units ([-box/2, box/2)).
 
-    Returns the structure selection (ids, tree arrays), one property row per
-    structure with members (halo_props.FIELDS, structure order = ascending id)
-    and per-stage times in ms (device stages by CUDA events, the rest by the
-    host clock around synchronised steps)."""
+    Returns the structure selection (ids, tree arrays; the per-particle arrays
+    whereIam_parts / pids_groupsorted only with particle_views), one property
+    row per structure with members (halo_props.FIELDS, structure order =
+    ascending id) and per-stage times in ms (device stages by CUDA events, the
+    rest by the host clock around synchronised steps)."""
     import torch
     n = int(mass.shape[0])
     finder.configure(n, box=box, **(finder_params or {}))
@@ -54,7 +56,7 @@ def run_snapshot(pos: np.ndarray, vel: np.ndarray, mass: np.ndarray, box: float 
     times["finder"] = (time.perf_counter() - t0) * 1e3
     times["finder_stages"] = L.timings()
     t0 = time.perf_counter()
-    sel = msm.select()
+    sel = msm.select(particle_views=particle_views)
     times["msm"] = (time.perf_counter() - t0) * 1e3
     t0 = time.perf_counter()
     off, ids, gpos, gvel, gmass, gdens = msm.gather_device(d_pos, d_vel, d_mass, stream=st)

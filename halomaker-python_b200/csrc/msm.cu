@@ -164,6 +164,7 @@ struct MsmState {
   int64_t nmembers = 0;    // particles in structures (id >= 1)
   int64_t n = 0;
   int32_t ns = 0;          // structures of the selection (sizes the run arrays)
+  bool particle_views = true;  // copy whereIam_parts / pids_groupsorted to the host
 };
 
 // Gather of the members of every structure (id >= 1) into structure order:
@@ -364,8 +365,10 @@ extern "C" int ahop_select_msm(AhopStructs* out) {
   AHOP_CUDA_TRY(S.h_sorted.ensure(n * 4 + 4));
   AHOP_CUDA_TRY(S.h_struct.ensure(S4 * 4));
   AHOP_CUDA_TRY(S.h_runs.ensure((size_t)(nr + 1) * 4 * 3));
-  AHOP_CUDA_TRY(cudaMemcpyAsync(S.h_wp.p, S.d_wp.p, n * 4, cudaMemcpyDeviceToHost, st));
-  AHOP_CUDA_TRY(cudaMemcpyAsync(S.h_sorted.p, S.d_val2.p, n * 4, cudaMemcpyDeviceToHost, st));
+  if (S.particle_views) {
+    AHOP_CUDA_TRY(cudaMemcpyAsync(S.h_wp.p, S.d_wp.p, n * 4, cudaMemcpyDeviceToHost, st));
+    AHOP_CUDA_TRY(cudaMemcpyAsync(S.h_sorted.p, S.d_val2.p, n * 4, cudaMemcpyDeviceToHost, st));
+  }
   if (ns > 0) AHOP_CUDA_TRY(cudaMemcpyAsync(S.h_struct.p, mother_s, S4 * 4, cudaMemcpyDeviceToHost, st));
   int32_t* hr = S.h_runs.as<int32_t>();
   AHOP_CUDA_TRY(cudaMemcpyAsync(hr, uids, (size_t)nr * 4, cudaMemcpyDeviceToHost, st));
@@ -378,17 +381,22 @@ extern "C" int ahop_select_msm(AhopStructs* out) {
   out->nb_of_halos = nhalo;
   out->nb_of_subhalos = ns - nhalo;
   out->nusedpart = n;
-  out->whereIam_parts = S.h_wp.as<int32_t>();
+  out->whereIam_parts = S.particle_views ? S.h_wp.as<int32_t>() : nullptr;
   out->mother = hs;
   out->first_sister = hs + sw;
   out->first_daughter = hs + 2 * sw;
   out->level = hs + 3 * sw;
-  out->pids_groupsorted = S.h_sorted.as<int32_t>();
+  out->pids_groupsorted = S.particle_views ? S.h_sorted.as<int32_t>() : nullptr;
   out->ngroupruns = nr;
   out->run_ids = hr;
   out->run_idxs = hr + nr;
   out->run_counts = hr + 2 * nr;
   S.have = true;
+  return AHOP_OK;
+}
+
+extern "C" int ahop_msm_set_particle_views(int32_t on) {
+  msm_state().particle_views = on != 0;
   return AHOP_OK;
 }
 

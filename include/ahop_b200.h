@@ -183,6 +183,10 @@ typedef struct {
   const int32_t *run_ids, *run_idxs, *run_counts;
 } AhopStructs;
 int ahop_select_msm(AhopStructs* out);
+/* on = 0: later selections skip the host copies of the two per-particle arrays
+ * (whereIam_parts and pids_groupsorted come back NULL); for callers that use
+ * the device gather below (default on). */
+int ahop_msm_set_particle_views(int32_t on);
 /* The per-halo member gather of the reference's property loop (CHP:497-506:
  * members of structure s are pids0_groupsorted[whereIam_idxs[s] ...]) on the
  * device, after ahop_select_msm.  nstructs = structures with at least one

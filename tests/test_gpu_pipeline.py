@@ -25,7 +25,7 @@ def test_device_pipeline_matches_host_steps():
     ps = synthetic.small_box(120_000, 120, seed=31, nmax=8000)
     halo_props.set_tiles([256] * halo_props.BUCKETS)
     try:
-        res = pipeline.run_snapshot(ps.pos, ps.vel, ps.mass, box=1.0, hub=70.0, epot=3)
+        res = pipeline.run_snapshot(ps.pos, ps.vel, ps.mass, box=1.0, hub=70.0, epot=3, particle_views=True)
         finder.configure(ps.n)
         out = finder.run(ps.pos, ps.mass)
         sel = msm.select()
