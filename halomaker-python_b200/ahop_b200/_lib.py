@@ -14,7 +14,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libahop_b200.so")
 
-AHOP_ERRORS = {1: "EINVAL", 2: "ECUDA", 3: "ENOMEM", 4: "ESTATE", 5: "EINVARIANT", 6: "ELIMIT"}
+AHOP_ERRORS = {1: "EINVAL", 2: "ECUDA", 3: "ENOMEM", 4: "ESTATE", 5: "EINVARIANT", 6: "ELIMIT", 7: "EDATA", 8: "EIO"}
 
 
 class AhopInit(C.Structure):

@@ -25,7 +25,7 @@ BUILD = os.path.join(PKG_ROOT, "_build")
 LIB = os.path.join(HERE, "libahop_b200.so")
 
 FINDER_SOURCES = ["knn.cu", "hop.cu", "saddle.cu", "forest.cu", "nodes.cu", "msm.cu", "adjoint.cu", "capi.cu"]
-PROPS_SOURCES = ["halo_props.cu", "halo_virial.cu"]
+PROPS_SOURCES = ["halo_props.cu", "halo_virial.cu", "ramses.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -18,7 +18,7 @@ import time
 import numpy as np
 
 from . import _lib as L
-from . import finder, halo_props, msm
+from . import finder, halo_props, msm, ramses
 
 
 def run_snapshot(pos: np.ndarray, vel: np.ndarray, mass: np.ndarray, box: float = 1.0, hub: float = 70.0,
@@ -35,8 +35,6 @@ def run_snapshot(pos: np.ndarray, vel: np.ndarray, mass: np.ndarray, box: float 
     n = int(mass.shape[0])
     finder.configure(n, box=box, **(finder_params or {}))
     dev = torch.device("cuda")
-    st = torch.cuda.current_stream()
-    lib = L.lib()
     times = {}
     t0 = time.perf_counter()
     h_pos = torch.from_numpy(np.ascontiguousarray(pos, np.float64)).pin_memory()
@@ -49,6 +47,16 @@ def run_snapshot(pos: np.ndarray, vel: np.ndarray, mass: np.ndarray, box: float 
     d_mass = h_mass.to(dev, non_blocking=True)
     torch.cuda.synchronize()
     times["h2d"] = (time.perf_counter() - t0) * 1e3
+    return _run_device(d_pos, d_vel, d_mass, box, hub, gravconst, epot, particle_views, times)
+
+
+def _run_device(d_pos, d_vel, d_mass, box, hub, gravconst, epot, particle_views, times):
+    """Finder, selection, member gather and properties on device arrays."""
+    import torch
+    n = int(d_mass.shape[0])
+    dev = d_pos.device
+    st = torch.cuda.current_stream()
+    lib = L.lib()
     t0 = time.perf_counter()
     L.check(lib.ahop_compute_adaptahop_device(d_pos.data_ptr(), d_mass.data_ptr(), n, C.c_void_p(st.cuda_stream)),
             "compute_adaptahop_device")
@@ -76,3 +84,22 @@ def run_snapshot(pos: np.ndarray, vel: np.ndarray, mass: np.ndarray, box: float 
     off_h = off.cpu().numpy()
     times["d2h"] = (time.perf_counter() - t0) * 1e3
     return dict(sel, ids=ids_h, offsets=off_h, props=rows, members=int(off_h[-1]) if ns else 0, timings=times)
+
+
+def run_snapshot_files(repository, version: int = 3, family: str = "all", scale_l: float = 1.0,
+                       scale_t: float = 1.0, box: float = 1.0, hub: float = 70.0, gravconst: float = 430.1,
+                       epot: int = 2, finder_params: dict | None = None, particle_views: bool = False) -> dict:
+    """The same snapshot step starting from RAMSES part files (an
+    output_NNNNN directory or the file paths): read_ramses_new_101's particle
+    arrays are decoded on the device (ramses.read_parts) and never visit host
+    memory.  Positions come out in [-0.5, 0.5) box units, as the reference's
+    reader leaves them."""
+    import torch
+    t0 = time.perf_counter()
+    r = ramses.read_parts(repository, version, family, scale_l, scale_t)
+    torch.cuda.synchronize()
+    times = {"read": (time.perf_counter() - t0) * 1e3}
+    finder.configure(int(r["nselected"]), box=box, **(finder_params or {}))
+    out = _run_device(r["pos"], r["vel"], r["mass"], box, hub, gravconst, epot, particle_views, times)
+    out.update(ndm=r["ndm"], nstar=r["nstar"], nselected=r["nselected"])
+    return out

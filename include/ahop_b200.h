@@ -29,7 +29,9 @@ enum {
   AHOP_ENOMEM = 3,     /* device allocation failed */
   AHOP_ESTATE = 4,     /* called out of order (e.g. outputs before compute) */
   AHOP_EINVARIANT = 5, /* an internal consistency check failed (Fortran would STOP) */
-  AHOP_ELIMIT = 6      /* a bounded device loop hit its iteration cap */
+  AHOP_ELIMIT = 6,     /* a bounded device loop hit its iteration cap */
+  AHOP_EDATA = 7,      /* input data rejected (malformed file, ids outside the dense layout) */
+  AHOP_EIO = 8         /* a file could not be opened or read */
 };
 
 /* Arguments of sync_from_init_adaptahop (fortran/compute_adaptahop.pyf:25-48,
@@ -199,6 +201,33 @@ int ahop_structure_members(int32_t* nstructs, int64_t* nmembers);
 int ahop_gather_members_device(const double* d_pos, const double* d_vel, const double* d_mass, int64_t* d_off,
                                int32_t* d_ids, double* d_gpos, double* d_gvel, double* d_gmass, double* d_gdens,
                                void* stream);
+
+/* ---- RAMSES particle reader --------------------------------------------------
+ * Replaces _read_ramses_new_1010 (src/input_output.py:624-760) and the
+ * count/load passes of read_ramses_new_101 (input_output.py:856-989) with the
+ * stellar payload off: the part files' records are decoded on the device into
+ * the dense arrays the finder reads (pos_10 = x - 0.5, vel_10 = v * scale_l /
+ * scale_t * 1e-5, mass_10; source_pid_10 = |id| for a single family), in the
+ * reference's layout (ind = |id| - 1, stars after the ndm dark-matter rows
+ * when family = all).  open reads every file once (paths in cpu order) and
+ * counts the families; decode fills caller device arrays of nselected rows
+ * (d_source_pid may be NULL; it is written for family dm/star only).  Errors
+ * as the reference raises them: AHOP_EDATA for record-length mismatches,
+ * selected ids outside [1, nselected] or repeated within a file, unwritten
+ * rows of a single family, no particle selected; AHOP_EIO for unreadable
+ * files. */
+typedef struct {
+  int32_t version;  /* 3 (Ra3: families from birth time and id sign) or 4 (Ra4: family record) */
+  int32_t family;   /* H.family: 0 all, 1 dm, 2 star */
+  double scale_l, scale_t; /* info file units (unit_l, unit_t) */
+} AhopRamsesParams;
+typedef struct {
+  int64_t total, ndm, nstar, nselected;
+  int32_t nfiles, ndim;
+} AhopRamsesCounts;
+int ahop_ramses_open(const char* const* paths, int32_t nfiles, const AhopRamsesParams* p, AhopRamsesCounts* out);
+int ahop_ramses_decode_device(double* d_pos, double* d_vel, double* d_mass, int64_t* d_source_pid, void* stream);
+int ahop_ramses_close(void);
 
 /* ---- batched halo properties ------------------------------------------------
  * Replaces the per-halo reductions of src/compute_halo_props.py run by
