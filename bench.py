@@ -228,6 +228,55 @@ def halo_section(args, torch, dist=None):
             "virial_members_per_s": float(off[-1]) * world / (statistics.mean(tv) / 1e3)}
 
 
+def reader_section(args):
+    """RAMSES part files -> device arrays: the device reader (record walk,
+    one read per file into pinned memory, payload copies, family count and
+    scatter kernels) against the CPU restatement of the reference's reader
+    (NumPy, one thread).  The files were just written, so they are read from
+    the page cache: this times decoding, not the disk."""
+    import tempfile
+    import numpy as np
+    import torch
+    from ahop_b200 import build, ramses, synthetic
+    sys.path.insert(0, os.path.join(REPO, "tests", "golden"))
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import ramses_files
+    import ramses_oracle
+    build.build()
+    ps = synthetic.workload(args.reader)
+    n = ps.n
+    star = ps.mass < 0.5 * ps.mass.max()
+    ids = np.empty(n, np.int32)
+    ids[~star] = np.arange(1, int((~star).sum()) + 1)
+    ids[star] = np.arange(1, int(star.sum()) + 1)
+    kind = np.where(star, 2, 1).astype(np.int8)
+    P = dict(pos=ps.pos + 0.5, vel=ps.vel, mass=ps.mass, id=ids, fam=kind, kind=kind,
+             tbirth=np.zeros(n), level=np.zeros(n, np.int32), metal=np.zeros(n))
+    ncpu = 64
+    bounds = np.linspace(0, n, ncpu + 1).astype(np.int64)
+    res = {"mode": "reader", "workload": args.reader, "npart": n, "stars": int(star.sum()), "files": ncpu,
+           "format": "Ra4"}
+    with tempfile.TemporaryDirectory() as tmp:
+        paths = ramses_files.write_arrays(tmp, P, 4, bounds)
+        res["bytes"] = int(sum(os.path.getsize(p) for p in paths))
+        walls = []
+        for i in range(args.warmup + max(1, args.steps)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = ramses.read_parts(paths, 4, "all", 1.0, 1.0)
+            torch.cuda.synchronize()
+            if i >= args.warmup:
+                walls.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        o = ramses_oracle.read_parts(paths, 4, "all", 1.0, 1.0)
+        cpu_s = time.perf_counter() - t0
+        same = all(np.array_equal(r[k].cpu().numpy(), o[k]) for k in ("pos", "vel", "mass"))
+    res.update(device_s=walls, device_Mpart_per_s=n / min(walls) / 1e6, device_GB_per_s=res["bytes"] / min(walls) / 1e9,
+               cpu_s=cpu_s, cpu_Mpart_per_s=n / cpu_s / 1e6, cpu_cores=1, cpu_kind="port (NumPy)",
+               identical_to_cpu=bool(same))
+    return res
+
+
 def pipeline_section(args):
     """Whole snapshots on one GPU: W untimed + K timed runs of
     pipeline.run_snapshot; per-stage times of the last run and the mean
@@ -274,6 +323,9 @@ def main():
                     help="pin the FP32 pair kernel's rows per item in every bucket (0: autotune)")
     ap.add_argument("--halo-only", action="store_true",
                     help="run only the batched halo section and print its JSON (profiling; not the bench line)")
+    ap.add_argument("--reader", default="", metavar="WORKLOAD",
+                    help="write a named synthetic workload as RAMSES Ra4 part files (64 files, in a temporary "
+                         "directory) and time the device reader against the CPU restatement (not the bench line)")
     ap.add_argument("--pipeline", default="", metavar="WORKLOAD",
                     help="run whole snapshots (finder, MSM, member gather, FP32-compensated properties) on a named "
                          "synthetic workload (e.g. c5_512cubed) and print per-stage times (not the bench line)")
@@ -296,6 +348,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     if args.pipeline:
         print(json.dumps(pipeline_section(args)))
+        return
+    if args.reader:
+        print(json.dumps(reader_section(args)))
         return
     if args.halo_only:
         from ahop_b200 import build

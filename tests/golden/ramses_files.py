@@ -71,6 +71,13 @@ def write_case(root: str, seed: int, version: int, ncpu: int, ndm: int, nstar: i
     rng = np.random.Generator(np.random.PCG64(seed + 1000))
     cuts = np.sort(rng.integers(0, n + 1, ncpu - 1))
     bounds = np.concatenate([[0], cuts, [n]])
+    return write_arrays(root, P, version, bounds, seed, nchar)
+
+
+def write_arrays(root: str, P: dict, version: int, bounds, seed: int = 0, nchar: str = "00001") -> list:
+    """Write the particle table P (make_particles' keys) as part files, file c
+    holding rows [bounds[c], bounds[c+1])."""
+    ncpu = len(bounds) - 1
     out = os.path.join(root, f"output_{nchar}")
     os.makedirs(out, exist_ok=True)
     paths = []
