@@ -199,7 +199,12 @@ __global__ void __launch_bounds__(kPB) halo_moments_kernel(HaloArgs A) {
     long long ii = s_best_i[0];
     for (int w = 1; w < kPB / 32; ++w)
       if (s_best_d[w] > d || (s_best_d[w] == d && s_best_i[w] < ii)) { d = s_best_d[w]; ii = s_best_i[w]; }
-    s_c[0] = A.pos[3 * ii]; s_c[1] = A.pos[3 * ii + 1]; s_c[2] = A.pos[3 * ii + 2];
+    if (ii != LLONG_MAX) {
+      s_c[0] = A.pos[3 * ii]; s_c[1] = A.pos[3 * ii + 1]; s_c[2] = A.pos[3 * ii + 2];
+    } else {  // a halo without members
+      s_c[0] = s_c[1] = s_c[2] = 0.0;
+      ii = b0;
+    }
     s_c[3] = mvx / m; s_c[4] = mvy / m; s_c[5] = mvz / m;
     s_c[6] = (double)(ii - b0);
   }
@@ -247,6 +252,197 @@ __global__ void __launch_bounds__(kPB) halo_moments_kernel(HaloArgs A) {
     o[HP_SIGMA] = sqrt(sg / m);
     o[HP_ICENTER] = s_c[6];
   }
+}
+
+// ------------------------------------------------- chunked moment passes
+// The same two passes as halo_moments_kernel with every halo cut into chunks
+// of kMomChunk members, one block per chunk, so a halo of a million members
+// no longer runs on one block.  Chunk partials are folded per halo in chunk
+// order (deterministic); the densest member is an exact argmax, so the centre
+// is the one the single-block kernel finds.
+constexpr int64_t kMomChunk = 8192;
+
+struct MomChunk {
+  int32_t h, pad;
+  int64_t b0, b1;
+};
+struct MomP1 {
+  double m, mvx, mvy, mvz, bd;
+  long long bi;
+};
+constexpr int kP2 = 11;  // Lx Ly Lz Ixx Ixy Ixz Iyy Iyz Izz ek sg
+struct MomP2 {
+  double v[kP2];
+  double r2max;
+};
+struct MomCentre {
+  double c[6];  // centre x, y, z, bulk velocity x, y, z
+  long long ic; // centre member (absolute index)
+};
+
+// Sums of N values over the block (warp shuffles, then warp 0 over the
+// warps in order); the totals land in every thread's v.
+template <int N>
+__device__ __forceinline__ void block_sum_n(double (&v)[N], double* sh) {
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    if (lane == 0) sh[k * (kPB / 32) + w] = v[k];
+  }
+  __syncthreads();
+  if (tid < N) {
+    double s = sh[tid * (kPB / 32)];
+    for (int j = 1; j < kPB / 32; ++j) s += sh[tid * (kPB / 32) + j];
+    sh[N * (kPB / 32) + tid] = s;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < N; ++k) v[k] = sh[N * (kPB / 32) + k];
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kPB) mom_pass1_kernel(HaloArgs A, const MomChunk* __restrict__ ch,
+                                                        MomP1* __restrict__ P) {
+  __shared__ double sh[5 * (kPB / 32) + 8];
+  __shared__ double s_bd[kPB / 32];
+  __shared__ long long s_bi[kPB / 32];
+  const int tid = threadIdx.x;
+  const MomChunk c = ch[blockIdx.x];
+  double v[4] = {0, 0, 0, 0}, bd = -DBL_MAX;
+  long long bi = LLONG_MAX;
+  for (int64_t i = c.b0 + tid; i < c.b1; i += kPB) {
+    const double w = A.mass[i];
+    v[0] += w;
+    v[1] += w * A.vel[3 * i];
+    v[2] += w * A.vel[3 * i + 1];
+    v[3] += w * A.vel[3 * i + 2];
+    const double d = A.dens[i];
+    if (d > bd || (d == bd && i < bi)) { bd = d; bi = i; }  // np.argmax: first maximum
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double od = __shfl_xor_sync(0xffffffffu, bd, o);
+    const long long oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (od > bd || (od == bd && oi < bi)) { bd = od; bi = oi; }
+  }
+  if ((tid & 31) == 0) { s_bd[tid >> 5] = bd; s_bi[tid >> 5] = bi; }
+  block_sum_n<4>(v, sh);
+  if (tid == 0) {
+    bd = s_bd[0]; bi = s_bi[0];
+    for (int w = 1; w < kPB / 32; ++w)
+      if (s_bd[w] > bd || (s_bd[w] == bd && s_bi[w] < bi)) { bd = s_bd[w]; bi = s_bi[w]; }
+    P[blockIdx.x] = MomP1{v[0], v[1], v[2], v[3], bd, bi};
+  }
+}
+
+// per halo: chunk partials in order -> mass, bulk velocity, densest member
+__global__ void mom_fold1_kernel(HaloArgs A, const int64_t* __restrict__ hcoff, const MomP1* __restrict__ P,
+                                 MomCentre* __restrict__ C, int64_t nhalo) {
+  const int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (h >= nhalo) return;
+  double m = 0, mvx = 0, mvy = 0, mvz = 0, bd = -DBL_MAX;
+  long long bi = LLONG_MAX;
+  for (int64_t k = hcoff[h]; k < hcoff[h + 1]; ++k) {
+    const MomP1 p = P[k];
+    m += p.m; mvx += p.mvx; mvy += p.mvy; mvz += p.mvz;
+    if (p.bd > bd || (p.bd == bd && p.bi < bi)) { bd = p.bd; bi = p.bi; }
+  }
+  MomCentre c;
+  if (bi != LLONG_MAX) {
+    c.c[0] = A.pos[3 * bi]; c.c[1] = A.pos[3 * bi + 1]; c.c[2] = A.pos[3 * bi + 2];
+  } else {
+    c.c[0] = c.c[1] = c.c[2] = 0.0;
+  }
+  c.c[3] = mvx / m; c.c[4] = mvy / m; c.c[5] = mvz / m;
+  c.ic = bi;
+  C[h] = c;
+  A.out[(size_t)kHaloFields * h + HP_M] = m;
+}
+
+// shrinking-sphere refinement (SC on): one block per halo, as in the
+// single-block kernel
+__global__ void __launch_bounds__(kPB) mom_sc_kernel(HaloArgs A, MomCentre* __restrict__ C) {
+  __shared__ double sh[kPB / 32];
+  __shared__ double s_best_d[kPB / 32];
+  __shared__ long long s_best_i[kPB / 32];
+  __shared__ double s_c[7];
+  const int64_t h = blockIdx.x;
+  const int64_t b0 = A.off[h], b1 = A.off[h + 1];
+  if (b1 <= b0) return;
+  if (threadIdx.x < 6) s_c[threadIdx.x] = C[h].c[threadIdx.x];
+  if (threadIdx.x == 6) s_c[6] = (double)(C[h].ic - b0);
+  __syncthreads();
+  shrink_sphere_centre(A, b0, b1, s_c, sh, s_best_d, s_best_i);
+  if (threadIdx.x < 3) C[h].c[threadIdx.x] = s_c[threadIdx.x];
+  if (threadIdx.x == 0) C[h].ic = b0 + (long long)s_c[6];
+}
+
+__global__ void __launch_bounds__(kPB) mom_pass2_kernel(HaloArgs A, const MomChunk* __restrict__ ch,
+                                                        const MomCentre* __restrict__ C, MomP2* __restrict__ P) {
+  __shared__ double sh[(kP2 + 1) * (kPB / 32) + 16];
+  __shared__ double s_r[kPB / 32];
+  const int tid = threadIdx.x;
+  const MomChunk k = ch[blockIdx.x];
+  const MomCentre c = C[k.h];
+  const double cx = c.c[0], cy = c.c[1], cz = c.c[2], vx = c.c[3], vy = c.c[4], vz = c.c[5];
+  double v[kP2] = {};
+  double r2max = 0;
+  for (int64_t i = k.b0 + tid; i < k.b1; i += kPB) {
+    const double w = A.mass[i];
+    const double dx = wrap_chp(A.pos[3 * i] - cx, A.L, A.h, A.periodic);
+    const double dy = wrap_chp(A.pos[3 * i + 1] - cy, A.L, A.h, A.periodic);
+    const double dz = wrap_chp(A.pos[3 * i + 2] - cz, A.L, A.h, A.periodic);
+    const double ux = A.vel[3 * i] - vx, uy = A.vel[3 * i + 1] - vy, uz = A.vel[3 * i + 2] - vz;
+    const double px = w * ux, py = w * uy, pz = w * uz;
+    v[0] += dy * pz - dz * py;
+    v[1] += dz * px - dx * pz;
+    v[2] += dx * py - dy * px;
+    r2max = fmax(r2max, dx * dx + dy * dy + dz * dz);
+    v[3] += w * dx * dx; v[4] += w * dx * dy; v[5] += w * dx * dz;
+    v[6] += w * dy * dy; v[7] += w * dy * dz; v[8] += w * dz * dz;
+    const double tx = ux + dx * A.hub, ty = uy + dy * A.hub, tz = uz + dz * A.hub;
+    v[9] += w * (tx * tx + ty * ty + tz * tz);
+    v[10] += w * (ux * ux + uy * uy + uz * uz);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) r2max = fmax(r2max, __shfl_xor_sync(0xffffffffu, r2max, o));
+  if ((tid & 31) == 0) s_r[tid >> 5] = r2max;
+  block_sum_n<kP2>(v, sh);
+  if (tid == 0) {
+    double rm = s_r[0];
+    for (int w = 1; w < kPB / 32; ++w) rm = fmax(rm, s_r[w]);
+    MomP2 p;
+#pragma unroll
+    for (int j = 0; j < kP2; ++j) p.v[j] = v[j];
+    p.r2max = rm;
+    P[blockIdx.x] = p;
+  }
+}
+
+__global__ void mom_fold2_kernel(HaloArgs A, const int64_t* __restrict__ hcoff, const MomP2* __restrict__ P,
+                                 const MomCentre* __restrict__ C, int64_t nhalo) {
+  const int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (h >= nhalo) return;
+  double v[kP2] = {};
+  double rm = 0;
+  for (int64_t k = hcoff[h]; k < hcoff[h + 1]; ++k) {
+#pragma unroll
+    for (int j = 0; j < kP2; ++j) v[j] += P[k].v[j];
+    rm = fmax(rm, P[k].r2max);
+  }
+  const MomCentre c = C[h];
+  double* o = A.out + (size_t)kHaloFields * h;
+  const double m = o[HP_M];
+  o[HP_PX] = c.c[0]; o[HP_PY] = c.c[1]; o[HP_PZ] = c.c[2];
+  o[HP_VX] = c.c[3]; o[HP_VY] = c.c[4]; o[HP_VZ] = c.c[5];
+  o[HP_LX] = v[0]; o[HP_LY] = v[1]; o[HP_LZ] = v[2];
+  o[HP_R] = sqrt(rm);
+  o[HP_IXX] = v[3]; o[HP_IXY] = v[4]; o[HP_IXZ] = v[5]; o[HP_IYY] = v[6]; o[HP_IYZ] = v[7]; o[HP_IZZ] = v[8];
+  o[HP_EK] = 0.5 * v[9];
+  o[HP_SIGMA] = sqrt(v[10] / m);
+  o[HP_ICENTER] = (double)(c.ic - A.off[h]);
 }
 
 // ---------------------------------------------------------------- pair sums
@@ -714,7 +910,8 @@ struct ListBufs {
 
 struct GraphSig {
   HaloArgs A;
-  const void* ptr[10];
+  const void* ptr[15];
+  int64_t nch;
   int64_t nhalo;
   int32_t n64, n32, grid64, grid32, epot, pad;
 };
@@ -723,6 +920,8 @@ struct HaloEngine {
   DevBuf d_off, d_pos, d_vel, d_mass, d_dens, d_out;  // staging for host inputs
   ListBufs l64, l32, tune;
   DevBuf d_hshape, d_counter, d_err;
+  DevBuf d_mch, d_mcoff, d_mp1, d_mp2, d_mcen;  // chunked moment passes
+  int64_t nch = 0;
   cudaEvent_t ev[5] = {};
   cudaEvent_t ev_in = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
   bool ready = false;
@@ -852,7 +1051,25 @@ static int enqueue_props(HaloEngine& H, const HaloArgs& A, int64_t nhalo, int ep
   AHOP_CUDA_TRY(cudaEventRecordWithFlags(H.ev[0], s, flags));
   *launches = 0;
   if (nhalo > 0) {
-    halo_moments_kernel<<<(unsigned)nhalo, kPB, 0, s>>>(A);
+    const unsigned hb = (unsigned)((nhalo + 127) / 128);
+    if (H.nch > 0) {
+      mom_pass1_kernel<<<(unsigned)H.nch, kPB, 0, s>>>(A, H.d_mch.as<MomChunk>(), H.d_mp1.as<MomP1>());
+      ++*launches;
+    }
+    mom_fold1_kernel<<<hb, 128, 0, s>>>(A, H.d_mcoff.as<int64_t>(), H.d_mp1.as<MomP1>(), H.d_mcen.as<MomCentre>(),
+                                        nhalo);
+    ++*launches;
+    if (A.sc) {
+      mom_sc_kernel<<<(unsigned)nhalo, kPB, 0, s>>>(A, H.d_mcen.as<MomCentre>());
+      ++*launches;
+    }
+    if (H.nch > 0) {
+      mom_pass2_kernel<<<(unsigned)H.nch, kPB, 0, s>>>(A, H.d_mch.as<MomChunk>(), H.d_mcen.as<MomCentre>(),
+                                                       H.d_mp2.as<MomP2>());
+      ++*launches;
+    }
+    mom_fold2_kernel<<<hb, 128, 0, s>>>(A, H.d_mcoff.as<int64_t>(), H.d_mp2.as<MomP2>(), H.d_mcen.as<MomCentre>(),
+                                        nhalo);
     ++*launches;
     AHOP_CUDA_TRY(cudaGetLastError());
   }
@@ -955,6 +1172,21 @@ static int halo_run(HaloEngine& H, const AhopHaloParams* p, const int64_t* d_off
   H.L32.hoff[nhalo] = (int64_t)H.L32.items.size();
   schedule(H.L64);
   schedule(H.L32);
+  // chunks of the moment passes
+  std::vector<MomChunk> mch;
+  std::vector<int64_t> mcoff(nhalo + 1, 0);
+  for (int64_t h = 0; h < nhalo; ++h) {
+    mcoff[h] = (int64_t)mch.size();
+    for (int64_t b = h_off[h]; b < h_off[h + 1]; b += kMomChunk)
+      mch.push_back(MomChunk{(int32_t)h, 0, b, std::min<int64_t>(h_off[h + 1], b + kMomChunk)});
+  }
+  mcoff[nhalo] = (int64_t)mch.size();
+  H.nch = (int64_t)mch.size();
+  if ((rc = upload(H.d_mch, mch, st))) return rc;
+  if ((rc = upload(H.d_mcoff, mcoff, st))) return rc;
+  AHOP_CUDA_TRY(H.d_mp1.ensure(std::max<size_t>(mch.size() * sizeof(MomP1), 16)));
+  AHOP_CUDA_TRY(H.d_mp2.ensure(std::max<size_t>(mch.size() * sizeof(MomP2), 16)));
+  AHOP_CUDA_TRY(H.d_mcen.ensure(std::max<size_t>((size_t)nhalo * sizeof(MomCentre), 16)));
   if ((rc = upload_list(H.l64, H.L64, st))) return rc;
   if ((rc = upload_list(H.l32, H.L32, st))) return rc;
   if ((rc = upload(H.d_hshape, hshape, st))) return rc;
@@ -968,9 +1200,11 @@ static int halo_run(HaloEngine& H, const AhopHaloParams* p, const int64_t* d_off
     GraphSig sig;
     memset(&sig, 0, sizeof sig);
     sig.A = A;
-    const void* ptrs[10] = {H.l64.items.p, H.l64.order.p, H.l64.hoff.p, H.l64.part.p, H.l32.items.p,
-                            H.l32.order.p, H.l32.hoff.p, H.l32.part.p, H.d_hshape.p, H.d_counter.p};
+    const void* ptrs[15] = {H.l64.items.p, H.l64.order.p, H.l64.hoff.p, H.l64.part.p, H.l32.items.p,
+                            H.l32.order.p, H.l32.hoff.p, H.l32.part.p, H.d_hshape.p, H.d_counter.p,
+                            H.d_mch.p,     H.d_mcoff.p,   H.d_mp1.p,    H.d_mp2.p,    H.d_mcen.p};
     memcpy(sig.ptr, ptrs, sizeof ptrs);
+    sig.nch = H.nch;
     sig.nhalo = nhalo; sig.n64 = H.l64.n; sig.n32 = H.l32.n; sig.grid64 = grid64; sig.grid32 = grid32;
     sig.epot = epot;
     if (!H.gexec || memcmp(&sig, &H.gsig, sizeof sig) != 0) {
