@@ -13,19 +13,22 @@
 //   compute_spin_parameter_1c (CHP:1599-1602)
 //
 // Layout: members of halo h are rows [off[h], off[h+1]) of pos/vel (n,3),
-// mass (n) and density (n), FP64 in HBM.  One block per halo computes the
-// O(n) quantities (two passes over the members, fixed-order block
-// reductions, so results are deterministic).  The O(n^2) potential runs as
-// one persistent launch over a work list of (halo, i-tile) items sorted by
-// decreasing cost; each item sums m_j / r_ij for its 256 i-particles over all
-// j > i.  Two forms share the schedule:
+// mass (n) and density (n), FP64 in HBM.  The O(n) quantities come from two
+// passes over the members in chunks of 8,192 (a block per chunk, partials
+// folded per halo in chunk order, so results are deterministic).  The O(n^2)
+// potential runs as persistent launches over a work list of (halo, row tile,
+// partner chunk) items sorted by decreasing cost; each item sums m_j / r_ij
+// for its rows over its partners j > i.  Two forms share the schedule:
 //   * FP64: relative positions, 1/r from the double reciprocal square root;
 //   * FP32-compensated: positions relative to the halo centre split into
-//     hi = float(r) and lo = float(r - hi) (float4 tiles in shared memory);
-//     a pair separation is (hi_j - hi_i) + (lo_j - lo_i) in FP32, 1/r from
-//     rsqrtf, partial sums Kahan-compensated in FP32 and folded into FP64 per
-//     item.
-// Per-item partials are reduced per halo in item order (deterministic).
+//     hi = float(r) and lo = float(r - hi) (packed pairs in shared memory);
+//     a pair separation is (hi_j - hi_i) + (lo_j - lo_i) in FP32 (packed
+//     f32x2 arithmetic), 1/r from the approximate reciprocal square root,
+//     partial sums Kahan-compensated in FP32 and folded into FP64 per item.
+// Per-item partials are reduced per halo in item order (deterministic); the
+// launch sequence is captured once as a CUDA graph and replayed.  The
+// allocation-free entry point at the end of the file keeps the single-block
+// moment kernel and one 256-row list.
 #include <cuda_runtime.h>
 #include <cfloat>
 #include <climits>
