@@ -237,8 +237,10 @@ struct WarpList {
 // settled by particle index, so one that does not precede the last entry
 // lands at position nv and drops out.  Particle indices are only read for
 // such ties.
+template <int C>
 __device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int32_t leaf, int64_t self, double qx,
                                             double qy, double qz, int lane, unsigned& nvis, unsigned& nins) {
+  const int nvv = C ? C : A.nv;
   ++nvis;
   const int32_t p = leaf * kLeaf + lane;
   const bool v = ((int64_t)p < A.n) && ((int64_t)p != self);
@@ -250,8 +252,8 @@ __device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int32
     const int src = __ffs(mask) - 1;
     const double cd = __shfl_sync(0xffffffffu, d, src);
     const int32_t cs = leaf * kLeaf + src;
-    bool prec = (lane < A.nv) && (L.ld < cd);
-    const bool tie = (lane < A.nv) && (L.ld == cd);
+    bool prec = (lane < nvv) && (L.ld < cd);
+    const bool tie = (lane < nvv) && (L.ld == cd);
     if (__any_sync(0xffffffffu, tie)) {
       const int32_t co = A.orig[cs];
       if (tie) prec = A.orig[L.ls] < co;
@@ -261,8 +263,8 @@ __device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int32
     const int32_t us = __shfl_up_sync(0xffffffffu, L.ls, 1);
     if (lane > pos) { L.ld = ud; L.ls = us; }
     if (lane == pos) { L.ld = cd; L.ls = cs; }
-    if (lane >= A.nv) { L.ld = CUDART_INF; L.ls = -1; }
-    L.r2 = __shfl_sync(0xffffffffu, L.ld, A.nv - 1);
+    if (lane >= nvv) { L.ld = CUDART_INF; L.ls = -1; }
+    L.r2 = __shfl_sync(0xffffffffu, L.ld, nvv - 1);
     mask &= ~(1u << src);
     mask &= __ballot_sync(0xffffffffu, d <= L.r2);
   }
@@ -290,8 +292,10 @@ __device__ __forceinline__ void seed_candidate(const KnnArgs& A, int64_t jl, int
 // network (two per lane, element 2*lane + slot), write the element numbers of
 // the first 32 in order to list[0..31], and return the nv-th smallest
 // distance (+inf when fewer than nv exist) to every lane.
+template <int C>
 __device__ __forceinline__ double seed_sort(const KnnArgs& A, int64_t jl, int64_t jn, int64_t self, double qx,
                                            double qy, double qz, int lane, unsigned char* list) {
+  const int nvv = C ? C : A.nv;
   double d0, d1;
   int32_t o0, o1, s0 = lane, s1 = 32 + lane;
   seed_candidate(A, jl, jn, self, qx, qy, qz, lane, d0, o0);
@@ -324,17 +328,76 @@ __device__ __forceinline__ double seed_sort(const KnnArgs& A, int64_t jl, int64_
     list[2 * lane] = (unsigned char)s0;
     list[2 * lane + 1] = (unsigned char)s1;
   }
-  const int e = A.nv - 1;
+  const int e = nvv - 1;
   const double a = __shfl_sync(0xffffffffu, d0, e >> 1), b = __shfl_sync(0xffffffffu, d1, e >> 1);
   return (e & 1) ? b : a;
+}
+
+// The same sort on distances alone: a squared distance is non-negative, so
+// its bit pattern orders like its value and one 64-bit key stands for the
+// (distance, index) pair whenever no two finite distances among the 64 are
+// equal.  Returns false (list untouched) when such an exact tie exists; the
+// caller then sorts with the particle indices (seed_sort).  Empty candidates
+// (+inf) may tie among themselves: they are never list entries.
+__device__ __forceinline__ unsigned long long seed_key(const KnnArgs& A, int64_t jl, int64_t jn, int64_t self,
+                                                       double qx, double qy, double qz, int e) {
+  const int64_t p = (e < 32) ? jl * kLeaf + e : jn * kLeaf + (e - 32);
+  double d = CUDART_INF;
+  if ((e < 32 || (jn >= 0 && jn != jl)) && p < A.n && p != self)
+    d = pdist2(qx, qy, qz, A.x[p], A.y[p], A.z[p], A.Lx, A.Ly, A.Lz);
+  return (unsigned long long)__double_as_longlong(d);
+}
+
+template <int C>
+__device__ __forceinline__ bool seed_sort_keys(const KnnArgs& A, int64_t jl, int64_t jn, int64_t self, double qx,
+                                               double qy, double qz, int lane, unsigned char* list, double& kth) {
+  const int nvv = C ? C : A.nv;
+  const unsigned long long kInf = 0x7FF0000000000000ull;
+  unsigned long long k0 = seed_key(A, jl, jn, self, qx, qy, qz, lane);
+  unsigned long long k1 = seed_key(A, jl, jn, self, qx, qy, qz, 32 + lane);
+  int32_t s0 = lane, s1 = 32 + lane;
+#pragma unroll
+  for (int size = 2; size <= 64; size <<= 1) {
+    const bool asc = ((2 * lane) & size) == 0;
+#pragma unroll
+    for (int stride = size >> 1; stride >= 1; stride >>= 1) {
+      if (stride == 1) {
+        if (asc ? (k1 < k0) : (k0 < k1)) {
+          const unsigned long long tk = k0; k0 = k1; k1 = tk;
+          const int32_t ts = s0; s0 = s1; s1 = ts;
+        }
+      } else {
+        const int ls = stride >> 1;
+        const unsigned long long pk0 = __shfl_xor_sync(0xffffffffu, k0, ls), pk1 = __shfl_xor_sync(0xffffffffu, k1, ls);
+        const int32_t ps0 = __shfl_xor_sync(0xffffffffu, s0, ls), ps1 = __shfl_xor_sync(0xffffffffu, s1, ls);
+        const bool kmin = (((lane & ls) == 0) == asc);
+        if (kmin ? (pk0 < k0) : (k0 < pk0)) { k0 = pk0; s0 = ps0; }
+        if (kmin ? (pk1 < k1) : (k1 < pk1)) { k1 = pk1; s1 = ps1; }
+      }
+    }
+  }
+  // sorted element 2*lane + slot: look for equal finite neighbours
+  const unsigned long long nx = __shfl_down_sync(0xffffffffu, k0, 1);
+  const bool tie = (k0 == k1 && k0 != kInf) || (lane < 31 && k1 == nx && k1 != kInf);
+  if (__any_sync(0xffffffffu, tie)) return false;
+  if (lane < 16) {
+    list[2 * lane] = (unsigned char)s0;
+    list[2 * lane + 1] = (unsigned char)s1;
+  }
+  const int e = nvv - 1;
+  const unsigned long long a = __shfl_sync(0xffffffffu, k0, e >> 1), b = __shfl_sync(0xffffffffu, k1, e >> 1);
+  kth = __longlong_as_double((long long)((e & 1) ? b : a));
+  return true;
 }
 
 // A query's first list: the nv smallest (distance, index) pairs of its 64
 // seed candidates, rebuilt from the order seed_sort recorded (one distance
 // per lane, the same expression, so the same bits).
+template <int C>
 __device__ __forceinline__ void seed_list(const KnnArgs& A, WarpList& L, int64_t jl, int64_t jn, int64_t self,
                                           double qx, double qy, double qz, int lane, const unsigned char* list,
                                           unsigned& nvis) {
+  const int nvv = C ? C : A.nv;
   const int e = list[lane];
   double d;
   int32_t o;
@@ -342,14 +405,15 @@ __device__ __forceinline__ void seed_list(const KnnArgs& A, WarpList& L, int64_t
   const int64_t p = (e < 32) ? jl * kLeaf + e : jn * kLeaf + (e - 32);
   L.ld = d;
   L.ls = (d < CUDART_INF) ? (int32_t)p : -1;
-  if (lane >= A.nv) { L.ld = CUDART_INF; L.ls = -1; }
-  L.r2 = __shfl_sync(0xffffffffu, L.ld, A.nv - 1);
+  if (lane >= nvv) { L.ld = CUDART_INF; L.ls = -1; }
+  L.r2 = __shfl_sync(0xffffffffu, L.ld, nvv - 1);
   nvis += (jn >= 0 && jn != jl) ? 2 : 1;
 }
 
 // Per-query depth-first traversal from the root, nearest child first (used
 // when a query leaf's candidate list overflows).  Leaves skip0/skip1 were
 // already scanned.
+template <int C>
 __device__ void query_dfs(const KnnArgs& A, WarpList& L, int64_t s, double qx, double qy, double qz, int lane,
                           int32_t* s_node, double* s_bd, int64_t skip0, int64_t skip1, unsigned& nvis, unsigned& nins) {
   const int top = A.nlev - 1;
@@ -367,7 +431,7 @@ __device__ void query_dfs(const KnnArgs& A, WarpList& L, int64_t s, double qx, d
     const int64_t j = ent & ((1 << 27) - 1);
     if (lvl == 0) {
       if (j == skip0 || j == skip1) continue;
-      leaf_insert(A, L, j, s, qx, qy, qz, lane, nvis, nins);
+      leaf_insert<C>(A, L, j, s, qx, qy, qz, lane, nvis, nins);
       continue;
     }
     const int64_t c = j * kFan + lane;
@@ -408,8 +472,9 @@ __device__ void query_dfs(const KnnArgs& A, WarpList& L, int64_t s, double qx, d
 
 // SPH density (f90:2816-2838) in the exact evaluation order, and the stored
 // neighbour slots.
+template <int C>
 __device__ __forceinline__ void finish_query(const KnnArgs& A, const WarpList& L, int64_t s, int lane) {
-  const int nv = A.nv;
+  const int nv = C ? C : A.nv;
   const double dlast = __shfl_sync(0xffffffffu, L.ld, nv - 1);
   const double r = xmul(xsqrt(dlast), 0.5);
   const double r3 = xmul(xmul(r, r), r);
@@ -448,6 +513,7 @@ constexpr int kMaxCandSpill = 4096;  // ... in the warp's global spill buffer (e
 //     distance and stopping at the first whose box-to-box distance exceeds it.
 // The candidate leaves are shared by the 32 queries, so the traversal is
 // paid once per leaf and the leaf data mostly comes from L1.
+template <int C>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArgs A) {
   __shared__ int32_t s_node[kWarpsPerBlock][kStack];
   __shared__ double s_bd[kWarpsPerBlock][kStack];
@@ -472,7 +538,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
     bool ok = true;
     for (int q = 0; q < nq; ++q) {
       const int64_t s = s0 + q;
-      const double kth = seed_sort(A, jl, jn, s, A.x[s], A.y[s], A.z[s], lane, s_list[wib][q]);
+      const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
+      double kth;
+      if (!seed_sort_keys<C>(A, jl, jn, s, qx, qy, qz, lane, s_list[wib][q], kth))
+        kth = seed_sort<C>(A, jl, jn, s, qx, qy, qz, lane, s_list[wib][q]);
       if (!(kth < CUDART_INF)) ok = false;  // fewer than nv others in the two leaves
       if (lane == q) Rq = kth;
     }
@@ -569,10 +638,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
       const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
       WarpList L;
       const long long tq0 = clock64();
-      seed_list(A, L, jl, jn, s, qx, qy, qz, lane, s_list[wib][q], nvis);
+      seed_list<C>(A, L, jl, jn, s, qx, qy, qz, lane, s_list[wib][q], nvis);
       const long long tq1 = clock64();
       if (overflow) {
-        query_dfs(A, L, s, qx, qy, qz, lane, s_node[wib], s_bd[wib], jl, jn, nvis, nins);
+        query_dfs<C>(A, L, s, qx, qy, qz, lane, s_node[wib], s_bd[wib], jl, jn, nvis, nins);
       } else {
         for (int c0 = 0; c0 < ncand; c0 += 32) {
           // every query lies in this leaf's box, so a candidate whose box is at
@@ -592,7 +661,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
             mask &= mask - 1;
             const double sbd = __shfl_sync(0xffffffffu, bd, src);
             const int32_t sl = __shfl_sync(0xffffffffu, leaf, src);
-            if (sbd < L.r2) leaf_insert(A, L, sl, s, qx, qy, qz, lane, nvis, nins);
+            if (sbd < L.r2) leaf_insert<C>(A, L, sl, s, qx, qy, qz, lane, nvis, nins);
           }
         }
       }
@@ -609,7 +678,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
         }
       }
       const long long tq3 = clock64();
-      finish_query(A, L, s, lane);
+      finish_query<C>(A, L, s, lane);
       __syncwarp();
       c_fin += clock64() - tq3;
     }
@@ -662,8 +731,12 @@ int stage_knn_density(Engine& E) {
   A.kdebug = E.task_profile ? 1 : 0;
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, E.device);
+  // the default nvoisins = 32 (one list entry per lane) has its own build with
+  // the count fixed at compile time
+  const bool nv32 = P.nvoisins == 32;
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, knn_leaf_kernel, kWarpsPerBlock * 32, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, nv32 ? (const void*)knn_leaf_kernel<32> : (const void*)knn_leaf_kernel<0>, kWarpsPerBlock * 32, 0);
   if (per_sm < 1) per_sm = 1;
   int64_t want = (E.lev_cnt[0] + kWarpsPerBlock - 1) / kWarpsPerBlock;
   int64_t grid = (int64_t)nsm * per_sm * 2;
@@ -672,7 +745,8 @@ int stage_knn_density(Engine& E) {
   A.kspill = E.d_kspill.as<unsigned>();
   E.launches++;
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[9], E.stream));
-  knn_leaf_kernel<<<(unsigned)grid, kWarpsPerBlock * 32, 0, E.stream>>>(A);
+  if (nv32) knn_leaf_kernel<32><<<(unsigned)grid, kWarpsPerBlock * 32, 0, E.stream>>>(A);
+  else knn_leaf_kernel<0><<<(unsigned)grid, kWarpsPerBlock * 32, 0, E.stream>>>(A);
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[10], E.stream));
   AHOP_CUDA_TRY(cudaGetLastError());
   int herr = 0;
