@@ -292,7 +292,7 @@ int ahop_get_timings(AhopTimings* t) {
 
 static void release_device(Engine& E) {
   DevBuf* bufs[] = {&E.d_pos_in, &E.d_mass_in, &E.d_key, &E.d_key2, &E.d_idx, &E.d_idx2, &E.d_x, &E.d_y,
-                    &E.d_z, &E.d_m, &E.d_orig, &E.d_rank, &E.d_box, &E.d_cub, &E.d_nei, &E.d_dens,
+                    &E.d_z, &E.d_m, &E.d_orig, &E.d_rank, &E.d_box, &E.d_box32, &E.d_cub, &E.d_nei, &E.d_dens,
                     &E.d_hop, &E.d_root, &E.d_group, &E.d_peakflag, &E.d_densg, &E.d_gpeak, &E.d_goff,
                     &E.d_gmem, &E.d_gmem_rho, &E.d_gmem_rho_pref, &E.d_sad_key, &E.d_sad_key2, &E.d_sad_val,
                     &E.d_sad_val2, &E.d_sad_cnt, &E.d_sad_keep, &E.d_sad_kpos, &E.d_flags, &E.d_soff,

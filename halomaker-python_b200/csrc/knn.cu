@@ -14,6 +14,7 @@
 // density use the reference's exact expression order in explicitly rounded
 // FP64 (no FMA), so the density matches the reference bit for bit whenever the
 // neighbour order does.
+#include <algorithm>
 #include <cub/cub.cuh>
 #include <cfloat>
 #include <climits>
@@ -209,6 +210,7 @@ struct KnnArgs {
   int* err;     // error flag (stack overflow)
   unsigned long long* kstats;  // [0] query leaves [1] candidate leaves [2] leaf visits [3] insertions [4] overflows
   unsigned* kspill;             // per-warp candidate spill buffers [grid warps][2 * kMaxCandSpill], or null
+  const float4* box32;          // leaf boxes in FP32, widened (leaf_box32_kernel)
   int kdebug;   // extra counters: [5] leaves within the final radius, [6]/[7] cycles of overflow/other leaves,
                 // [24..28] phase cycles of the other leaves (bound, candidates + sort, seed lists, scan, density)
 };
@@ -399,9 +401,7 @@ __device__ __forceinline__ void seed_list(const KnnArgs& A, WarpList& L, int64_t
                                           unsigned& nvis) {
   const int nvv = C ? C : A.nv;
   const int e = list[lane];
-  double d;
-  int32_t o;
-  seed_candidate(A, jl, jn, self, qx, qy, qz, e, d, o);
+  const double d = __longlong_as_double((long long)seed_key(A, jl, jn, self, qx, qy, qz, e));
   const int64_t p = (e < 32) ? jl * kLeaf + e : jn * kLeaf + (e - 32);
   L.ld = d;
   L.ls = (d < CUDART_INF) ? (int32_t)p : -1;
@@ -490,6 +490,37 @@ __device__ __forceinline__ void finish_query(const KnnArgs& A, const WarpList& L
   if (lane < A.nstore) A.nei[s * A.nstore + lane] = L.ls;
 }
 
+// Leaf boxes in FP32 for the per-query candidate test: centre rounded to
+// float, half width widened to cover that rounding plus every rounding of the
+// FP32 test below (2^-21 L), so the FP32 distance is never above the exact
+// point-to-box distance: a pruning bound, looser by a negligible margin.
+__global__ void leaf_box32_kernel(const double* __restrict__ box, int64_t nleaf, double Lmax,
+                                  float4* __restrict__ out) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= nleaf) return;
+  const double* b = box + 6 * j;
+  const double pad = Lmax * 0x1p-21;
+  float c[3], w[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    c[k] = (float)b[k];
+    w[k] = __double2float_ru(b[3 + k] + fabs(b[k] - (double)c[k]) + pad);
+  }
+  out[2 * j] = make_float4(c[0], c[1], c[2], 0.f);
+  out[2 * j + 1] = make_float4(w[0], w[1], w[2], 0.f);
+}
+
+// Lower bound of the squared periodic distance from (qx, qy, qz) (as floats)
+// to a leaf's FP32 box, rounded down at every step.
+__device__ __forceinline__ float box_dist2_lb(const float4* __restrict__ b, float qx, float qy, float qz, float Lx,
+                                              float Ly, float Lz) {
+  const float4 c = b[0], w = b[1];
+  float dx = fabsf(c.x - qx); dx = fminf(dx, Lx - dx); dx = fmaxf(0.f, __fsub_rd(dx, w.x));
+  float dy = fabsf(c.y - qy); dy = fminf(dy, Ly - dy); dy = fmaxf(0.f, __fsub_rd(dy, w.y));
+  float dz = fabsf(c.z - qz); dz = fminf(dz, Lz - dz); dz = fmaxf(0.f, __fsub_rd(dz, w.z));
+  return __fadd_rd(__fadd_rd(__fmul_rd(dx, dx), __fmul_rd(dy, dy)), __fmul_rd(dz, dz));
+}
+
 // Periodic squared distance between two padded boxes (centre, half width).
 __device__ __forceinline__ double boxbox_dist2(const double* __restrict__ a, const double* __restrict__ b,
                                                double Lx, double Ly, double Lz) {
@@ -524,6 +555,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
   const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
   const int64_t nleaf = A.lev_cnt[0];
   const int top = A.nlev - 1;
+  const float Lxf = (float)A.Lx, Lyf = (float)A.Ly, Lzf = (float)A.Lz;
   // candidate sort keys; s_bd is only used by the per-query fallback, which
   // runs exactly when there is no candidate list
   unsigned* s_key = reinterpret_cast<unsigned*>(s_bd[wib]);
@@ -636,6 +668,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
     for (int q = 0; q < nq; ++q) {
       const int64_t s = s0 + q;
       const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
+      const float qxf = (float)qx, qyf = (float)qy, qzf = (float)qz;
       WarpList L;
       const long long tq0 = clock64();
       seed_list<C>(A, L, jl, jn, s, qx, qy, qz, lane, s_list[wib][q], nvis);
@@ -653,7 +686,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
           double bd = CUDART_INF;
           if (ci < ncand) {
             leaf = cb[kb[ci] & 4095u];
-            if (leaf != jl && leaf != jn) bd = box_dist2(A.box + 6 * (int64_t)leaf, qx, qy, qz, A.Lx, A.Ly, A.Lz);
+            if (leaf != jl && leaf != jn)
+              bd = (double)box_dist2_lb(A.box32 + 2 * (int64_t)leaf, qxf, qyf, qzf, Lxf, Lyf, Lzf);
           }
           unsigned mask = __ballot_sync(0xffffffffu, bd < L.r2);
           while (mask) {
@@ -716,6 +750,12 @@ int stage_knn_density(Engine& E) {
   A.x = E.d_x.as<double>(); A.y = E.d_y.as<double>(); A.z = E.d_z.as<double>(); A.m = E.d_m.as<double>();
   A.orig = E.d_orig.as<int32_t>();
   A.box = E.d_box.as<double>();
+  AHOP_CUDA_TRY(E.d_box32.ensure((size_t)E.lev_cnt[0] * 32 + 32));
+  A.box32 = E.d_box32.as<float4>();
+  E.launches++;
+  leaf_box32_kernel<<<(unsigned)((E.lev_cnt[0] + 255) / 256), 256, 0, E.stream>>>(
+      A.box, E.lev_cnt[0], std::max(P.xlong, std::max(P.ylong, P.zlong)), E.d_box32.as<float4>());
+  AHOP_CUDA_TRY(cudaGetLastError());
   for (int l = 0; l < kMaxLevels; ++l) { A.lev_off[l] = E.lev_off[l]; A.lev_cnt[l] = E.lev_cnt[l]; }
   A.nlev = E.nlev;
   A.n = n;
