@@ -111,7 +111,7 @@ struct Engine {
   DevBuf d_orig;                         // orig index (0-based) per sorted slot
   DevBuf d_rank;                         // sorted slot per orig index
   DevBuf d_box;                          // AABBs of all levels (6 doubles each)
-  DevBuf d_box32;                        // leaf AABBs in FP32, widened (2 float4 each)
+  DevBuf d_box32;                        // AABBs of all levels in FP32, widened (2 float4 each)
   int32_t nlev = 0;
   int64_t lev_off[kMaxLevels + 1] = {};
   int64_t lev_cnt[kMaxLevels] = {};

@@ -210,7 +210,7 @@ struct KnnArgs {
   int* err;     // error flag (stack overflow)
   unsigned long long* kstats;  // [0] query leaves [1] candidate leaves [2] leaf visits [3] insertions [4] overflows
   unsigned* kspill;             // per-warp candidate spill buffers [grid warps][2 * kMaxCandSpill], or null
-  const float4* box32;          // leaf boxes in FP32, widened (leaf_box32_kernel)
+  const float4* box32;          // boxes of every level in FP32, widened (leaf_box32_kernel)
   int kdebug;   // extra counters: [5] leaves within the final radius, [6]/[7] cycles of overflow/other leaves,
                 // [24..28] phase cycles of the other leaves (bound, candidates + sort, seed lists, scan, density)
 };
@@ -490,7 +490,7 @@ __device__ __forceinline__ void finish_query(const KnnArgs& A, const WarpList& L
   if (lane < A.nstore) A.nei[s * A.nstore + lane] = L.ls;
 }
 
-// Leaf boxes in FP32 for the per-query candidate test: centre rounded to
+// Boxes in FP32 for the candidate tests: centre rounded to
 // float, half width widened to cover that rounding plus every rounding of the
 // FP32 test below (2^-21 L), so the FP32 distance is never above the exact
 // point-to-box distance: a pruning bound, looser by a negligible margin.
@@ -522,6 +522,16 @@ __device__ __forceinline__ float box_dist2_lb(const float4* __restrict__ b, floa
 }
 
 // Periodic squared distance between two padded boxes (centre, half width).
+// Lower bound of the squared periodic distance between two widened FP32 boxes.
+__device__ __forceinline__ float boxbox_dist2_lb(const float4* __restrict__ a, const float4* __restrict__ b,
+                                                 float Lx, float Ly, float Lz) {
+  const float4 ca = a[0], wa = a[1], cb = b[0], wb = b[1];
+  float dx = fabsf(ca.x - cb.x); dx = fminf(dx, Lx - dx); dx = fmaxf(0.f, __fsub_rd(__fsub_rd(dx, wa.x), wb.x));
+  float dy = fabsf(ca.y - cb.y); dy = fminf(dy, Ly - dy); dy = fmaxf(0.f, __fsub_rd(__fsub_rd(dy, wa.y), wb.y));
+  float dz = fabsf(ca.z - cb.z); dz = fminf(dz, Lz - dz); dz = fmaxf(0.f, __fsub_rd(__fsub_rd(dz, wa.z), wb.z));
+  return __fadd_rd(__fadd_rd(__fmul_rd(dx, dx), __fmul_rd(dy, dy)), __fmul_rd(dz, dz));
+}
+
 __device__ __forceinline__ double boxbox_dist2(const double* __restrict__ a, const double* __restrict__ b,
                                                double Lx, double Ly, double Lz) {
   double dx = fabs(a[0] - b[0]); dx = fmin(dx, Lx - dx); dx = fmax(0.0, dx - a[3] - b[3]);
@@ -585,7 +595,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
     const long long t_a = clock64();
     // ---- B: candidate leaves within R of this leaf's box; the list lives in
     // shared memory and moves to the warp's global spill buffer past kMaxCand
-    const double* myb = A.box + 6 * jl;
+    const float4* myb32 = A.box32 + 2 * jl;
     int ncand = 0;
     unsigned* kb = s_key;
     int32_t* cb = s_cand[wib];
@@ -608,7 +618,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
         bool cand = false;
         double bbd = CUDART_INF;
         if (valid) {
-          bbd = boxbox_dist2(myb, A.box + 6 * (A.lev_off[lvl - 1] + c), A.Lx, A.Ly, A.Lz);
+          bbd = (double)boxbox_dist2_lb(myb32, A.box32 + 2 * (A.lev_off[lvl - 1] + c), Lxf, Lyf, Lzf);
           cand = bbd <= lim;
         }
         const unsigned mask = __ballot_sync(0xffffffffu, cand);
@@ -750,11 +760,12 @@ int stage_knn_density(Engine& E) {
   A.x = E.d_x.as<double>(); A.y = E.d_y.as<double>(); A.z = E.d_z.as<double>(); A.m = E.d_m.as<double>();
   A.orig = E.d_orig.as<int32_t>();
   A.box = E.d_box.as<double>();
-  AHOP_CUDA_TRY(E.d_box32.ensure((size_t)E.lev_cnt[0] * 32 + 32));
+  const int64_t nbox = E.lev_off[E.nlev];  // boxes of every level
+  AHOP_CUDA_TRY(E.d_box32.ensure((size_t)nbox * 32 + 32));
   A.box32 = E.d_box32.as<float4>();
   E.launches++;
-  leaf_box32_kernel<<<(unsigned)((E.lev_cnt[0] + 255) / 256), 256, 0, E.stream>>>(
-      A.box, E.lev_cnt[0], std::max(P.xlong, std::max(P.ylong, P.zlong)), E.d_box32.as<float4>());
+  leaf_box32_kernel<<<(unsigned)((nbox + 255) / 256), 256, 0, E.stream>>>(
+      A.box, nbox, std::max(P.xlong, std::max(P.ylong, P.zlong)), E.d_box32.as<float4>());
   AHOP_CUDA_TRY(cudaGetLastError());
   for (int l = 0; l < kMaxLevels; ++l) { A.lev_off[l] = E.lev_off[l]; A.lev_cnt[l] = E.lev_cnt[l]; }
   A.nlev = E.nlev;
