@@ -542,6 +542,9 @@ __device__ __forceinline__ double boxbox_dist2(const double* __restrict__ a, con
 
 constexpr int kMaxCand = 512;        // candidate leaves per query leaf held in shared memory
 constexpr int kMaxCandSpill = 4096;  // ... in the warp's global spill buffer (else per-query DFS)
+// the candidate sort pads a list to the next power of two inside its buffer
+static_assert((kMaxCand & (kMaxCand - 1)) == 0 && (kMaxCandSpill & (kMaxCandSpill - 1)) == 0,
+              "candidate capacities must be powers of two");
 
 // One warp per query leaf (its 32 Morton-consecutive particles).
 //  A. every query sorts the 64 particles of its own and the adjacent leaf
