@@ -58,8 +58,8 @@ def _file(path, version):
     nstar = int(R.read(np.int32)[0])
     R.skip(2)
     nsink = int(R.read(np.int32)[0])
-    pos = np.stack([R.read(np.float64) for _ in range(ndim)], 1) if npart else np.zeros((0, ndim))
-    vel = np.stack([R.read(np.float64) for _ in range(ndim)], 1) if npart else np.zeros((0, ndim))
+    pos = np.stack([R.read(np.float64) for _ in range(ndim)], 1)
+    vel = np.stack([R.read(np.float64) for _ in range(ndim)], 1)
     mass = R.read(np.float64)
     idp = R.read(np.int32)
     R.skip(1)

@@ -106,3 +106,18 @@ def test_snapshot_from_files_matches_host_arrays(tmp_path):
     assert a["nselected"] == int(g["nselected"])
     assert np.array_equal(a["ids"], b["ids"]) and np.array_equal(a["offsets"], b["offsets"])
     assert np.array_equal(a["props"], b["props"], equal_nan=True)
+
+
+def test_decoder_reads_an_empty_file(tmp_path):
+    """A cpu file without particles: no payload copies, no scatter launch; the
+    rows equal the restatement's."""
+    from ahop_b200 import ramses
+    P = ramses_files.make_particles(44, 4, 500, 120, 30)
+    n = len(P["mass"])
+    paths = ramses_files.write_arrays(str(tmp_path), P, 4, [0, 0, n // 2, n])
+    for fam in ("all", "dm", "star"):
+        r = ramses.read_parts(paths, 4, fam, 2.0, 3.0)
+        o = ramses_oracle.read_parts(paths, 4, fam, 2.0, 3.0)
+        assert r["nselected"] == o["nselected"]
+        for k in ("pos", "vel", "mass"):
+            assert np.array_equal(r[k].cpu().numpy(), o[k]), (fam, k)

@@ -54,3 +54,18 @@ def ramses_oracle_repeat_id(path):
     pos = np.flatnonzero(ids > 0)[:2]
     ids[pos[1]] = ids[pos[0]]
     R.buf.tofile(path)
+
+
+def test_oracle_reads_an_empty_file(tmp_path):
+    """A cpu file without particles (npart = 0, empty records) contributes nothing."""
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import ramses_files
+    P = ramses_files.make_particles(44, 4, 500, 120, 30)
+    n = len(P["mass"])
+    paths = ramses_files.write_arrays(str(tmp_path), P, 4, [0, 0, n // 2, n])
+    r = ramses_oracle.read_parts(paths, 4, "all")
+    full = ramses_oracle.read_parts(ramses_files.write_arrays(str(tmp_path / "one"), P, 4, [0, n]), 4, "all")
+    assert r["nselected"] == 620
+    for k in ("pos", "vel", "mass"):
+        assert np.array_equal(r[k], full[k])
