@@ -51,3 +51,46 @@ def test_dropin_module_surface():
         assert callable(getattr(neikdtree, name))
     for name in ("liste_parts", "density", "nnodes", "real_table", "integer_table"):
         assert hasattr(neikdtree, name)
+
+
+STRUCTS = {
+    "AhopInit": ("ahop_b200._lib", "AhopInit"),
+    "AhopOthers": ("ahop_b200._lib", "AhopOthers"),
+    "AhopOutputs": ("ahop_b200._lib", "AhopOutputs"),
+    "AhopTimings": ("ahop_b200._lib", "AhopTimings"),
+    "AhopStructs": ("ahop_b200.msm", "AhopStructs"),
+    "AhopRamsesParams": ("ahop_b200.ramses", "AhopRamsesParams"),
+    "AhopRamsesCounts": ("ahop_b200.ramses", "AhopRamsesCounts"),
+    "AhopHaloParams": ("ahop_b200.halo_props", "AhopHaloParams"),
+    "AhopHaloTimings": ("ahop_b200.halo_props", "AhopHaloTimings"),
+    "AhopVirialParams": ("ahop_b200.halo_props", "AhopVirialParams"),
+    "AhopAdjParams": ("ahop_b200.autograd", "AhopAdjParams"),
+}
+
+
+def test_python_structs_match_the_header(tmp_path):
+    """Every ctypes mirror has the C struct's size and field offsets (a C
+    program compiled against include/ahop_b200.h prints them)."""
+    import importlib
+    mirrors = {k: getattr(importlib.import_module(m), c) for k, (m, c) in STRUCTS.items()}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "ahop_b200.h"', "int main(void) {"]
+    for name, cls in mirrors.items():
+        lines.append(f'  printf("{name} size %zu\\n", sizeof({name}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("{name} {fname} %zu\\n", offsetof({name}, {fname}));')
+    lines.append("  return 0;\n}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(REPO, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    seen = 0
+    for line in out:
+        if not line:
+            continue
+        name, what, val = line.split()
+        cls = mirrors[name]
+        got = ctypes.sizeof(cls) if what == "size" else getattr(cls, what).offset
+        assert got == int(val), f"{name}.{what}: ctypes {got}, C {val}"
+        seen += 1
+    assert seen == sum(1 + len(c._fields_) for c in mirrors.values())
