@@ -54,7 +54,7 @@ __host__ __device__ constexpr int ipt_for(int nt) { return nt >= 1024 ? 2 : kIPT
 // groups whose union-find parents a task block keeps in shared memory
 __host__ __device__ constexpr int par_cap(int nt) { return nt >= 1024 ? 32768 : 1024; }
 constexpr int kBigGroup = 96;   // groups larger than this are summed by a warp
-constexpr int kRowWarp = 32;    // saddle-row prefixes longer than this are linked by a warp
+constexpr int kRowWarp = 8;     // saddle-row prefixes longer than this are linked by a warp
 constexpr int kMaxBigRows = 512;
 constexpr long long kMaxTaskLevels = 4000000LL;  // cap on one task's threshold levels (error, never a hang)
 
