@@ -1110,7 +1110,7 @@ static int halo_run(HaloEngine& H, const AhopHaloParams* p, const int64_t* d_off
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   AHOP_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
   if (cs != cudaStreamCaptureStatusNone) {
-    set_error("the stream is being captured; use ahop_halo_props_noalloc inside a stream capture");
+    set_error("the stream is being captured; this entry point synchronises with the host and cannot run inside a stream capture");
     return AHOP_EINVAL;
   }
   if (!H.ready) {
