@@ -206,6 +206,7 @@ int ahop_compute_adaptahop_device(const double* d_pos, const double* d_mass, int
   E.n = npart;
   E.stream = static_cast<cudaStream_t>(stream);
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[0], E.stream));
+  E.mass_pending = false;  // the caller's device inputs are ready on its stream
   if ((rc = run_pipeline(E, d_pos, d_mass))) return rc;
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[8], E.stream));
   AHOP_CUDA_TRY(cudaStreamSynchronize(E.stream));
@@ -227,9 +228,21 @@ int ahop_compute_adaptahop(const double* pos_in, const double* mass_in, int64_t 
   AHOP_CUDA_TRY(E.d_pos_in.ensure(npart * 24));
   AHOP_CUDA_TRY(E.d_mass_in.ensure(npart * 8));
   AHOP_CUDA_TRY(E.h_dens.ensure(npart * 8));
+  if (!E.stream_copy) {
+    AHOP_CUDA_TRY(cudaStreamCreateWithFlags(&E.stream_copy, cudaStreamNonBlocking));
+    AHOP_CUDA_TRY(cudaEventCreateWithFlags(&E.ev_dens, cudaEventDisableTiming));
+    AHOP_CUDA_TRY(cudaEventCreateWithFlags(&E.ev_copied, cudaEventDisableTiming));
+  }
+  if (!E.ev_mass) AHOP_CUDA_TRY(cudaEventCreateWithFlags(&E.ev_mass, cudaEventDisableTiming));
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[0], st));
+  // positions first on the compute stream (the Morton keys and the sort need
+  // only them); the masses go up on the copy stream meanwhile and are waited
+  // for just before the sorted gather
+  AHOP_CUDA_TRY(cudaStreamWaitEvent(E.stream_copy, E.ev[0], 0));
   AHOP_CUDA_TRY(cudaMemcpyAsync(E.d_pos_in.p, pos_in, npart * 24, cudaMemcpyHostToDevice, st));
-  AHOP_CUDA_TRY(cudaMemcpyAsync(E.d_mass_in.p, mass_in, npart * 8, cudaMemcpyHostToDevice, st));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(E.d_mass_in.p, mass_in, npart * 8, cudaMemcpyHostToDevice, E.stream_copy));
+  AHOP_CUDA_TRY(cudaEventRecord(E.ev_mass, E.stream_copy));
+  E.mass_pending = true;
   // the density goes back to the host on a copy stream during the later stages
   if ((rc = run_pipeline(E, E.d_pos_in.as<double>(), E.d_mass_in.as<double>(), 99, E.h_dens.as<double>())))
     return rc;
@@ -342,6 +355,7 @@ int ahop_debug_compute_stages(const double* pos_in, const double* mass_in, int64
   AHOP_CUDA_TRY(E.d_mass_in.ensure(npart * 8));
   AHOP_CUDA_TRY(cudaMemcpyAsync(E.d_pos_in.p, pos_in, npart * 24, cudaMemcpyHostToDevice, E.stream));
   AHOP_CUDA_TRY(cudaMemcpyAsync(E.d_mass_in.p, mass_in, npart * 8, cudaMemcpyHostToDevice, E.stream));
+  E.mass_pending = false;  // both inputs on the compute stream here
   rc = run_pipeline(E, E.d_pos_in.as<double>(), E.d_mass_in.as<double>(), last_stage);
   if (rc) return rc;
   AHOP_CUDA_TRY(cudaStreamSynchronize(E.stream));

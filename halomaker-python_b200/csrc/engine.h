@@ -85,6 +85,8 @@ struct Engine {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaStream_t stream_copy = nullptr;   // host path: density copy-out during the later stages
   cudaEvent_t ev_dens = nullptr, ev_copied = nullptr;
+  cudaEvent_t ev_mass = nullptr;        // host path: masses uploaded on the copy stream
+  bool mass_pending = false;            // ... and not yet waited for by the compute stream
   cudaEvent_t wave_ev[4] = {};          // per-wave timing (task profile only)
   float wave_prof[4 * 64] = {};         // per wave: small tasks, ms, large tasks, ms
   int32_t nwave_prof = 0;

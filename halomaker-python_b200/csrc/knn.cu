@@ -153,6 +153,10 @@ int stage_sort_and_tree(Engine& E, const double* d_pos, const double* d_mass) {
                                                 E.d_key2.as<unsigned long long>(), E.d_idx.as<int32_t>(),
                                                 E.d_idx2.as<int32_t>(), (int)n, 0, 63, st));
   E.launches++;
+  if (E.mass_pending) {  // host path: the masses were uploaded on the copy stream
+    AHOP_CUDA_TRY(cudaStreamWaitEvent(st, E.ev_mass, 0));
+    E.mass_pending = false;
+  }
   gather_sorted_kernel<<<grid, T, 0, st>>>(d_pos, d_mass, E.d_idx2.as<int32_t>(), n, E.d_x.as<double>(),
                                            E.d_y.as<double>(), E.d_z.as<double>(), E.d_m.as<double>(),
                                            E.d_orig.as<int32_t>(), E.d_rank.as<int32_t>());
