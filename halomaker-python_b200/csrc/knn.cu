@@ -253,6 +253,7 @@ __device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int32
   double d = CUDART_INF;
   if (v) d = pdist2(qx, qy, qz, A.x[p], A.y[p], A.z[p], A.Lx, A.Ly, A.Lz);
   unsigned mask = __ballot_sync(0xffffffffu, v && d <= L.r2);
+  if (!mask) return;
   while (mask) {
     ++nins;
     const int src = __ffs(mask) - 1;
@@ -270,10 +271,12 @@ __device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int32
     if (lane > pos) { L.ld = ud; L.ls = us; }
     if (lane == pos) { L.ld = cd; L.ls = cs; }
     if (lane >= nvv) { L.ld = CUDART_INF; L.ls = -1; }
-    L.r2 = __shfl_sync(0xffffffffu, L.ld, nvv - 1);
+    // the bound is refreshed once per leaf: a candidate that an earlier one
+    // of this leaf pushed beyond the list finds every entry ahead of it
+    // (pos = nv) and changes nothing
     mask &= ~(1u << src);
-    mask &= __ballot_sync(0xffffffffu, d <= L.r2);
   }
+  L.r2 = __shfl_sync(0xffffffffu, L.ld, nvv - 1);
 }
 
 __device__ __forceinline__ bool key_less(double da, int32_t oa, double db, int32_t ob) {
