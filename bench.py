@@ -14,10 +14,13 @@ fudgepsilon=1e-5, alphap=1, nmembthresh=20.
   roofline -- the fused kNN + density kernel (the dominant kernel) against the
             measured HBM copy bandwidth;
   cpu_baseline -- the CPU restatement of the reference finder (OpenMP, all host
-            cores) on a bounded sample: the 128^3 box from the same generator.
+            cores): one full pass over the same 256^3 box.
 
 --impl reference times that CPU restatement (the reference's own Fortran
-cannot be built: no Fortran compiler in the image) on the same sample.
+cannot be built: no Fortran compiler in the image) on the same 256^3 box, one
+full finder pass per timed step; its warm-up steps run the 64^3 box of the same
+generator (the CPU path has no caches or compiled code to warm beyond its
+thread pool, and a full pass takes tens of seconds).
 Multi-GPU: the finder does not shard (its structure tree needs a global
 merge), so --gpus N runs N independent replicas (weak scaling).
 """
@@ -40,7 +43,14 @@ FP32_OPS_PER_PAIR = 13.5  # FP32 operations per pair in the compensated pair ker
 METRIC = "Mpart/s end-to-end vs host CPU; halo Epot pairs/s FP32-comp vs FP64 at 1e-6"
 PARAMS = dict(nvoisins=32, nhop=16, rho_threshold=80.0, fudge=4.0, fudgepsilon=1e-5, alphap=1.0, nmembthresh=20)
 WORKLOAD = dict(name="c2_256cubed", npart=16_777_216, nhalo=19_200, seed=2, nmin=20, nmax=2_000_000)
-CPU_SAMPLE = dict(name="128cubed_same_generator", npart=2_097_152, nhalo=2_400, seed=2, nmax=250_000)
+WARM_SAMPLE = dict(name="64cubed_same_generator", npart=262_144, nhalo=300, seed=2, nmax=31_250)
+
+# ncu counters of knn_leaf_kernel (DRAM read + write bytes and warp
+# instructions, per particle) from the capture summarised in
+# profiles/knn_leaf_kernel_8m.md; the bench line scales them to the workload.
+# They are re-measured whenever the kernel changes.
+NCU_KNN = dict(profiled="knn_leaf_kernel, 8,000,000-particle clustered box, one launch",
+               dram_bytes_per_particle=257.998511, warp_instructions_per_particle=5985.22261175)
 
 
 def _gen(spec):
@@ -102,11 +112,19 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_sample_rate(nthreads=None):
-    """Oracle (CPU restatement, OpenMP) Mparticles/s on the bounded sample."""
+def workload_config(spec, world):
+    """The bench line's config; both arms print the same one."""
+    # change_pos_1310: epsilon = fudgepsilon * xlong / npart**(1/3)
+    eps = PARAMS["fudgepsilon"] * 1.0 / spec["npart"] ** (1.0 / 3.0)
+    return {"workload": spec["name"], "npart": spec["npart"], "nhalo": spec["nhalo"], "seed": spec["seed"],
+            "epsilon": eps, **PARAMS, "l2": f"inputs ({spec['npart'] * 32 / 1e6:.0f} MB) larger than L2",
+            "parallelism": f"replicas{world}"}
+
+
+def cpu_rate(ps, nthreads=None):
+    """Oracle (CPU restatement, OpenMP) Mparticles/s of one full finder pass."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
-    ps = _gen(CPU_SAMPLE)
     prm = oracle.default_params(ps.n, nthreads=nthreads or os.cpu_count(),
                                 **{k: PARAMS[k] for k in ("nvoisins", "nhop", "rho_threshold", "fudge", "alphap",
                                                           "nmembthresh")})
@@ -116,25 +134,41 @@ def cpu_sample_rate(nthreads=None):
     return ps.n / dt / 1e6, dt, prm["nthreads"], r
 
 
-def run_reference(args, rank):
+def run_reference(args, rank, world):
+    """The CPU path on the bench workload: K full passes over the 256^3 box,
+    after W warm-up passes over the 64^3 box of the same generator."""
     if rank != 0:
         return
-    rates = []
+    warm = _gen(WARM_SAMPLE)
+    for _ in range(args.warmup):
+        cpu_rate(warm)
+    del warm
+    spec = dict(WORKLOAD)
+    if args.npart:
+        spec = _scaled(spec, args.npart)
+    ps = _gen(spec)
+    secs = []
     nth = os.cpu_count()
-    for i in range(args.warmup + args.steps):
-        rate, dt, nth, _ = cpu_sample_rate()
-        if i >= args.warmup:
-            rates.append(rate)
-    v = statistics.mean(rates)
-    sample = (f"{CPU_SAMPLE['npart']} particles ({CPU_SAMPLE['name']}, {CPU_SAMPLE['nhalo']} halos, seed "
-              f"{CPU_SAMPLE['seed']}), full finder per step")
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mpart/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": CPU_SAMPLE["npart"] / v / 1e3,
+    for _ in range(args.steps):
+        _, dt, nth, _ = cpu_rate(ps)
+        secs.append(dt)
+    tot = sum(secs)
+    v = ps.n * len(secs) / tot / 1e6
+    sample = (f"{ps.n} particles ({spec['name']}, {spec['nhalo']} halos, seed {spec['seed']}): the full bench box, "
+              f"one full finder pass per timed step ({min(secs):.1f}-{max(secs):.1f} s); warm-up passes on "
+              f"{WARM_SAMPLE['npart']} particles ({WARM_SAMPLE['name']})")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mpart/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / len(secs) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD["name"], "sample": CPU_SAMPLE["name"], **PARAMS},
+            "config": workload_config(spec, world),
             "cpu_baseline": {"value": v, "unit": "Mpart/s", "cores": nth, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "Mpart/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def _scaled(spec, npart):
+    return dict(spec, npart=npart, nhalo=max(10, int(spec["nhalo"] * npart / spec["npart"])),
+                name=f"scaled_{npart}")
 
 
 def halo_section(args, torch, dist=None):
@@ -335,7 +369,7 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", 0))
 
     if args.impl == "reference":
-        run_reference(args, rank)
+        run_reference(args, rank, world)
         return
 
     import numpy as np
@@ -367,8 +401,7 @@ def main():
     build.build()
     spec = dict(WORKLOAD)
     if args.npart:
-        spec.update(npart=args.npart, nhalo=max(10, int(WORKLOAD["nhalo"] * args.npart / WORKLOAD["npart"])),
-                    name=f"scaled_{args.npart}")
+        spec = _scaled(spec, args.npart)
     ps = _gen(spec)
     n = ps.n
     eps = finder.configure(n, **PARAMS)
@@ -440,17 +473,13 @@ def main():
     peak = float(peaks.get("hbm_gbs", 6650.0))
     alg = 168.0 * n
     achieved = alg / (knn_avg / 1e3) / 1e9
-    traffic = None
-    inst = None
-    try:
-        prof = json.load(open(os.path.join(REPO, "profiles", "knn_density_traffic.txt")))
-        traffic = prof["dram_bytes_per_particle"] * n
-        inst = prof.get("warp_instructions_per_particle")
-    except Exception:
-        pass
+    traffic = NCU_KNN["dram_bytes_per_particle"] * n
+    inst = NCU_KNN["warp_instructions_per_particle"]
     roof = {"kernel": "knn_leaf_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "alg_bytes_per_launch": alg,
-            "launch_ms": knn_avg, "peak_source": "measured" if peaks else "fallback"}
+            "launch_ms": knn_avg, "peak_source": "measured" if peaks else "fallback",
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per particle x n (" +
+                              NCU_KNN["profiled"] + ")"}
     if inst:
         # the kernel is bound by instruction issue, not HBM: the warp instructions
         # ncu counted per query (profiles/) over this launch's time, against the
@@ -461,6 +490,14 @@ def main():
         ach = inst * n / (knn_avg / 1e3)
         roof["issue"] = {"achieved_warp_inst_per_s": ach, "peak_warp_inst_per_s": issue_peak,
                          "frac": ach / issue_peak, "warp_inst_per_query": inst}
+    # kNN and structure-tree counters come from one more call, after the timed
+    # region, with the profiling instances of the kernels (the timed calls run
+    # the production instances, which count nothing)
+    lib.ahop_debug_set_task_profile.argtypes = [C.c_int32]
+    L.check(lib.ahop_debug_set_task_profile(1), "set_task_profile")
+    dev_step()
+    torch.cuda.synchronize()
+    L.check(lib.ahop_debug_set_task_profile(0), "set_task_profile")
     ts = (C.c_int64 * 13)()
     lib.ahop_debug_tree_stats(ts, 13)
     tree_stats = {"structural_Mcycles": ts[0] / 1e6, "level_stats_Mcycles": ts[1] / 1e6,
@@ -475,9 +512,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": "Mpart/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": spec["name"], "npart": n, "nhalo": spec["nhalo"], "seed": spec["seed"],
-                       "epsilon": eps, **PARAMS, "l2": f"inputs ({n * 32 / 1e6:.0f} MB) larger than L2",
-                       "parallelism": f"replicas{world}"},
+            "config": workload_config(spec, world),
             "e2e": {"value": e2e, "unit": "Mpart/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roof, "stages_ms": mean_stage,
             "stages_mpart_per_s": {k: (n / (v / 1e3) / 1e6 if v > 0 else None) for k, v in mean_stage.items()},
@@ -487,9 +522,9 @@ def main():
     if not args.no_halo:
         line["halo_epot"] = halo_section(args, torch, dist if world > 1 else None)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, dt, nth, _ = cpu_sample_rate()
+        rate, dt, nth, _ = cpu_rate(ps)
         line["cpu_baseline"] = {"value": rate, "unit": "Mpart/s", "cores": nth, "kind": "port",
-                                "sample": f"{CPU_SAMPLE['npart']} particles ({CPU_SAMPLE['name']}), full finder, "
+                                "sample": f"{n} particles ({spec['name']}, the bench box): one full finder pass, "
                                           f"{dt:.1f} s"}
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -90,13 +90,19 @@ def compute_device(d_off, d_pos, d_vel, d_mass, d_dens, d_out, Lbox, Hub_pt, gra
 def compute_device_noalloc(d_off, d_pos, d_vel, d_mass, d_dens, d_out, Lbox, Hub_pt, gravconst=430.1,
                            periodic=True, epot=3, stream=None):
     """Same as compute_device, through the allocation-free entry point
-    (ahop_halo_props_noalloc): no device memory is allocated by the call."""
+    (ahop_halo_props_noalloc): no device memory is allocated by the call.
+    The default stream is torch's current stream.  The call blocks the host
+    twice and refuses a capturing stream; next to another thread's capture
+    pass a non-blocking stream (the legacy default stream would join it)."""
     lib = _lib()
     lib.ahop_halo_props_noalloc.argtypes = [C.POINTER(AhopHaloParams), C.c_void_p, C.c_int64, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     p = params(Lbox, Hub_pt, gravconst, periodic, epot)
     nh = d_off.numel() - 1
-    st = C.c_void_p(stream.cuda_stream if stream is not None else 0)
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    st = C.c_void_p(stream.cuda_stream)
     L.check(lib.ahop_halo_props_noalloc(C.byref(p), d_off.data_ptr(), nh, d_pos.data_ptr(), d_vel.data_ptr(),
                                         d_mass.data_ptr(), d_dens.data_ptr(), d_out.data_ptr(), st),
             "halo_props_noalloc")

@@ -1462,9 +1462,19 @@ extern "C" int ahop_halo_props_noalloc(const AhopHaloParams* p, const int64_t* d
     return AHOP_EINVAL;
   }
   if (nhalo == 0) return AHOP_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // the call reads the item count and the error flag back to the host, so it
+  // cannot be recorded into a graph: refuse a capturing stream before any
+  // work is enqueued (enqueueing would invalidate the caller's capture)
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  AHOP_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone) {
+    set_error("the stream is being captured; ahop_halo_props_noalloc synchronises with the host and cannot run "
+              "inside a stream capture");
+    return AHOP_EINVAL;
+  }
   NoAllocScratch* S = nullptr;
   if ((rc = noalloc_setup(&S))) return rc;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   noalloc_offsets_kernel<<<1, 1024, 0, st>>>(d_off, nhalo, S);
   AHOP_CUDA_TRY(cudaGetLastError());
   int32_t total = 0;

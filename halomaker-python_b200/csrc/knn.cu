@@ -215,8 +215,9 @@ struct KnnArgs {
   unsigned long long* kstats;  // [0] query leaves [1] candidate leaves [2] leaf visits [3] insertions [4] overflows
   unsigned* kspill;             // per-warp candidate spill buffers [grid warps][2 * kMaxCandSpill], or null
   const float4* box32;          // boxes of every level in FP32, widened (leaf_box32_kernel)
-  int kdebug;   // extra counters: [5] leaves within the final radius, [6]/[7] cycles of overflow/other leaves,
-                // [24..28] phase cycles of the other leaves (bound, candidates + sort, seed lists, scan, density)
+                // profiled instances also count [5] leaves within the final radius, [6]/[7] cycles of
+                // overflow/other leaves, [24..28] phase cycles of the other leaves (bound, candidates +
+                // sort, seed lists, scan, density)
 };
 
 constexpr int kWarpsPerBlock = 8;
@@ -564,7 +565,9 @@ static_assert((kMaxCand & (kMaxCand - 1)) == 0 && (kMaxCandSpill & (kMaxCandSpil
 //     distance and stopping at the first whose box-to-box distance exceeds it.
 // The candidate leaves are shared by the 32 queries, so the traversal is
 // paid once per leaf and the leaf data mostly comes from L1.
-template <int C>
+// kProf: the counters and cycle stamps of the profiling API (off in the
+// production instances, so they cost nothing there).
+template <int C, bool kProf>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArgs A) {
   __shared__ int32_t s_node[kWarpsPerBlock][kStack];
   __shared__ double s_bd[kWarpsPerBlock][kStack];
@@ -581,7 +584,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
   unsigned* s_key = reinterpret_cast<unsigned*>(s_bd[wib]);
   static_assert(kStack * 2 >= kMaxCand, "sort keys must fit the fallback stack");
   for (int64_t jl = (int64_t)blockIdx.x * kWarpsPerBlock + wib; jl < nleaf; jl += nwarps) {
-    const long long t_leaf = clock64();
+    const long long t_leaf = kProf ? clock64() : 0;
     const int64_t jn = (jl + 1 < nleaf) ? jl + 1 : jl - 1;  // adjacent leaf (jn >= 0 when nleaf >= 2)
     const int64_t s0 = jl * kLeaf;
     const int nq = (int)((A.n - s0) < kLeaf ? (A.n - s0) : (int64_t)kLeaf);
@@ -602,7 +605,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) R2 = fmax(R2, __shfl_xor_sync(0xffffffffu, R2, o));
     if (!ok) R2 = CUDART_INF;
-    const long long t_a = clock64();
+    const long long t_a = kProf ? clock64() : 0;
     // ---- B: candidate leaves within R of this leaf's box; the list lives in
     // shared memory and moves to the warp's global spill buffer past kMaxCand
     const float4* myb32 = A.box32 + 2 * jl;
@@ -681,7 +684,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
         }
       }
     }
-    const long long t_b = clock64();
+    const long long t_b = kProf ? clock64() : 0;
     long long c_init = 0, c_scan = 0, c_fin = 0;
     // ---- C: per-query kNN over the candidates
     unsigned nvis = 0, nins = 0, nideal = 0;
@@ -690,9 +693,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
       const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
       const float qxf = (float)qx, qyf = (float)qy, qzf = (float)qz;
       WarpList L;
-      const long long tq0 = clock64();
+      const long long tq0 = kProf ? clock64() : 0;
       seed_list<C>(A, L, jl, jn, s, qx, qy, qz, lane, s_list[wib][q], nvis);
-      const long long tq1 = clock64();
+      const long long tq1 = kProf ? clock64() : 0;
       if (overflow) {
         query_dfs<C>(A, L, s, qx, qy, qz, lane, s_node[wib], s_bd[wib], jl, jn, nvis, nins);
       } else {
@@ -719,10 +722,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
           }
         }
       }
-      const long long tq2 = clock64();
+      const long long tq2 = kProf ? clock64() : 0;
       c_init += tq1 - tq0;
       c_scan += tq2 - tq1;
-      if (A.kdebug && !overflow) {
+      if (kProf && !overflow) {
         // leaves that any search with these boxes must visit: box within the final radius
         for (int c0 = 0; c0 < ncand; c0 += 32) {
           const int ci = c0 + lane;
@@ -731,12 +734,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
           nideal += __popc(__ballot_sync(0xffffffffu, in));
         }
       }
-      const long long tq3 = clock64();
+      const long long tq3 = kProf ? clock64() : 0;
       finish_query<C>(A, L, s, lane);
       __syncwarp();
-      c_fin += clock64() - tq3;
+      if (kProf) c_fin += clock64() - tq3;
     }
-    if (lane == 0 && A.kstats && A.kdebug) {
+    if (kProf && lane == 0) {
       unsigned long long* ph = A.kstats + 24;  // phase cycles of non-overflow leaves
       if (!overflow) {
         atomicAdd(&ph[0], (unsigned long long)(t_a - t_leaf));
@@ -748,7 +751,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
       atomicAdd(&A.kstats[5], (unsigned long long)nideal);
       atomicAdd(&A.kstats[overflow ? 6 : 7], (unsigned long long)(clock64() - t_leaf));
     }
-    if (lane == 0 && A.kstats) {
+    if (kProf && lane == 0) {
       atomicAdd(&A.kstats[0], 1ULL);
       atomicAdd(&A.kstats[1], (unsigned long long)ncand);
       atomicAdd(&A.kstats[2], (unsigned long long)nvis);
@@ -789,15 +792,16 @@ int stage_knn_density(Engine& E) {
   AHOP_CUDA_TRY(cudaMemsetAsync(E.d_flags.p, 0, 512, E.stream));
   A.err = E.d_flags.as<int>();
   A.kstats = reinterpret_cast<unsigned long long*>(E.d_flags.as<char>() + 64);
-  A.kdebug = E.task_profile ? 1 : 0;
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, E.device);
   // the default nvoisins = 32 (one list entry per lane) has its own build with
   // the count fixed at compile time
   const bool nv32 = P.nvoisins == 32;
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm, nv32 ? (const void*)knn_leaf_kernel<32> : (const void*)knn_leaf_kernel<0>, kWarpsPerBlock * 32, 0);
+  const bool prof = E.task_profile;
+  const void* kfn = nv32 ? (prof ? (const void*)knn_leaf_kernel<32, true> : (const void*)knn_leaf_kernel<32, false>)
+                         : (prof ? (const void*)knn_leaf_kernel<0, true> : (const void*)knn_leaf_kernel<0, false>);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kWarpsPerBlock * 32, 0);
   if (per_sm < 1) per_sm = 1;
   int64_t want = (E.lev_cnt[0] + kWarpsPerBlock - 1) / kWarpsPerBlock;
   int64_t grid = (int64_t)nsm * per_sm * 2;
@@ -806,8 +810,10 @@ int stage_knn_density(Engine& E) {
   A.kspill = E.d_kspill.as<unsigned>();
   E.launches++;
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[9], E.stream));
-  if (nv32) knn_leaf_kernel<32><<<(unsigned)grid, kWarpsPerBlock * 32, 0, E.stream>>>(A);
-  else knn_leaf_kernel<0><<<(unsigned)grid, kWarpsPerBlock * 32, 0, E.stream>>>(A);
+  if (nv32 && prof) knn_leaf_kernel<32, true><<<(unsigned)grid, kWarpsPerBlock * 32, 0, E.stream>>>(A);
+  else if (nv32) knn_leaf_kernel<32, false><<<(unsigned)grid, kWarpsPerBlock * 32, 0, E.stream>>>(A);
+  else if (prof) knn_leaf_kernel<0, true><<<(unsigned)grid, kWarpsPerBlock * 32, 0, E.stream>>>(A);
+  else knn_leaf_kernel<0, false><<<(unsigned)grid, kWarpsPerBlock * 32, 0, E.stream>>>(A);
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[10], E.stream));
   AHOP_CUDA_TRY(cudaGetLastError());
   int herr = 0;

@@ -302,7 +302,12 @@ int ahop_halo_set_graph(int32_t on);
  * inputs and the device output [nhalo][AHOP_HALO_NFIELDS].  Every call shares
  * that array, so calls that overlap on the GPU (other streams, other host
  * threads) race; serialise them.  The first call on a device looks up the
- * array's address and should come before any stream capture. */
+ * array's address and should come before any stream capture.  Each call
+ * blocks the host twice (it reads the work-item count, then the error flag,
+ * back from the device), so it must not be called on a stream that is being
+ * captured (it returns AHOP_EINVAL there).  Next to another thread's capture,
+ * pass a non-blocking stream (cudaStreamNonBlocking): the legacy default
+ * stream synchronises implicitly with blocking streams and would join it. */
 int ahop_halo_props_noalloc(const AhopHaloParams* p, const int64_t* d_off, int64_t nhalo, const double* d_pos,
                             const double* d_vel, const double* d_mass, const double* d_density, double* d_out,
                             void* stream);
