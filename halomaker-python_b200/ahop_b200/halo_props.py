@@ -2,9 +2,11 @@
 
 Replaces the per-halo property chain of the reference
 (_compute_halo_props, src/compute_halo_props.py:270-301) for the fields it
-lists: mass, centre (densest member), bulk velocity, sigma, angular momentum,
-r, inertia tensor and principal axes, E_kin (with Hubble flow), the direct-sum
-E_pot in FP64 and FP32-compensated forms, and spin.
+lists: mass with its dark-matter / star split, centre (densest member, the
+member closest to the centre of mass with cdm, or the shrinking sphere),
+bulk velocity, sigma (all, dark matter, stars), angular momentum, r, inertia
+tensor and principal axes, E_kin (with Hubble flow), the direct-sum E_pot in
+FP64 and FP32-compensated forms, and spin.
 """
 from __future__ import annotations
 
@@ -15,14 +17,16 @@ import numpy as np
 from . import _lib as L
 
 FIELDS = ["m", "px", "py", "pz", "vx", "vy", "vz", "Lx", "Ly", "Lz", "r", "Ixx", "Ixy", "Ixz", "Iyy", "Iyz",
-          "Izz", "ek", "ep64", "ep32c", "sigma", "sha", "shb", "shc", "spin64", "spin32c", "icenter"]
+          "Izz", "ek", "ep64", "ep32c", "sigma", "sha", "shb", "shc", "spin64", "spin32c", "icenter",
+          "ndm", "nstar", "mdm", "m*", "mcontam", "sigma_dm", "sigma*"]
 NF = len(FIELDS)
 
 
 class AhopHaloParams(C.Structure):
     _fields_ = [("Lbox", C.c_double), ("Hub_pt", C.c_double), ("gravconst", C.c_double),
                 ("periodic", C.c_int32), ("epot", C.c_int32), ("sc", C.c_int32), ("pad", C.c_int32),
-                ("dcell_min", C.c_double), ("eps_sc", C.c_double)]
+                ("dcell_min", C.c_double), ("eps_sc", C.c_double), ("cdm", C.c_int32), ("pad2", C.c_int32),
+                ("ndm", C.c_int64), ("massp", C.c_double), ("index", C.c_void_p)]
 
 
 class AhopHaloTimings(C.Structure):
@@ -53,16 +57,25 @@ def _lib():
     return lib
 
 
-def params(Lbox, Hub_pt, gravconst=430.1, periodic=True, epot=3, sc=None):
+def params(Lbox, Hub_pt, gravconst=430.1, periodic=True, epot=3, sc=None, cdm=False, ndm=None, massp=0.0,
+           index=None):
     """sc: None (centre = densest member) or (dcell_min, eps_SC) for the
-    shrinking-sphere centre of refine_centers_1b."""
+    shrinking-sphere centre of refine_centers_1b.  cdm: centre = member
+    closest to the centre of mass (H.cdm).  index: the members' particle
+    indices (a pointer in the memory of the call's other arrays, or None:
+    every member is dark matter); members with index < ndm are dark matter
+    (H.ndm), those heavier than massp * 1.00001 count as contamination."""
     on = sc is not None
     return AhopHaloParams(float(Lbox), float(Hub_pt), float(gravconst), int(bool(periodic)), int(epot), int(on), 0,
-                          float(sc[0]) if on else 0.0, float(sc[1]) if on else 0.0)
+                          float(sc[0]) if on else 0.0, float(sc[1]) if on else 0.0, int(bool(cdm)), 0,
+                          int(ndm if ndm is not None else 2 ** 62), float(massp), index)
 
 
-def compute(off, pos, vel, mass, dens, Lbox, Hub_pt, gravconst=430.1, periodic=True, epot=3, sc=None) -> dict:
-    """Host arrays in, dict of per-halo arrays out (FIELDS)."""
+def compute(off, pos, vel, mass, dens, Lbox, Hub_pt, gravconst=430.1, periodic=True, epot=3, sc=None, cdm=False,
+            index=None, ndm=None, massp=0.0) -> dict:
+    """Host arrays in, dict of per-halo arrays out (FIELDS).  index: the
+    members' particle indices (int32, the reference's indexps), members with
+    index < ndm being dark matter; None: every member is dark matter."""
     off = np.ascontiguousarray(off, np.int64)
     nh = len(off) - 1
     pos = np.ascontiguousarray(pos, np.float64)
@@ -70,16 +83,20 @@ def compute(off, pos, vel, mass, dens, Lbox, Hub_pt, gravconst=430.1, periodic=T
     mass = np.ascontiguousarray(mass, np.float64)
     dens = np.ascontiguousarray(dens, np.float64)
     out = np.zeros((max(nh, 1), NF))
-    p = params(Lbox, Hub_pt, gravconst, periodic, epot, sc)
+    idx = None if index is None else np.ascontiguousarray(index, np.int32)
+    p = params(Lbox, Hub_pt, gravconst, periodic, epot, sc, cdm, ndm, massp,
+               None if idx is None else idx.ctypes.data)
     L.check(_lib().ahop_halo_props(C.byref(p), off.ctypes.data, nh, pos.ctypes.data, vel.ctypes.data,
                                    mass.ctypes.data, dens.ctypes.data, out.ctypes.data), "halo_props")
     return {f: out[:nh, k].copy() for k, f in enumerate(FIELDS)}
 
 
 def compute_device(d_off, d_pos, d_vel, d_mass, d_dens, d_out, Lbox, Hub_pt, gravconst=430.1, periodic=True,
-                   epot=3, stream=None):
-    """torch CUDA tensors in; fills d_out (nhalo, NF) in place."""
-    p = params(Lbox, Hub_pt, gravconst, periodic, epot)
+                   epot=3, stream=None, sc=None, cdm=False, d_index=None, ndm=None, massp=0.0):
+    """torch CUDA tensors in; fills d_out (nhalo, NF) in place.  d_index: the
+    members' particle indices (int32 tensor) or None."""
+    p = params(Lbox, Hub_pt, gravconst, periodic, epot, sc, cdm, ndm, massp,
+               None if d_index is None else d_index.data_ptr())
     nh = d_off.numel() - 1
     st = C.c_void_p(stream.cuda_stream if stream is not None else 0)
     L.check(_lib().ahop_halo_props_device(C.byref(p), d_off.data_ptr(), nh, d_pos.data_ptr(), d_vel.data_ptr(),

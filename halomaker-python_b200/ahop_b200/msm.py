@@ -70,3 +70,15 @@ def gather_device(d_pos, d_vel, d_mass, stream=None):
     L.check(lib.ahop_gather_members_device(ptr(d_pos), ptr(d_vel), ptr(d_mass), ptr(off), ptr(ids), ptr(pos),
                                            ptr(vel), ptr(mass), ptr(dens), st), "gather_members_device")
     return off, ids[:ns.value], pos[:m], (vel[:m] if vel is not None else None), mass[:m], dens[:m]
+
+
+def gather_index_device(nmembers, device, stream=None):
+    """Particle index (0-based, caller's order) of every member gathered by
+    gather_device, in the same order, as an int32 CUDA tensor."""
+    import torch
+    lib = L.lib()
+    lib.ahop_gather_member_index_device.argtypes = [C.c_void_p, C.c_void_p]
+    idx = torch.empty(max(int(nmembers), 1), dtype=torch.int32, device=device)
+    st = stream.cuda_stream if stream is not None else 0
+    L.check(lib.ahop_gather_member_index_device(idx.data_ptr(), st), "gather_member_index_device")
+    return idx[:int(nmembers)]

@@ -23,14 +23,22 @@ from . import finder, halo_props, msm, ramses
 
 def run_snapshot(pos: np.ndarray, vel: np.ndarray, mass: np.ndarray, box: float = 1.0, hub: float = 70.0,
                  gravconst: float = 430.1, epot: int = 2, finder_params: dict | None = None,
-                 particle_views: bool = False) -> dict:
+                 particle_views: bool = False, ndm: int | None = None, cdm: bool = False, massp: float = 0.0,
+                 virial: bool = True, vir_overdens: float = 178.0, rho_mean: float | None = None) -> dict:
     """Host arrays pos (N,3), vel (N,3), mass (N,) in box units ([-box/2, box/2)).
 
     Returns the structure selection (ids, tree arrays; the per-particle arrays
     whereIam_parts / pids_groupsorted only with particle_views), one property
     row per structure with members (halo_props.FIELDS, structure order =
-    ascending id) and per-stage times in ms (device stages by CUDA events, the
-    rest by the host clock around synchronised steps)."""
+    ascending id), with virial one row of the virial step per structure
+    (halo_props.VIR_FIELDS), and per-stage times in ms (device stages by CUDA
+    events, the rest by the host clock around synchronised steps).
+
+    ndm: particles [0, ndm) are dark matter, the rest stars (det_mass_17's
+    split; None: all dark matter); cdm: centre = member closest to the centre
+    of mass; massp: dark-matter contamination threshold (H.massp);
+    vir_overdens, rho_mean: H.vir_overdens and H.rho_mean of the virial step
+    (CHP:1330-1331; rho_mean defaults to the total mass over box**3)."""
     import torch
     n = int(mass.shape[0])
     finder.configure(n, box=box, **(finder_params or {}))
@@ -47,11 +55,14 @@ def run_snapshot(pos: np.ndarray, vel: np.ndarray, mass: np.ndarray, box: float 
     d_mass = h_mass.to(dev, non_blocking=True)
     torch.cuda.synchronize()
     times["h2d"] = (time.perf_counter() - t0) * 1e3
-    return _run_device(d_pos, d_vel, d_mass, box, hub, gravconst, epot, particle_views, times)
+    opts = dict(ndm=ndm, cdm=cdm, massp=massp, virial=virial, vir_overdens=vir_overdens, rho_mean=rho_mean)
+    return _run_device(d_pos, d_vel, d_mass, box, hub, gravconst, epot, particle_views, times, **opts)
 
 
-def _run_device(d_pos, d_vel, d_mass, box, hub, gravconst, epot, particle_views, times):
-    """Finder, selection, member gather and properties on device arrays."""
+def _run_device(d_pos, d_vel, d_mass, box, hub, gravconst, epot, particle_views, times, ndm=None, cdm=False,
+                massp=0.0, virial=True, vir_overdens=178.0, rho_mean=None):
+    """Finder, selection, member gather, properties and the virial step on
+    device arrays."""
     import torch
     n = int(d_mass.shape[0])
     dev = d_pos.device
@@ -68,38 +79,58 @@ def _run_device(d_pos, d_vel, d_mass, box, hub, gravconst, epot, particle_views,
     times["msm"] = (time.perf_counter() - t0) * 1e3
     t0 = time.perf_counter()
     off, ids, gpos, gvel, gmass, gdens = msm.gather_device(d_pos, d_vel, d_mass, stream=st)
+    gidx = msm.gather_index_device(gmass.shape[0], dev, stream=st) if ndm is not None else None
     torch.cuda.synchronize()
     times["gather"] = (time.perf_counter() - t0) * 1e3
     ns = int(ids.numel())
     out = torch.empty((max(ns, 1), halo_props.NF), dtype=torch.float64, device=dev)
     t0 = time.perf_counter()
     if ns:
-        halo_props.compute_device(off, gpos, gvel, gmass, gdens, out, box, hub, gravconst, True, epot, stream=st)
+        halo_props.compute_device(off, gpos, gvel, gmass, gdens, out, box, hub, gravconst, True, epot, stream=st,
+                                  cdm=cdm, d_index=gidx, ndm=ndm, massp=massp)
     torch.cuda.synchronize()
     times["props"] = (time.perf_counter() - t0) * 1e3
     times["props_stages"] = halo_props.timings() if ns else {}
+    vrows = None
+    if virial and ns:
+        # det_vir_1b on the same members (CHP:1241-1262), from the rows above
+        t0 = time.perf_counter()
+        rm = float(rho_mean) if rho_mean is not None else float(d_mass.sum().item()) / box ** 3
+        vout = torch.empty((ns, halo_props.NV), dtype=torch.float64, device=dev)
+        ep = "ep64" if epot & 1 else "ep32c"
+        halo_props.virial_device(off, gpos, gvel, gmass, out, vout, box, hub, gravconst, vir_overdens, rm,
+                                 ep=ep, stream=st)
+        torch.cuda.synchronize()
+        times["virial"] = (time.perf_counter() - t0) * 1e3
+        vrows = vout.cpu().numpy()
     t0 = time.perf_counter()
     rows = out[:ns].cpu().numpy()
     ids_h = ids.cpu().numpy()
     off_h = off.cpu().numpy()
     times["d2h"] = (time.perf_counter() - t0) * 1e3
-    return dict(sel, ids=ids_h, offsets=off_h, props=rows, members=int(off_h[-1]) if ns else 0, timings=times)
+    return dict(sel, ids=ids_h, offsets=off_h, props=rows, virial=vrows, members=int(off_h[-1]) if ns else 0,
+                timings=times)
 
 
 def run_snapshot_files(repository, version: int = 3, family: str = "all", scale_l: float = 1.0,
                        scale_t: float = 1.0, box: float = 1.0, hub: float = 70.0, gravconst: float = 430.1,
-                       epot: int = 2, finder_params: dict | None = None, particle_views: bool = False) -> dict:
+                       epot: int = 2, finder_params: dict | None = None, particle_views: bool = False,
+                       cdm: bool = False, massp: float = 0.0, virial: bool = True, vir_overdens: float = 178.0,
+                       rho_mean: float | None = None) -> dict:
     """The same snapshot step starting from RAMSES part files (an
     output_NNNNN directory or the file paths): read_ramses_new_101's particle
     arrays are decoded on the device (ramses.read_parts) and never visit host
     memory.  Positions come out in [-0.5, 0.5) box units, as the reference's
-    reader leaves them."""
+    reader leaves them; dark-matter rows come first (family 'all'), so the
+    reader's ndm splits dark matter from stars in the properties."""
     import torch
     t0 = time.perf_counter()
     r = ramses.read_parts(repository, version, family, scale_l, scale_t)
     torch.cuda.synchronize()
     times = {"read": (time.perf_counter() - t0) * 1e3}
     finder.configure(int(r["nselected"]), box=box, **(finder_params or {}))
-    out = _run_device(r["pos"], r["vel"], r["mass"], box, hub, gravconst, epot, particle_views, times)
+    ndm = int(r["ndm"]) if family == "all" else (int(r["nselected"]) if family == "dm" else 0)
+    out = _run_device(r["pos"], r["vel"], r["mass"], box, hub, gravconst, epot, particle_views, times, ndm=ndm,
+                      cdm=cdm, massp=massp, virial=virial, vir_overdens=vir_overdens, rho_mean=rho_mean)
     out.update(ndm=r["ndm"], nstar=r["nstar"], nselected=r["nselected"])
     return out

@@ -31,6 +31,7 @@ class ParticleSet:
     halo_counts: np.ndarray   # (nhalo,) int64 particles per host halo (incl. subhalos)
     box: float = 1.0
     seed: int = 0
+    ndm: int | None = None    # particles [0, ndm) are dark matter, the rest stars (None: all dark matter)
 
     @property
     def n(self) -> int:
@@ -77,7 +78,9 @@ def clustered_box(npart: int, nhalo: int, seed: int, halo_fraction: float = 0.6,
 
     ``star_fraction`` > 0 turns that fraction of each halo's particles into
     stars of mass 0.1 m concentrated in the halo core (half-mass radius 0.05
-    r_vir); masses are then renormalised to a total of 1.
+    r_vir); masses are then renormalised to a total of 1, and the particles
+    are ordered dark matter first, then stars (as the RAMSES reader lays out
+    family 'all'), with ``ndm`` the dark-matter count.
     """
     rng = np.random.Generator(np.random.PCG64(seed))
     counts = _powerlaw_counts(rng, nhalo, slope, nmin, nmax)
@@ -142,10 +145,14 @@ def clustered_box(npart: int, nhalo: int, seed: int, halo_fraction: float = 0.6,
     perm = rng.permutation(npart)
     pos, vel, hid, is_star = pos[perm], vel[perm], hid[perm], is_star[perm]
     mass = np.full(npart, 1.0 / npart, np.float64)
+    ndm = None
     if star_fraction > 0.0:
         mass[is_star] *= 0.1
         mass /= mass.sum()
-    return ParticleSet(np.ascontiguousarray(pos), np.ascontiguousarray(vel), mass, hid, counts, box, seed)
+        order = np.argsort(is_star, kind="stable")  # dark matter first
+        pos, vel, hid, mass = pos[order], vel[order], hid[order], mass[order]
+        ndm = int(npart - np.count_nonzero(is_star))
+    return ParticleSet(np.ascontiguousarray(pos), np.ascontiguousarray(vel), mass, hid, counts, box, seed, ndm)
 
 
 # Named workloads (seeds fixed per workload).

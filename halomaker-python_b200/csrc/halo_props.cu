@@ -56,6 +56,16 @@ __device__ __forceinline__ double wrap_chp(double d, double L, double h, int per
   return d;
 }
 
+// det_mass_17's dmmask (CHP:766): particle index below ndm
+__device__ __forceinline__ bool member_is_dm(const HaloArgs& A, int64_t i) {
+  return A.index == nullptr || (int64_t)A.index[i] < A.ndm;
+}
+
+// correct_for_periodicity on an absolute coordinate (CHP:880-885)
+__device__ __forceinline__ double wrap_abs(double x, double L, double h, int periodic) {
+  return wrap_chp(x, L, h, periodic);
+}
+
 template <class T, int NT = kPB>
 __device__ __forceinline__ T block_sum(T v, T* sh) {
   const int tid = threadIdx.x;
@@ -176,13 +186,27 @@ __global__ void __launch_bounds__(kPB) halo_moments_kernel(HaloArgs A) {
   const int64_t b0 = A.off[h], b1 = A.off[h + 1];
   // pass 1
   double m = 0, mvx = 0, mvy = 0, mvz = 0, bd = -DBL_MAX;
+  double mdm = 0, mst = 0, ndm = 0, nst = 0, mcon = 0, cmx = 0, cmy = 0, cmz = 0;
   long long bi = LLONG_MAX;
+  const double fx = b1 > b0 ? A.pos[3 * b0] : 0.0, fy = b1 > b0 ? A.pos[3 * b0 + 1] : 0.0,
+               fz = b1 > b0 ? A.pos[3 * b0 + 2] : 0.0;
   for (int64_t i = b0 + tid; i < b1; i += kPB) {
     const double w = A.mass[i];
     m += w;
     mvx += w * A.vel[3 * i];
     mvy += w * A.vel[3 * i + 1];
     mvz += w * A.vel[3 * i + 2];
+    if (member_is_dm(A, i)) {
+      mdm += w; ndm += 1.0;
+      if (w > A.massp * 1.00001) mcon += w;
+    } else {
+      mst += w; nst += 1.0;
+    }
+    if (A.cdm) {
+      cmx += w * wrap_chp(A.pos[3 * i] - fx, A.L, A.h, A.periodic);
+      cmy += w * wrap_chp(A.pos[3 * i + 1] - fy, A.L, A.h, A.periodic);
+      cmz += w * wrap_chp(A.pos[3 * i + 2] - fz, A.L, A.h, A.periodic);
+    }
     const double d = A.dens[i];
     if (d > bd || (d == bd && i < bi)) { bd = d; bi = i; }  // np.argmax: first maximum
   }
@@ -197,6 +221,9 @@ __global__ void __launch_bounds__(kPB) halo_moments_kernel(HaloArgs A) {
   mvx = block_sum(mvx, sh);
   mvy = block_sum(mvy, sh);
   mvz = block_sum(mvz, sh);
+  mdm = block_sum(mdm, sh); mst = block_sum(mst, sh); ndm = block_sum(ndm, sh); nst = block_sum(nst, sh);
+  mcon = block_sum(mcon, sh);
+  if (A.cdm) { cmx = block_sum(cmx, sh); cmy = block_sum(cmy, sh); cmz = block_sum(cmz, sh); }
   if (tid == 0) {
     double d = s_best_d[0];
     long long ii = s_best_i[0];
@@ -212,10 +239,43 @@ __global__ void __launch_bounds__(kPB) halo_moments_kernel(HaloArgs A) {
     s_c[6] = (double)(ii - b0);
   }
   __syncthreads();
+  if (A.cdm && b1 > b0) {
+    // the member closest to the centre of mass (CHP:917-934)
+    const double px = wrap_abs(cmx / m + fx, A.L, A.h, A.periodic);
+    const double py = wrap_abs(cmy / m + fy, A.L, A.h, A.periodic);
+    const double pz = wrap_abs(cmz / m + fz, A.L, A.h, A.periodic);
+    double bdd = DBL_MAX;
+    long long bii = LLONG_MAX;
+    for (int64_t i = b0 + tid; i < b1; i += kPB) {
+      const double dx = wrap_chp(A.pos[3 * i] - px, A.L, A.h, A.periodic);
+      const double dy = wrap_chp(A.pos[3 * i + 1] - py, A.L, A.h, A.periodic);
+      const double dz = wrap_chp(A.pos[3 * i + 2] - pz, A.L, A.h, A.periodic);
+      const double dd = dx * dx + dy * dy + dz * dz;
+      if (dd < bdd || (dd == bdd && i < bii)) { bdd = dd; bii = i; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double od = __shfl_xor_sync(0xffffffffu, bdd, o);
+      const long long oi = __shfl_xor_sync(0xffffffffu, bii, o);
+      if (od < bdd || (od == bdd && oi < bii)) { bdd = od; bii = oi; }
+    }
+    if ((tid & 31) == 0) { s_best_d[tid >> 5] = bdd; s_best_i[tid >> 5] = bii; }
+    __syncthreads();
+    if (tid == 0) {
+      double d = s_best_d[0];
+      long long ii = s_best_i[0];
+      for (int w = 1; w < kPB / 32; ++w)
+        if (s_best_d[w] < d || (s_best_d[w] == d && s_best_i[w] < ii)) { d = s_best_d[w]; ii = s_best_i[w]; }
+      s_c[0] = A.pos[3 * ii]; s_c[1] = A.pos[3 * ii + 1]; s_c[2] = A.pos[3 * ii + 2];
+      s_c[6] = (double)(ii - b0);
+    }
+    __syncthreads();
+  }
   if (A.sc) shrink_sphere_centre(A, b0, b1, s_c, sh, s_best_d, s_best_i);
   const double cx = s_c[0], cy = s_c[1], cz = s_c[2], vx = s_c[3], vy = s_c[4], vz = s_c[5];
   // pass 2
   double Lx = 0, Ly = 0, Lz = 0, r2max = 0, Ixx = 0, Ixy = 0, Ixz = 0, Iyy = 0, Iyz = 0, Izz = 0, ek = 0, sg = 0;
+  double sgd = 0, sgs = 0;
   for (int64_t i = b0 + tid; i < b1; i += kPB) {
     const double w = A.mass[i];
     const double dx = wrap_chp(A.pos[3 * i] - cx, A.L, A.h, A.periodic);
@@ -231,7 +291,10 @@ __global__ void __launch_bounds__(kPB) halo_moments_kernel(HaloArgs A) {
     Iyy += w * dy * dy; Iyz += w * dy * dz; Izz += w * dz * dz;
     const double tx = ux + dx * A.hub, ty = uy + dy * A.hub, tz = uz + dz * A.hub;
     ek += w * (tx * tx + ty * ty + tz * tz);
-    sg += w * (ux * ux + uy * uy + uz * uz);
+    const double dv2 = w * (ux * ux + uy * uy + uz * uz);
+    sg += dv2;
+    if (member_is_dm(A, i)) sgd += dv2;
+    else sgs += dv2;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) r2max = fmax(r2max, __shfl_xor_sync(0xffffffffu, r2max, o));
@@ -241,6 +304,8 @@ __global__ void __launch_bounds__(kPB) halo_moments_kernel(HaloArgs A) {
   Iyy = block_sum(Iyy, sh); Iyz = block_sum(Iyz, sh); Izz = block_sum(Izz, sh);
   ek = block_sum(ek, sh);
   sg = block_sum(sg, sh);
+  sgd = block_sum(sgd, sh);
+  sgs = block_sum(sgs, sh);
   if (tid == 0) {
     double rm = s_best_d[0];
     for (int w = 1; w < kPB / 32; ++w) rm = fmax(rm, s_best_d[w]);
@@ -254,6 +319,9 @@ __global__ void __launch_bounds__(kPB) halo_moments_kernel(HaloArgs A) {
     o[HP_EK] = 0.5 * ek;
     o[HP_SIGMA] = sqrt(sg / m);
     o[HP_ICENTER] = s_c[6];
+    o[HP_MDM] = mdm; o[HP_MSTAR] = mst; o[HP_NDM] = ndm; o[HP_NSTAR] = nst; o[HP_MCONTAM] = mcon;
+    o[HP_SIGMA_DM] = mdm > 0 ? sqrt(sgd / mdm) : 0.0;
+    o[HP_SIGMA_STAR] = mst > 0 ? sqrt(sgs / mst) : 0.0;
   }
 }
 
@@ -269,11 +337,16 @@ struct MomChunk {
   int32_t h, pad;
   int64_t b0, b1;
 };
+// pass 1 sums: mass, momentum, the dark-matter / star split of det_mass_17
+// (CHP:766-780) and the mass-weighted offsets from the halo's first member
+// that det_center_18's centre of mass starts from (CHP:920-926)
+constexpr int kP1 = 12;  // m mvx mvy mvz mdm mstar ndm nstar mcontam cmx cmy cmz
 struct MomP1 {
-  double m, mvx, mvy, mvz, bd;
+  double v[kP1];
+  double bd;
   long long bi;
 };
-constexpr int kP2 = 11;  // Lx Ly Lz Ixx Ixy Ixz Iyy Iyz Izz ek sg
+constexpr int kP2 = 13;  // Lx Ly Lz Ixx Ixy Ixz Iyy Iyz Izz ek sg sg_dm sg_star
 struct MomP2 {
   double v[kP2];
   double r2max;
@@ -281,6 +354,11 @@ struct MomP2 {
 struct MomCentre {
   double c[6];  // centre x, y, z, bulk velocity x, y, z
   long long ic; // centre member (absolute index)
+  double cm[3]; // centre of mass (cdm)
+};
+struct MomArg {  // chunk argmin of the distance to the centre of mass (cdm)
+  double d;
+  long long i;
 };
 
 // Sums of N values over the block (warp shuffles, then warp 0 over the
@@ -308,19 +386,35 @@ __device__ __forceinline__ void block_sum_n(double (&v)[N], double* sh) {
 
 __global__ void __launch_bounds__(kPB) mom_pass1_kernel(HaloArgs A, const MomChunk* __restrict__ ch,
                                                         MomP1* __restrict__ P) {
-  __shared__ double sh[5 * (kPB / 32) + 8];
+  __shared__ double sh[(kP1 + 1) * (kPB / 32) + 16];
   __shared__ double s_bd[kPB / 32];
   __shared__ long long s_bi[kPB / 32];
   const int tid = threadIdx.x;
   const MomChunk c = ch[blockIdx.x];
-  double v[4] = {0, 0, 0, 0}, bd = -DBL_MAX;
+  double v[kP1] = {}, bd = -DBL_MAX;
   long long bi = LLONG_MAX;
+  const int64_t first = A.off[c.h];
+  const double fx = A.pos[3 * first], fy = A.pos[3 * first + 1], fz = A.pos[3 * first + 2];
+  const double heavy = A.massp * 1.00001;
   for (int64_t i = c.b0 + tid; i < c.b1; i += kPB) {
     const double w = A.mass[i];
     v[0] += w;
     v[1] += w * A.vel[3 * i];
     v[2] += w * A.vel[3 * i + 1];
     v[3] += w * A.vel[3 * i + 2];
+    if (member_is_dm(A, i)) {
+      v[4] += w;
+      v[6] += 1.0;
+      if (w > heavy) v[8] += w;
+    } else {
+      v[5] += w;
+      v[7] += 1.0;
+    }
+    if (A.cdm) {
+      v[9] += w * wrap_chp(A.pos[3 * i] - fx, A.L, A.h, A.periodic);
+      v[10] += w * wrap_chp(A.pos[3 * i + 1] - fy, A.L, A.h, A.periodic);
+      v[11] += w * wrap_chp(A.pos[3 * i + 2] - fz, A.L, A.h, A.periodic);
+    }
     const double d = A.dens[i];
     if (d > bd || (d == bd && i < bi)) { bd = d; bi = i; }  // np.argmax: first maximum
   }
@@ -331,12 +425,17 @@ __global__ void __launch_bounds__(kPB) mom_pass1_kernel(HaloArgs A, const MomChu
     if (od > bd || (od == bd && oi < bi)) { bd = od; bi = oi; }
   }
   if ((tid & 31) == 0) { s_bd[tid >> 5] = bd; s_bi[tid >> 5] = bi; }
-  block_sum_n<4>(v, sh);
+  block_sum_n<kP1>(v, sh);
   if (tid == 0) {
     bd = s_bd[0]; bi = s_bi[0];
     for (int w = 1; w < kPB / 32; ++w)
       if (s_bd[w] > bd || (s_bd[w] == bd && s_bi[w] < bi)) { bd = s_bd[w]; bi = s_bi[w]; }
-    P[blockIdx.x] = MomP1{v[0], v[1], v[2], v[3], bd, bi};
+    MomP1 r;
+#pragma unroll
+    for (int k = 0; k < kP1; ++k) r.v[k] = v[k];
+    r.bd = bd;
+    r.bi = bi;
+    P[blockIdx.x] = r;
   }
 }
 
@@ -345,23 +444,81 @@ __global__ void mom_fold1_kernel(HaloArgs A, const int64_t* __restrict__ hcoff, 
                                  MomCentre* __restrict__ C, int64_t nhalo) {
   const int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (h >= nhalo) return;
-  double m = 0, mvx = 0, mvy = 0, mvz = 0, bd = -DBL_MAX;
+  double v[kP1] = {}, bd = -DBL_MAX;
   long long bi = LLONG_MAX;
   for (int64_t k = hcoff[h]; k < hcoff[h + 1]; ++k) {
-    const MomP1 p = P[k];
-    m += p.m; mvx += p.mvx; mvy += p.mvy; mvz += p.mvz;
+    const MomP1& p = P[k];
+#pragma unroll
+    for (int j = 0; j < kP1; ++j) v[j] += p.v[j];
     if (p.bd > bd || (p.bd == bd && p.bi < bi)) { bd = p.bd; bi = p.bi; }
   }
+  const double m = v[0];
   MomCentre c;
   if (bi != LLONG_MAX) {
     c.c[0] = A.pos[3 * bi]; c.c[1] = A.pos[3 * bi + 1]; c.c[2] = A.pos[3 * bi + 2];
   } else {
     c.c[0] = c.c[1] = c.c[2] = 0.0;
   }
-  c.c[3] = mvx / m; c.c[4] = mvy / m; c.c[5] = mvz / m;
+  c.c[3] = v[1] / m; c.c[4] = v[2] / m; c.c[5] = v[3] / m;
   c.ic = bi;
+  c.cm[0] = c.cm[1] = c.cm[2] = 0.0;
+  const int64_t first = A.off[h];
+  if (A.cdm && A.off[h + 1] > first) {
+    // centre of mass about the first member, then wrapped (CHP:920-927)
+    c.cm[0] = wrap_abs(v[9] / m + A.pos[3 * first], A.L, A.h, A.periodic);
+    c.cm[1] = wrap_abs(v[10] / m + A.pos[3 * first + 1], A.L, A.h, A.periodic);
+    c.cm[2] = wrap_abs(v[11] / m + A.pos[3 * first + 2], A.L, A.h, A.periodic);
+  }
   C[h] = c;
-  A.out[(size_t)kHaloFields * h + HP_M] = m;
+  double* o = A.out + (size_t)kHaloFields * h;
+  o[HP_M] = m;
+  o[HP_MDM] = v[4]; o[HP_MSTAR] = v[5]; o[HP_NDM] = v[6]; o[HP_NSTAR] = v[7]; o[HP_MCONTAM] = v[8];
+}
+
+// cdm: per chunk, the member closest to the halo's centre of mass
+// (np.argmin: first minimum, CHP:929-934)
+__global__ void __launch_bounds__(kPB) mom_cdm_kernel(HaloArgs A, const MomChunk* __restrict__ ch,
+                                                      const MomCentre* __restrict__ C, MomArg* __restrict__ P) {
+  __shared__ double s_bd[kPB / 32];
+  __shared__ long long s_bi[kPB / 32];
+  const int tid = threadIdx.x;
+  const MomChunk k = ch[blockIdx.x];
+  const double* cm = C[k.h].cm;
+  double bd = DBL_MAX;
+  long long bi = LLONG_MAX;
+  for (int64_t i = k.b0 + tid; i < k.b1; i += kPB) {
+    const double dx = wrap_chp(A.pos[3 * i] - cm[0], A.L, A.h, A.periodic);
+    const double dy = wrap_chp(A.pos[3 * i + 1] - cm[1], A.L, A.h, A.periodic);
+    const double dz = wrap_chp(A.pos[3 * i + 2] - cm[2], A.L, A.h, A.periodic);
+    const double d = dx * dx + dy * dy + dz * dz;
+    if (d < bd || (d == bd && i < bi)) { bd = d; bi = i; }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double od = __shfl_xor_sync(0xffffffffu, bd, o);
+    const long long oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (od < bd || (od == bd && oi < bi)) { bd = od; bi = oi; }
+  }
+  if ((tid & 31) == 0) { s_bd[tid >> 5] = bd; s_bi[tid >> 5] = bi; }
+  __syncthreads();
+  if (tid == 0) {
+    for (int w = 1; w < kPB / 32; ++w)
+      if (s_bd[w] < s_bd[0] || (s_bd[w] == s_bd[0] && s_bi[w] < s_bi[0])) { s_bd[0] = s_bd[w]; s_bi[0] = s_bi[w]; }
+    P[blockIdx.x] = MomArg{s_bd[0], s_bi[0]};
+  }
+}
+
+__global__ void mom_cdm_fold_kernel(HaloArgs A, const int64_t* __restrict__ hcoff, const MomArg* __restrict__ P,
+                                    MomCentre* __restrict__ C, int64_t nhalo) {
+  const int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (h >= nhalo) return;
+  double bd = DBL_MAX;
+  long long bi = LLONG_MAX;
+  for (int64_t k = hcoff[h]; k < hcoff[h + 1]; ++k)
+    if (P[k].d < bd || (P[k].d == bd && P[k].i < bi)) { bd = P[k].d; bi = P[k].i; }
+  if (bi == LLONG_MAX) return;
+  C[h].c[0] = A.pos[3 * bi]; C[h].c[1] = A.pos[3 * bi + 1]; C[h].c[2] = A.pos[3 * bi + 2];
+  C[h].ic = bi;
 }
 
 // shrinking-sphere refinement (SC on): one block per halo, as in the
@@ -407,7 +564,9 @@ __global__ void __launch_bounds__(kPB) mom_pass2_kernel(HaloArgs A, const MomChu
     v[6] += w * dy * dy; v[7] += w * dy * dz; v[8] += w * dz * dz;
     const double tx = ux + dx * A.hub, ty = uy + dy * A.hub, tz = uz + dz * A.hub;
     v[9] += w * (tx * tx + ty * ty + tz * tz);
-    v[10] += w * (ux * ux + uy * uy + uz * uz);
+    const double dv2 = w * (ux * ux + uy * uy + uz * uz);
+    v[10] += dv2;
+    v[member_is_dm(A, i) ? 11 : 12] += dv2;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) r2max = fmax(r2max, __shfl_xor_sync(0xffffffffu, r2max, o));
@@ -446,6 +605,9 @@ __global__ void mom_fold2_kernel(HaloArgs A, const int64_t* __restrict__ hcoff, 
   o[HP_EK] = 0.5 * v[9];
   o[HP_SIGMA] = sqrt(v[10] / m);
   o[HP_ICENTER] = (double)(c.ic - A.off[h]);
+  // det_center_18, mode 'full' (CHP:962-966)
+  o[HP_SIGMA_DM] = o[HP_MDM] > 0 ? sqrt(v[11] / o[HP_MDM]) : 0.0;
+  o[HP_SIGMA_STAR] = o[HP_MSTAR] > 0 ? sqrt(v[12] / o[HP_MSTAR]) : 0.0;
 }
 
 // ---------------------------------------------------------------- pair sums
@@ -521,20 +683,38 @@ __global__ void __launch_bounds__(kT64) epot64_kernel(HaloArgs A, const PairItem
 }
 
 // FP32-compensated form on packed FP32 pairs (the sm_100 f32x2 add/sub/mul/fma
-// instructions: two lanes per 64-bit register, one instruction).  Positions
-// relative to the halo centre are split into hi = float(r) and
-// lo = float(r - hi); a separation is (hi_j - hi_i) + (lo_j - lo_i).  The two
-// lanes of every packed register hold two partners j, 2q and 2q+1, of the same
-// row i, so a row's own coordinates are loop-invariant (hi_i, hi_i) pairs.
-// Each thread owns R rows (rows tid + 128 r); partner tiles are 128 * R
-// wide, shared memory holds them as packed pairs.  For every row, sixteen
-// partner pairs (32 terms) are accumulated by a fused multiply-add chain per
-// lane, then enter a Kahan-compensated FP32 sum; rows fold into FP64 per item.
-// Separations of exactly zero (coincident members) are excluded like in the
-// FP64 form: the fast path does not test for them -- rsqrt(0) = inf makes the
-// row's sum non-finite, and the block then recomputes the item with a
-// per-pair test.  The tile shape (R = 1, 2 or 4 rows per thread) is chosen
-// per halo-size bucket by the host-side autotuner and read per item.
+// instructions: two lanes per 64-bit register, one instruction).
+//
+// Members are read in the Morton order of their position about the halo
+// centre (sort32_* kernels below), so a run of consecutive members is a
+// compact region.  Every item takes an origin o, the centre of its rows' box,
+// and expresses rows and partners relative to it, split into hi = float(b)
+// and lo = float(b - hi).  Two pair forms:
+//   * near: separation (hi_j - hi_i) + (lo_j - lo_i) per axis (9 operations
+//     per pair for the three axes);
+//   * far: separation hi_j - hi_i (3 operations).  Its error per axis is at
+//     most 2^-24 (|a_i| + |b_j| + |d|) (the roundings of both hi values and of
+//     the difference), so relative to the separation d it is at most
+//     2^-24 (K + 1) with K = (|a_i| + |b_j|) / |d|.  A warp takes the far form
+//     for a group of 32 partners when K <= kFarK = 4 holds for every pair of
+//     its rows with that group, from boxes: K <= (rho_w + beta_g) / dist,
+//     rho_w = the largest |a_i| of the warp's rows, beta_g = the largest |b_j|
+//     of the group, dist = the distance between the rows' box and the group's
+//     box.  The far form thus adds at most 5 * 2^-24 = 3.0e-7 relative error
+//     to a pair's 1/r; every term of the sum is positive, so the halo's sum
+//     keeps that bound.
+// The two lanes of every packed register hold two partners j, 2q and 2q+1, of
+// the same row i, so a row's own coordinates are loop-invariant (hi_i, hi_i)
+// pairs.  Each thread owns R rows; the warp's rows are 32 R consecutive
+// members.  Partner tiles are 128 R wide, shared memory holds them as packed
+// pairs.  For every row, sixteen partner pairs (32 terms) are accumulated by a
+// fused multiply-add chain per lane, then enter a Kahan-compensated FP32 sum;
+// rows fold into FP64 per item.  Separations of exactly zero (coincident
+// members) are excluded like in the FP64 form: the fast loops do not test for
+// them -- rsqrt(0) = inf makes the row's sum non-finite, and the block then
+// recomputes the item with a per-pair test.  The tile shape (R = 1, 2 or 4
+// rows per thread) is chosen per halo-size bucket by the host-side autotuner
+// and read per item.
 typedef unsigned long long f2_t;
 
 __device__ __forceinline__ f2_t f2_pack(float a, float b) {
@@ -574,15 +754,20 @@ __device__ __forceinline__ float rsqrt_ftz(float x) {
 constexpr int kB32 = 128;              // threads per block of the FP32 form
 constexpr int kMaxR32 = 4;             // rows per thread, largest shape
 constexpr int kMaxT32 = kB32 * kMaxR32;
-constexpr int kGroup32 = 16;           // partner pairs per compensated fold
+constexpr int kGroup32 = 16;           // partner pairs per compensated fold (= one bound group of 32 partners)
 constexpr int kChunkJ = 32768;         // partners per item at most (a multiple of every tile width)
 constexpr float kFar = 1.0e18f;        // padding position: its terms vanish (mass 0, finite r)
+// far form when (rho_w + beta_g)^2 <= kFarK^2 dist^2; the factor below 16
+// covers the FP32 roundings of that test (a few 2^-24 relative)
+constexpr float kFarK2 = 16.0f * (1.0f - 1.0e-4f);
 
 struct Tile32 {
   float4 a[kMaxT32 / 2];  // hi x(2q), x(2q+1), y(2q), y(2q+1)
   float4 b[kMaxT32 / 2];  // hi z(2q), z(2q+1), mass(2q), mass(2q+1)
   float4 c[kMaxT32 / 2];  // lo x, x, y, y
   float2 d[kMaxT32 / 2];  // lo z, z
+  float4 glo[kMaxT32 / 32];  // per group of 32 partners: box low corner (x, y, z), largest |b| (w)
+  float4 ghi[kMaxT32 / 32];  // box high corner
 };
 
 __device__ __forceinline__ void split_hilo(double r, float& hi, float& lo) {
@@ -590,24 +775,50 @@ __device__ __forceinline__ void split_hilo(double r, float& hi, float& lo) {
   lo = (float)(r - (double)hi);
 }
 
-// Stage partners [j0, j0 + T) (T = 128 R) of one item; slots past j1 get the
-// padding (mass 0, far away).
+// Member k relative to the halo centre, and its mass: from the Morton-sorted
+// copy when there is one, else from the caller's arrays.
+__device__ __forceinline__ void member_rel(const HaloArgs& A, int64_t k, double cx, double cy, double cz, double& rx,
+                                           double& ry, double& rz, double& m) {
+  if (A.srel) {
+    const double4 v = A.srel[k];
+    rx = v.x; ry = v.y; rz = v.z; m = v.w;
+  } else {
+    rel_pos(A, k, cx, cy, cz, rx, ry, rz);
+    m = A.mass[k];
+  }
+}
+
+// |v| rounded up to float (the double norm's own rounding is covered by the
+// 1e-12 widening).
+__device__ __forceinline__ float norm_ru(double x, double y, double z) {
+  return __double2float_ru(sqrt(x * x + y * y + z * z) * (1.0 + 1e-12));
+}
+
+// Stage partners [j0, j0 + T) (T = 128 R) of one item relative to the origin
+// o, with the box and radius bound of every group of 32; slots past j1 get the
+// padding (mass 0, far away) and stay out of the bounds.
 template <int R>
 __device__ __forceinline__ void stage_tile32(Tile32& S, const HaloArgs& A, int64_t base, int32_t j0, int32_t j1,
-                                             double cx, double cy, double cz) {
-  constexpr int P = kB32 * R / 2;
+                                             double cx, double cy, double cz, double ox, double oy, double oz) {
+  constexpr int P = kB32 * R / 2;  // a multiple of 32: a warp is in or out of an iteration as a whole
   for (int q = threadIdx.x; q < P; q += kB32) {
     float hx[2], hy[2], hz[2], m[2], lx[2], ly[2], lz[2];
+    float blx = FLT_MAX, bly = FLT_MAX, blz = FLT_MAX, bhx = -FLT_MAX, bhy = -FLT_MAX, bhz = -FLT_MAX, bm = 0.f;
 #pragma unroll
     for (int l = 0; l < 2; ++l) {
       const int32_t j = j0 + 2 * q + l;
       if (j < j1) {
-        double rx, ry, rz;
-        rel_pos(A, base + j, cx, cy, cz, rx, ry, rz);
-        split_hilo(rx, hx[l], lx[l]);
-        split_hilo(ry, hy[l], ly[l]);
-        split_hilo(rz, hz[l], lz[l]);
-        m[l] = (float)A.mass[base + j];
+        double rx, ry, rz, mm;
+        member_rel(A, base + j, cx, cy, cz, rx, ry, rz, mm);
+        const double bx = rx - ox, by = ry - oy, bz = rz - oz;
+        split_hilo(bx, hx[l], lx[l]);
+        split_hilo(by, hy[l], ly[l]);
+        split_hilo(bz, hz[l], lz[l]);
+        m[l] = (float)mm;
+        blx = fminf(blx, __double2float_rd(bx)); bhx = fmaxf(bhx, __double2float_ru(bx));
+        bly = fminf(bly, __double2float_rd(by)); bhy = fmaxf(bhy, __double2float_ru(by));
+        blz = fminf(blz, __double2float_rd(bz)); bhz = fmaxf(bhz, __double2float_ru(bz));
+        bm = fmaxf(bm, norm_ru(bx, by, bz));
       } else {
         hx[l] = hy[l] = hz[l] = kFar;
         lx[l] = ly[l] = lz[l] = 0.f;
@@ -618,6 +829,21 @@ __device__ __forceinline__ void stage_tile32(Tile32& S, const HaloArgs& A, int64
     S.b[q] = make_float4(hz[0], hz[1], m[0], m[1]);
     S.c[q] = make_float4(lx[0], lx[1], ly[0], ly[1]);
     S.d[q] = make_float2(lz[0], lz[1]);
+    // the 16 lanes of a half warp stage one group of 32 partners
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) {
+      blx = fminf(blx, __shfl_xor_sync(0xffffffffu, blx, o));
+      bly = fminf(bly, __shfl_xor_sync(0xffffffffu, bly, o));
+      blz = fminf(blz, __shfl_xor_sync(0xffffffffu, blz, o));
+      bhx = fmaxf(bhx, __shfl_xor_sync(0xffffffffu, bhx, o));
+      bhy = fmaxf(bhy, __shfl_xor_sync(0xffffffffu, bhy, o));
+      bhz = fmaxf(bhz, __shfl_xor_sync(0xffffffffu, bhz, o));
+      bm = fmaxf(bm, __shfl_xor_sync(0xffffffffu, bm, o));
+    }
+    if ((q & 15) == 0) {
+      S.glo[q >> 4] = make_float4(blx, bly, blz, bm);
+      S.ghi[q >> 4] = make_float4(bhx, bhy, bhz, 0.f);
+    }
   }
 }
 
@@ -644,40 +870,98 @@ __device__ __forceinline__ void pair_checked(const Tile32& S, int jj, float hx, 
   if (r2 > 0.f) kahan_add(b[2 + l] * rsqrtf(r2), ks, kc);
 }
 
+__device__ __forceinline__ void warp_minmax_f(float& lo, float& hi) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+}
+
+// sred: 6 * (kB32 / 32) doubles of shared scratch for the origin.
 template <int R>
-__device__ double epot32_item(Tile32& S, double* sh, const HaloArgs& A, const PairItem& it, bool checked) {
+__device__ double epot32_item(Tile32& S, double* sh, double* sred, const HaloArgs& A, const PairItem& it,
+                              bool checked) {
   constexpr int T = kB32 * R;
-  const int tid = threadIdx.x;
+  constexpr int NW = kB32 / 32;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int64_t base = A.off[it.h];
   const int32_t n = (int32_t)(A.off[it.h + 1] - base);
   const double* cen = A.out + (size_t)kHaloFields * it.h;
   const double cx = cen[HP_PX], cy = cen[HP_PY], cz = cen[HP_PZ];
-  float hx[R], hy[R], hz[R], lx[R], ly[R], lz[R];
-  f2_t HX[R], HY[R], HZ[R], LX[R], LY[R], LZ[R], ks[R], kc[R];
-  float ksd[R], kcd[R];  // per-pair path sums
+  // rows: warp w owns the 32 R consecutive rows [32 R w, 32 R (w + 1)) of the
+  // item; they are read twice (for the origin, then relative to it) rather
+  // than held in registers across the block reduction
   bool vi[R];
+  double lo3[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi3[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    const int32_t i = it.i0 + tid + kB32 * r;
+    const int32_t i = it.i0 + 32 * R * wid + lane + 32 * r;
     vi[r] = i < n;
     if (vi[r]) {
-      double rx, ry, rz;
-      rel_pos(A, base + i, cx, cy, cz, rx, ry, rz);
-      split_hilo(rx, hx[r], lx[r]);
-      split_hilo(ry, hy[r], ly[r]);
-      split_hilo(rz, hz[r], lz[r]);
+      double rx, ry, rz, mm;
+      member_rel(A, base + i, cx, cy, cz, rx, ry, rz, mm);
+      lo3[0] = fmin(lo3[0], rx); hi3[0] = fmax(hi3[0], rx);
+      lo3[1] = fmin(lo3[1], ry); hi3[1] = fmax(hi3[1], ry);
+      lo3[2] = fmin(lo3[2], rz); hi3[2] = fmax(hi3[2], rz);
+    }
+  }
+  // origin: centre of the box of the item's rows
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo3[k] = fmin(lo3[k], __shfl_xor_sync(0xffffffffu, lo3[k], o));
+      hi3[k] = fmax(hi3[k], __shfl_xor_sync(0xffffffffu, hi3[k], o));
+    }
+    if (lane == 0) { sred[k * NW + wid] = lo3[k]; sred[(3 + k) * NW + wid] = hi3[k]; }
+  }
+  __syncthreads();
+  double o3[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    double l = sred[k * NW], h = sred[(3 + k) * NW];
+    for (int w = 1; w < NW; ++w) { l = fmin(l, sred[k * NW + w]); h = fmax(h, sred[(3 + k) * NW + w]); }
+    o3[k] = 0.5 * (l + h);
+  }
+  const double ox = o3[0], oy = o3[1], oz = o3[2];
+  f2_t HX[R], HY[R], HZ[R], LX[R], LY[R], LZ[R], ks[R], kc[R];
+  float ksd[R], kcd[R];  // per-pair path sums
+  // the warp's rows: box and radius bound about o (rounded outwards)
+  float wlx = FLT_MAX, wly = FLT_MAX, wlz = FLT_MAX, whx = -FLT_MAX, why = -FLT_MAX, whz = -FLT_MAX, wrho = 0.f;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    float hx, hy, hz, lx, ly, lz;
+    if (vi[r]) {
+      double rx, ry, rz, mm;
+      member_rel(A, base + it.i0 + 32 * R * wid + lane + 32 * r, cx, cy, cz, rx, ry, rz, mm);
+      const double bx = rx - ox, by = ry - oy, bz = rz - oz;
+      split_hilo(bx, hx, lx);
+      split_hilo(by, hy, ly);
+      split_hilo(bz, hz, lz);
+      wlx = fminf(wlx, __double2float_rd(bx)); whx = fmaxf(whx, __double2float_ru(bx));
+      wly = fminf(wly, __double2float_rd(by)); why = fmaxf(why, __double2float_ru(by));
+      wlz = fminf(wlz, __double2float_rd(bz)); whz = fmaxf(whz, __double2float_ru(bz));
+      wrho = fmaxf(wrho, norm_ru(bx, by, bz));
     } else {
       // far on the other side from the padding: every separation stays finite
-      hx[r] = hy[r] = hz[r] = -kFar;
-      lx[r] = ly[r] = lz[r] = 0.f;
+      hx = hy = hz = -kFar;
+      lx = ly = lz = 0.f;
     }
-    HX[r] = f2_pack(hx[r], hx[r]); HY[r] = f2_pack(hy[r], hy[r]); HZ[r] = f2_pack(hz[r], hz[r]);
-    LX[r] = f2_pack(lx[r], lx[r]); LY[r] = f2_pack(ly[r], ly[r]); LZ[r] = f2_pack(lz[r], lz[r]);
+    HX[r] = f2_pack(hx, hx); HY[r] = f2_pack(hy, hy); HZ[r] = f2_pack(hz, hz);
+    LX[r] = f2_pack(lx, lx); LY[r] = f2_pack(ly, ly); LZ[r] = f2_pack(lz, lz);
     ks[r] = kc[r] = 0ull;
     ksd[r] = kcd[r] = 0.f;
   }
+  warp_minmax_f(wlx, whx);
+  warp_minmax_f(wly, why);
+  warp_minmax_f(wlz, whz);
+  float dummy = 0.f;
+  warp_minmax_f(dummy, wrho);
+  // a warp without rows takes the far form: its sums are discarded
+  const bool wvalid = whx >= wlx;
   for (int32_t j0 = it.j0; j0 < it.j1; j0 += T) {
-    stage_tile32<R>(S, A, base, j0, it.j1, cx, cy, cz);
+    stage_tile32<R>(S, A, base, j0, it.j1, cx, cy, cz, ox, oy, oz);
     __syncthreads();
     const int jend = min(T, it.j1 - j0);
     if (j0 == it.i0 || checked) {
@@ -685,9 +969,11 @@ __device__ double epot32_item(Tile32& S, double* sh, const HaloArgs& A, const Pa
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         if (!vi[r]) continue;
-        const int jstart = (j0 == it.i0) ? tid + kB32 * r + 1 : 0;
-        for (int jj = jstart; jj < jend; ++jj)
-          pair_checked(S, jj, hx[r], hy[r], hz[r], lx[r], ly[r], lz[r], ksd[r], kcd[r]);
+        const int jstart = (j0 == it.i0) ? 32 * R * wid + lane + 32 * r + 1 : 0;
+        float hx, hy, hz, lx, ly, lz, t;
+        f2_unpack(HX[r], hx, t); f2_unpack(HY[r], hy, t); f2_unpack(HZ[r], hz, t);
+        f2_unpack(LX[r], lx, t); f2_unpack(LY[r], ly, t); f2_unpack(LZ[r], lz, t);
+        for (int jj = jstart; jj < jend; ++jj) pair_checked(S, jj, hx, hy, hz, lx, ly, lz, ksd[r], kcd[r]);
       }
     } else {
       const int np = ((jend + 2 * kGroup32 - 1) / (2 * kGroup32)) * kGroup32;  // partner pairs, padded
@@ -696,22 +982,46 @@ __device__ double epot32_item(Tile32& S, double* sh, const HaloArgs& A, const Pa
       const ulonglong2* Sc = reinterpret_cast<const ulonglong2*>(S.c);
       const f2_t* Sd = reinterpret_cast<const f2_t*>(S.d);
       for (int q0 = 0; q0 < np; q0 += kGroup32) {
+        const float4 gl = S.glo[q0 / kGroup32], gh = S.ghi[q0 / kGroup32];
+        const float gx = fmaxf(0.f, fmaxf(gl.x - whx, wlx - gh.x));
+        const float gy = fmaxf(0.f, fmaxf(gl.y - why, wly - gh.y));
+        const float gz = fmaxf(0.f, fmaxf(gl.z - whz, wlz - gh.z));
+        const float dist2 = gx * gx + gy * gy + gz * gz;
+        const float num = wrho + gl.w;
+        const bool far = !wvalid || (dist2 > 0.f && num * num <= kFarK2 * dist2);
         f2_t acc[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) acc[r] = 0ull;
+        if (far) {
 #pragma unroll
-        for (int g = 0; g < kGroup32; ++g) {
-          const ulonglong2 pa = Sa[q0 + g], pb = Sb[q0 + g], pc = Sc[q0 + g];
-          const f2_t pd = Sd[q0 + g];
+          for (int g = 0; g < kGroup32; ++g) {
+            const ulonglong2 pa = Sa[q0 + g], pb = Sb[q0 + g];
 #pragma unroll
-          for (int r = 0; r < R; ++r) {
-            const f2_t dx = f2_add(f2_sub(pa.x, HX[r]), f2_sub(pc.x, LX[r]));
-            const f2_t dy = f2_add(f2_sub(pa.y, HY[r]), f2_sub(pc.y, LY[r]));
-            const f2_t dz = f2_add(f2_sub(pb.x, HZ[r]), f2_sub(pd, LZ[r]));
-            const f2_t r2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_mul(dz, dz)));
-            float u, v;
-            f2_unpack(r2, u, v);
-            acc[r] = f2_fma(pb.y, f2_pack(rsqrt_ftz(u), rsqrt_ftz(v)), acc[r]);
+            for (int r = 0; r < R; ++r) {
+              const f2_t dx = f2_sub(pa.x, HX[r]);
+              const f2_t dy = f2_sub(pa.y, HY[r]);
+              const f2_t dz = f2_sub(pb.x, HZ[r]);
+              const f2_t r2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_mul(dz, dz)));
+              float u, v;
+              f2_unpack(r2, u, v);
+              acc[r] = f2_fma(pb.y, f2_pack(rsqrt_ftz(u), rsqrt_ftz(v)), acc[r]);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int g = 0; g < kGroup32; ++g) {
+            const ulonglong2 pa = Sa[q0 + g], pb = Sb[q0 + g], pc = Sc[q0 + g];
+            const f2_t pd = Sd[q0 + g];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const f2_t dx = f2_add(f2_sub(pa.x, HX[r]), f2_sub(pc.x, LX[r]));
+              const f2_t dy = f2_add(f2_sub(pa.y, HY[r]), f2_sub(pc.y, LY[r]));
+              const f2_t dz = f2_add(f2_sub(pb.x, HZ[r]), f2_sub(pd, LZ[r]));
+              const f2_t r2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_mul(dz, dz)));
+              float u, v;
+              f2_unpack(r2, u, v);
+              acc[r] = f2_fma(pb.y, f2_pack(rsqrt_ftz(u), rsqrt_ftz(v)), acc[r]);
+            }
           }
         }
 #pragma unroll
@@ -733,7 +1043,9 @@ __device__ double epot32_item(Tile32& S, double* sh, const HaloArgs& A, const Pa
     f2_unpack(ks[r], s0, s1);
     f2_unpack(kc[r], c0, c1);
     const double row = (((double)s0 - (double)c0) + ((double)s1 - (double)c1)) + ((double)ksd[r] - (double)kcd[r]);
-    mine += A.mass[base + it.i0 + tid + kB32 * r] * row;
+    double rx, ry, rz, mm;
+    member_rel(A, base + it.i0 + 32 * R * wid + lane + 32 * r, cx, cy, cz, rx, ry, rz, mm);
+    mine += mm * row;
   }
   return block_sum<double, kB32>(mine, sh);
 }
@@ -747,6 +1059,7 @@ __global__ void __launch_bounds__(kB32, 4) epot32_kernel(HaloArgs A, const PairI
                                                          double* __restrict__ part) {
   __shared__ Tile32 S;
   __shared__ double sh[kB32 / 32];
+  __shared__ double sred[6 * (kB32 / 32)];
   __shared__ int32_t s_item;
   const int tid = threadIdx.x;
   for (;;) {
@@ -758,17 +1071,67 @@ __global__ void __launch_bounds__(kB32, 4) epot32_kernel(HaloArgs A, const PairI
     const PairItem it = items[w];
     const int code = hshape ? (int)hshape[it.h] : fixed_code;
     double tot;
-    if (code == 2) tot = epot32_item<4>(S, sh, A, it, false);
-    else if (code == 1) tot = epot32_item<2>(S, sh, A, it, false);
-    else tot = epot32_item<1>(S, sh, A, it, false);
+    if (code == 2) tot = epot32_item<4>(S, sh, sred, A, it, false);
+    else if (code == 1) tot = epot32_item<2>(S, sh, sred, A, it, false);
+    else tot = epot32_item<1>(S, sh, sred, A, it, false);
     // a zero separation in the fast path shows as a non-finite sum: recompute
     // the item with the per-pair test (block-uniform decision)
     if (__syncthreads_or(tid == 0 && !isfinite(tot))) {
-      if (code == 2) tot = epot32_item<4>(S, sh, A, it, true);
-      else if (code == 1) tot = epot32_item<2>(S, sh, A, it, true);
-      else tot = epot32_item<1>(S, sh, A, it, true);
+      if (code == 2) tot = epot32_item<4>(S, sh, sred, A, it, true);
+      else if (code == 1) tot = epot32_item<2>(S, sh, sred, A, it, true);
+      else tot = epot32_item<1>(S, sh, sred, A, it, true);
     }
     if (tid == 0) part[w] = tot;
+  }
+}
+
+// ---- Morton-sorted member copy for the FP32-compensated form
+// Members of every halo ordered by the Morton key of their position about the
+// halo centre (10 bits per axis over the halo's largest radius), stored as
+// (x, y, z relative to the centre, mass).  The key's high bits are the halo,
+// so a halo's members stay in its own range [off[h], off[h+1]).
+__device__ __forceinline__ unsigned spread10(unsigned v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x30000ffu;
+  v = (v | (v << 8)) & 0x300f00fu;
+  v = (v | (v << 4)) & 0x30c30c3u;
+  v = (v | (v << 2)) & 0x9249249u;
+  return v;
+}
+
+__device__ __forceinline__ unsigned quant10(double r, double inv) {
+  const double u = fmin(fmax((r * inv + 1.0) * 512.0, 0.0), 1023.0);
+  return (unsigned)u;
+}
+
+__global__ void __launch_bounds__(kPB) sort32_keys_kernel(HaloArgs A, const MomChunk* __restrict__ ch,
+                                                          unsigned long long* __restrict__ key,
+                                                          int32_t* __restrict__ val) {
+  const MomChunk c = ch[blockIdx.x];
+  const double* o = A.out + (size_t)kHaloFields * c.h;
+  const double cx = o[HP_PX], cy = o[HP_PY], cz = o[HP_PZ], rr = o[HP_R];
+  const double inv = rr > 0.0 ? 1.0 / (rr * (1.0 + 1e-9)) : 0.0;
+  for (int64_t k = c.b0 + threadIdx.x; k < c.b1; k += kPB) {
+    double rx, ry, rz;
+    rel_pos(A, k, cx, cy, cz, rx, ry, rz);
+    const unsigned m =
+        (spread10(quant10(rx, inv)) << 2) | (spread10(quant10(ry, inv)) << 1) | spread10(quant10(rz, inv));
+    key[k] = ((unsigned long long)c.h << 30) | m;
+    val[k] = (int32_t)k;
+  }
+}
+
+__global__ void __launch_bounds__(kPB) sort32_gather_kernel(HaloArgs A, const MomChunk* __restrict__ ch,
+                                                            const int32_t* __restrict__ val,
+                                                            double4* __restrict__ srel) {
+  const MomChunk c = ch[blockIdx.x];
+  const double* o = A.out + (size_t)kHaloFields * c.h;
+  const double cx = o[HP_PX], cy = o[HP_PY], cz = o[HP_PZ];
+  for (int64_t q = c.b0 + threadIdx.x; q < c.b1; q += kPB) {
+    const int64_t k = val[q];
+    double rx, ry, rz;
+    rel_pos(A, k, cx, cy, cz, rx, ry, rz);
+    srel[q] = make_double4(rx, ry, rz, A.mass[k]);
   }
 }
 
@@ -913,8 +1276,10 @@ struct ListBufs {
 
 struct GraphSig {
   HaloArgs A;
-  const void* ptr[15];
-  int64_t nch;
+  const void* ptr[21];
+  int64_t nch, nmem;
+  size_t scub_bytes;
+  int32_t sort_end_bit, pad2;
   int64_t nhalo;
   int32_t n64, n32, grid64, grid32, epot, pad;
 };
@@ -923,8 +1288,14 @@ struct HaloEngine {
   DevBuf d_off, d_pos, d_vel, d_mass, d_dens, d_out;  // staging for host inputs
   ListBufs l64, l32, tune;
   DevBuf d_hshape, d_counter, d_err;
-  DevBuf d_mch, d_mcoff, d_mp1, d_mp2, d_mcen;  // chunked moment passes
+  DevBuf d_mch, d_mcoff, d_mp1, d_mp2, d_mcen, d_marg;  // chunked moment passes
+  DevBuf d_index;                                        // staging of the host entry point's member indices
   int64_t nch = 0;
+  // Morton-sorted member copy of the FP32-compensated form
+  DevBuf d_skey, d_skey2, d_sval, d_sval2, d_srel, d_scub;
+  size_t scub_bytes = 0;
+  int64_t nmem = 0;
+  int sort_end_bit = 31;
   cudaEvent_t ev[5] = {};
   cudaEvent_t ev_in = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
   bool ready = false;
@@ -1044,6 +1415,47 @@ static int tune_buckets(HaloEngine& H, const HaloArgs& A, const int64_t* h_off, 
   return AHOP_OK;
 }
 
+// Buffers of the Morton-sorted member copy (keys, values, CUB scratch, the
+// copy itself) for nmem members of nhalo halos.
+static int ensure_sort32(HaloEngine& H, int64_t nhalo, int64_t nmem, cudaStream_t st) {
+  if (nmem > INT32_MAX) { set_error("more than 2^31 - 1 members in one call"); return AHOP_EINVAL; }
+  H.nmem = nmem;
+  int hb = 1;
+  while ((int64_t(1) << hb) < nhalo) ++hb;
+  H.sort_end_bit = 30 + hb;
+  const size_t m = (size_t)std::max<int64_t>(nmem, 1);
+  AHOP_CUDA_TRY(H.d_skey.ensure(m * 8));
+  AHOP_CUDA_TRY(H.d_skey2.ensure(m * 8));
+  AHOP_CUDA_TRY(H.d_sval.ensure(m * 4));
+  AHOP_CUDA_TRY(H.d_sval2.ensure(m * 4));
+  AHOP_CUDA_TRY(H.d_srel.ensure(m * 32));
+  size_t tmp = 0;
+  AHOP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp, H.d_skey.as<unsigned long long>(),
+                                                H.d_skey2.as<unsigned long long>(), H.d_sval.as<int32_t>(),
+                                                H.d_sval2.as<int32_t>(), (int)m, 0, H.sort_end_bit, st));
+  AHOP_CUDA_TRY(H.d_scub.ensure(std::max<size_t>(tmp, 16)));
+  H.scub_bytes = tmp;
+  return AHOP_OK;
+}
+
+// Morton keys about each halo centre (needs the centres and radii in A.out),
+// one radix sort, then the sorted copy A.srel.
+static int enqueue_sort32(HaloEngine& H, const HaloArgs& A, cudaStream_t s, int* launches) {
+  if (H.nch == 0 || H.nmem == 0) return AHOP_OK;
+  sort32_keys_kernel<<<(unsigned)H.nch, kPB, 0, s>>>(A, H.d_mch.as<MomChunk>(), H.d_skey.as<unsigned long long>(),
+                                                     H.d_sval.as<int32_t>());
+  AHOP_CUDA_TRY(cudaGetLastError());
+  size_t tmp = H.scub_bytes;
+  AHOP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(H.d_scub.p, tmp, H.d_skey.as<unsigned long long>(),
+                                                H.d_skey2.as<unsigned long long>(), H.d_sval.as<int32_t>(),
+                                                H.d_sval2.as<int32_t>(), (int)H.nmem, 0, H.sort_end_bit, s));
+  sort32_gather_kernel<<<(unsigned)H.nch, kPB, 0, s>>>(A, H.d_mch.as<MomChunk>(), H.d_sval2.as<int32_t>(),
+                                                       H.d_srel.as<double4>());
+  AHOP_CUDA_TRY(cudaGetLastError());
+  if (launches) *launches += 3;
+  return AHOP_OK;
+}
+
 // The device work of one call, in stream order; `capture` marks the timing
 // events as graph nodes.
 static int enqueue_props(HaloEngine& H, const HaloArgs& A, int64_t nhalo, int epot, int grid64, int grid32,
@@ -1062,6 +1474,13 @@ static int enqueue_props(HaloEngine& H, const HaloArgs& A, int64_t nhalo, int ep
     mom_fold1_kernel<<<hb, 128, 0, s>>>(A, H.d_mcoff.as<int64_t>(), H.d_mp1.as<MomP1>(), H.d_mcen.as<MomCentre>(),
                                         nhalo);
     ++*launches;
+    if (A.cdm && H.nch > 0) {
+      mom_cdm_kernel<<<(unsigned)H.nch, kPB, 0, s>>>(A, H.d_mch.as<MomChunk>(), H.d_mcen.as<MomCentre>(),
+                                                     H.d_marg.as<MomArg>());
+      mom_cdm_fold_kernel<<<hb, 128, 0, s>>>(A, H.d_mcoff.as<int64_t>(), H.d_marg.as<MomArg>(),
+                                             H.d_mcen.as<MomCentre>(), nhalo);
+      *launches += 2;
+    }
     if (A.sc) {
       mom_sc_kernel<<<(unsigned)nhalo, kPB, 0, s>>>(A, H.d_mcen.as<MomCentre>());
       ++*launches;
@@ -1085,6 +1504,9 @@ static int enqueue_props(HaloEngine& H, const HaloArgs& A, int64_t nhalo, int ep
   }
   AHOP_CUDA_TRY(cudaEventRecordWithFlags(H.ev[2], s, flags));
   if ((epot & 2) && H.l32.n > 0) {
+    // the sort belongs to the FP32-compensated form and is timed with it
+    int rc;
+    if ((rc = enqueue_sort32(H, A, s, launches))) return rc;
     epot32_kernel<<<grid32, kB32, 0, s>>>(A, H.l32.items.as<PairItem>(), H.d_hshape.as<int8_t>(), kDefaultShape,
                                           H.l32.n, H.d_counter.as<int32_t>() + 1, H.l32.part.as<double>());
     ++*launches;
@@ -1130,11 +1552,28 @@ static int halo_run(HaloEngine& H, const AhopHaloParams* p, const int64_t* d_off
   A.off = d_off; A.pos = d_pos; A.vel = d_vel; A.mass = d_mass; A.dens = d_dens; A.out = d_out;
   A.L = p->Lbox; A.h = 0.5 * p->Lbox; A.hub = p->Hub_pt; A.G = p->gravconst; A.periodic = p->periodic != 0;
   A.sc = p->sc != 0; A.dcell_min = p->dcell_min; A.eps_sc = p->eps_sc;
+  A.cdm = p->cdm != 0; A.ndm = p->ndm; A.massp = p->massp; A.index = p->index;
   AHOP_CUDA_TRY(H.d_err.ensure(16));
   AHOP_CUDA_TRY(H.d_counter.ensure(16));
   A.err = H.d_err.as<int>();
   const int epot = p->epot & 3;
   int rc;
+  // chunks of the moment passes (also the blocks of the member sort)
+  std::vector<MomChunk> mch;
+  std::vector<int64_t> mcoff(nhalo + 1, 0);
+  for (int64_t h = 0; h < nhalo; ++h) {
+    mcoff[h] = (int64_t)mch.size();
+    for (int64_t b = h_off[h]; b < h_off[h + 1]; b += kMomChunk)
+      mch.push_back(MomChunk{(int32_t)h, 0, b, std::min<int64_t>(h_off[h + 1], b + kMomChunk)});
+  }
+  mcoff[nhalo] = (int64_t)mch.size();
+  H.nch = (int64_t)mch.size();
+  if ((rc = upload(H.d_mch, mch, st))) return rc;
+  if ((rc = upload(H.d_mcoff, mcoff, st))) return rc;
+  if (epot & 2) {
+    if ((rc = ensure_sort32(H, nhalo, nhalo > 0 ? h_off[nhalo] - h_off[0] : 0, st))) return rc;
+    A.srel = H.d_srel.as<double4>();
+  }
   float tune_total = 0.f;
   if (epot & 2) {
     // shapes for this call's buckets; the tuner needs the centres first
@@ -1148,6 +1587,7 @@ static int halo_run(HaloEngine& H, const AhopHaloParams* p, const int64_t* d_off
       AHOP_CUDA_TRY(cudaMemsetAsync(H.d_err.p, 0, 4, st));
       halo_moments_kernel<<<(unsigned)nhalo, kPB, 0, st>>>(A);
       AHOP_CUDA_TRY(cudaGetLastError());
+      if ((rc = enqueue_sort32(H, A, st, nullptr))) return rc;
       if ((rc = tune_buckets(H, A, h_off, nhalo, st))) return rc;
       tune_total = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
@@ -1175,20 +1615,9 @@ static int halo_run(HaloEngine& H, const AhopHaloParams* p, const int64_t* d_off
   H.L32.hoff[nhalo] = (int64_t)H.L32.items.size();
   schedule(H.L64);
   schedule(H.L32);
-  // chunks of the moment passes
-  std::vector<MomChunk> mch;
-  std::vector<int64_t> mcoff(nhalo + 1, 0);
-  for (int64_t h = 0; h < nhalo; ++h) {
-    mcoff[h] = (int64_t)mch.size();
-    for (int64_t b = h_off[h]; b < h_off[h + 1]; b += kMomChunk)
-      mch.push_back(MomChunk{(int32_t)h, 0, b, std::min<int64_t>(h_off[h + 1], b + kMomChunk)});
-  }
-  mcoff[nhalo] = (int64_t)mch.size();
-  H.nch = (int64_t)mch.size();
-  if ((rc = upload(H.d_mch, mch, st))) return rc;
-  if ((rc = upload(H.d_mcoff, mcoff, st))) return rc;
   AHOP_CUDA_TRY(H.d_mp1.ensure(std::max<size_t>(mch.size() * sizeof(MomP1), 16)));
   AHOP_CUDA_TRY(H.d_mp2.ensure(std::max<size_t>(mch.size() * sizeof(MomP2), 16)));
+  AHOP_CUDA_TRY(H.d_marg.ensure(std::max<size_t>(mch.size() * sizeof(MomArg), 16)));
   AHOP_CUDA_TRY(H.d_mcen.ensure(std::max<size_t>((size_t)nhalo * sizeof(MomCentre), 16)));
   if ((rc = upload_list(H.l64, H.L64, st))) return rc;
   if ((rc = upload_list(H.l32, H.L32, st))) return rc;
@@ -1203,11 +1632,16 @@ static int halo_run(HaloEngine& H, const AhopHaloParams* p, const int64_t* d_off
     GraphSig sig;
     memset(&sig, 0, sizeof sig);
     sig.A = A;
-    const void* ptrs[15] = {H.l64.items.p, H.l64.order.p, H.l64.hoff.p, H.l64.part.p, H.l32.items.p,
+    const void* ptrs[21] = {H.l64.items.p, H.l64.order.p, H.l64.hoff.p, H.l64.part.p, H.l32.items.p,
                             H.l32.order.p, H.l32.hoff.p, H.l32.part.p, H.d_hshape.p, H.d_counter.p,
-                            H.d_mch.p,     H.d_mcoff.p,   H.d_mp1.p,    H.d_mp2.p,    H.d_mcen.p};
+                            H.d_mch.p,     H.d_mcoff.p,   H.d_mp1.p,    H.d_mp2.p,    H.d_mcen.p,
+                            H.d_skey.p,    H.d_skey2.p,   H.d_sval.p,   H.d_sval2.p,  H.d_scub.p,
+                            H.d_marg.p};
     memcpy(sig.ptr, ptrs, sizeof ptrs);
     sig.nch = H.nch;
+    sig.nmem = H.nmem;
+    sig.scub_bytes = H.scub_bytes;
+    sig.sort_end_bit = H.sort_end_bit;
     sig.nhalo = nhalo; sig.n64 = H.l64.n; sig.n32 = H.l32.n; sig.grid64 = grid64; sig.grid32 = grid32;
     sig.epot = epot;
     if (!H.gexec || memcmp(&sig, &H.gsig, sizeof sig) != 0) {
@@ -1300,7 +1734,13 @@ int ahop_halo_props(const AhopHaloParams* p, const int64_t* off, int64_t nhalo, 
   AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_vel.p, vel, n * 24, cudaMemcpyHostToDevice, st));
   AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_mass.p, mass, n * 8, cudaMemcpyHostToDevice, st));
   AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_dens.p, density, n * 8, cudaMemcpyHostToDevice, st));
-  if ((rc = halo_run(H, p, H.d_off.as<int64_t>(), off, nhalo, H.d_pos.as<double>(), H.d_vel.as<double>(),
+  AhopHaloParams pd = *p;  // the member indices move to the device with the other inputs
+  if (p->index) {
+    AHOP_CUDA_TRY(H.d_index.ensure(n * 4 + 8));
+    AHOP_CUDA_TRY(cudaMemcpyAsync(H.d_index.p, p->index, n * 4, cudaMemcpyHostToDevice, st));
+    pd.index = H.d_index.as<int32_t>();
+  }
+  if ((rc = halo_run(H, &pd, H.d_off.as<int64_t>(), off, nhalo, H.d_pos.as<double>(), H.d_vel.as<double>(),
                      H.d_mass.as<double>(), H.d_dens.as<double>(), H.d_out.as<double>(), st)))
     return rc;
   AHOP_CUDA_TRY(cudaMemcpyAsync(out, H.d_out.p, (size_t)nhalo * kHaloFields * 8, cudaMemcpyDeviceToHost, st));
@@ -1496,6 +1936,7 @@ extern "C" int ahop_halo_props_noalloc(const AhopHaloParams* p, const int64_t* d
   A.off = d_off; A.pos = d_pos; A.vel = d_vel; A.mass = d_mass; A.dens = d_density; A.out = d_out;
   A.L = p->Lbox; A.h = 0.5 * p->Lbox; A.hub = p->Hub_pt; A.G = p->gravconst; A.periodic = p->periodic != 0;
   A.sc = p->sc != 0; A.dcell_min = p->dcell_min; A.eps_sc = p->eps_sc;
+  A.cdm = p->cdm != 0; A.ndm = p->ndm; A.massp = p->massp; A.index = p->index;
   A.err = &S->counter[3];
   halo_moments_kernel<<<(unsigned)nhalo, kPB, 0, st>>>(A);
   AHOP_CUDA_TRY(cudaGetLastError());

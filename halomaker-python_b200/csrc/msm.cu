@@ -409,6 +409,19 @@ extern "C" int ahop_structure_members(int32_t* nstructs, int64_t* nmembers) {
   return AHOP_OK;
 }
 
+extern "C" int ahop_gather_member_index_device(int32_t* d_index, void* stream) {
+  Engine& E = engine();
+  MsmState& S = msm_state();
+  if (!S.have || !E.have_result) { set_error("no selection (call ahop_select_msm first)"); return AHOP_ESTATE; }
+  if (!d_index && S.nmembers > 0) { set_error("null device buffer"); return AHOP_EINVAL; }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  AHOP_CUDA_TRY(cudaStreamSynchronize(E.stream));
+  if (S.nmembers > 0)
+    AHOP_CUDA_TRY(cudaMemcpyAsync(d_index, S.d_val2.as<int32_t>() + (S.n - S.nmembers),
+                                  (size_t)S.nmembers * 4, cudaMemcpyDeviceToDevice, st));
+  return AHOP_OK;
+}
+
 extern "C" int ahop_gather_members_device(const double* d_pos, const double* d_vel, const double* d_mass,
                                           int64_t* d_off, int32_t* d_ids, double* d_gpos, double* d_gvel,
                                           double* d_gmass, double* d_gdens, void* stream) {

@@ -201,6 +201,11 @@ int ahop_structure_members(int32_t* nstructs, int64_t* nmembers);
 int ahop_gather_members_device(const double* d_pos, const double* d_vel, const double* d_mass, int64_t* d_off,
                                int32_t* d_ids, double* d_gpos, double* d_gvel, double* d_gmass, double* d_gdens,
                                void* stream);
+/* The particle index (0-based, caller's order; the reference's indexps) of
+ * every gathered member, in the same structure order, into d_index[nmembers]
+ * on `stream`: with ahop_halo_props' index/ndm it splits dark matter from
+ * stars (CHP:766, 962). */
+int ahop_gather_member_index_device(int32_t* d_index, void* stream);
 
 /* ---- RAMSES particle reader --------------------------------------------------
  * Replaces _read_ramses_new_1010 (src/input_output.py:624-760) and the
@@ -231,16 +236,20 @@ int ahop_ramses_close(void);
 
 /* ---- batched halo properties ------------------------------------------------
  * Replaces the per-halo reductions of src/compute_halo_props.py run by
- * _compute_halo_props (CHP:270-301): det_mass_17, det_center_18 (densest
- * member as centre, cdm=False), compute_ang_mom_19, r_halos_1a,
+ * _compute_halo_props (CHP:270-301): det_mass_17 (with the dark-matter /
+ * star split of mode 'full', CHP:766-780), det_center_18 (densest member, or
+ * with cdm the member closest to the centre of mass, CHP:917-936; sigma_dm and
+ * sigma* of CHP:962-966), compute_ang_mom_19, r_halos_1a,
  * det_inertial_tensor_1b20 + det_main_axis_1b2, det_halo_energies_1b3 (E_kin
  * with Hubble flow; E_pot as the direct pair sum for every halo size) and
  * compute_spin_parameter_1c.  Members of halo h are rows [off[h], off[h+1]).
- * Each halo gets AHOP_HALO_NFIELDS doubles, indexed by the HP_* constants. */
+ * Each halo gets AHOP_HALO_NFIELDS doubles, indexed by the HP_* constants
+ * (counts as doubles). */
 enum {
   HP_M = 0, HP_PX, HP_PY, HP_PZ, HP_VX, HP_VY, HP_VZ, HP_LX, HP_LY, HP_LZ, HP_R,
   HP_IXX, HP_IXY, HP_IXZ, HP_IYY, HP_IYZ, HP_IZZ, HP_EK, HP_EP64, HP_EP32C, HP_SIGMA,
-  HP_SHA, HP_SHB, HP_SHC, HP_SPIN64, HP_SPIN32C, HP_ICENTER, AHOP_HALO_NFIELDS
+  HP_SHA, HP_SHB, HP_SHC, HP_SPIN64, HP_SPIN32C, HP_ICENTER,
+  HP_NDM, HP_NSTAR, HP_MDM, HP_MSTAR, HP_MCONTAM, HP_SIGMA_DM, HP_SIGMA_STAR, AHOP_HALO_NFIELDS
 };
 
 typedef struct {
@@ -253,6 +262,13 @@ typedef struct {
   int32_t pad;
   double dcell_min; /* H.dcell_min: smallest sphere radius */
   double eps_sc;    /* H.eps_SC: radius shrink factor per step, in (0, 1) when sc is on */
+  int32_t cdm;      /* H.cdm: centre = member closest to the centre of mass instead of the densest one */
+  int32_t pad2;
+  int64_t ndm;      /* H.ndm: a member whose particle index is below ndm is dark matter (CHP:766, 962) */
+  double massp;     /* H.massp: dark-matter members heavier than massp * 1.00001 are contamination (CHP:768) */
+  const int32_t* index; /* particle index of every member (the reference's indexps), in the same memory as
+                           the call's other arrays (host for ahop_halo_props, device otherwise); NULL: every
+                           member is dark matter */
 } AhopHaloParams;
 
 typedef struct {

@@ -18,7 +18,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _lib = None
 
 FIELDS = ["m", "px", "py", "pz", "vx", "vy", "vz", "Lx", "Ly", "Lz", "r", "Ixx", "Ixy", "Ixz", "Iyy", "Iyz",
-          "Izz", "ek", "ep64", "ep32c", "sigma", "sha", "shb", "shc", "spin64", "spin32c", "icenter"]
+          "Izz", "ek", "ep64", "ep32c", "sigma", "sha", "shb", "shc", "spin64", "spin32c", "icenter",
+          "ndm", "nstar", "mdm", "m*", "mcontam", "sigma_dm", "sigma*"]
 
 
 def lib():
@@ -77,16 +78,31 @@ def shrink_sphere(p, m, c, L, periodic, dcell_min, eps_sc):
         return int(np.argmin(offs(xc, yc, zc)[3]))
 
 
-def props(off, pos, vel, mass, dens, L, hub, G=430.1, periodic=True, epot=True, nthreads=None, sc=None):
+def props(off, pos, vel, mass, dens, L, hub, G=430.1, periodic=True, epot=True, nthreads=None, sc=None, cdm=False,
+          index=None, ndm=None, massp=0.0):
     """Per-halo fields as a dict of arrays (names as in FIELDS, ep = FP64 pair sum).
-    sc = (dcell_min, eps_SC) refines the centre with the shrinking sphere."""
+    sc = (dcell_min, eps_SC) refines the centre with the shrinking sphere;
+    cdm: the centre is the member closest to the centre of mass (CHP:917-934);
+    index/ndm/massp: det_mass_17's dark-matter / star split (CHP:766-780),
+    every member dark matter when index is None."""
     nh = len(off) - 1
     res = {f: np.zeros(nh) for f in FIELDS}
     for h in range(nh):
         a, b = off[h], off[h + 1]
         p, v, m, d = pos[a:b], vel[a:b], mass[a:b], dens[a:b]
         mt = np.sum(m)
-        ic = int(np.argmax(d))
+        dmm = np.ones(b - a, bool) if index is None else np.asarray(index[a:b]) < ndm
+        res["ndm"][h], res["nstar"][h] = np.count_nonzero(dmm), np.count_nonzero(~dmm)
+        res["mdm"][h], res["m*"][h] = np.sum(m[dmm]), np.sum(m[~dmm])
+        idm = m[dmm]
+        res["mcontam"][h] = np.sum(idm[idm > massp * 1.00001])
+        if cdm and b > a:
+            w = lambda x: _wrap(x, L) if periodic else x
+            pc = np.array([np.sum(m * w(p[:, k] - p[0, k])) / mt + p[0, k] for k in range(3)])
+            pc = np.array([w(np.array([x]))[0] for x in pc])
+            ic = int(np.argmin(sum(w(p[:, k] - pc[k]) ** 2 for k in range(3))))
+        else:
+            ic = int(np.argmax(d))
         if sc is not None:
             j = shrink_sphere(p, m, p[ic], L, periodic, sc[0], sc[1])
             if j is not None:
@@ -109,7 +125,10 @@ def props(off, pos, vel, mass, dens, L, hub, G=430.1, periodic=True, epot=True, 
         for k, f in enumerate(["Ixx", "Ixy", "Ixz", "Iyy", "Iyz", "Izz"]):
             res[f][h] = I[[0, 0, 0, 1, 1, 2][k], [0, 1, 2, 1, 2, 2][k]]
         res["ek"][h] = 0.5 * np.sum(m * np.sum(t * t, 1))
-        res["sigma"][h] = np.sqrt(np.sum(m * np.sum(u * u, 1)) / mt)
+        dv2 = m * np.sum(u * u, 1)
+        res["sigma"][h] = np.sqrt(np.sum(dv2) / mt)
+        res["sigma_dm"][h] = np.sqrt(np.sum(dv2[dmm]) / res["mdm"][h]) if res["mdm"][h] > 0 else 0.0
+        res["sigma*"][h] = np.sqrt(np.sum(dv2[~dmm]) / res["m*"][h]) if res["m*"][h] > 0 else 0.0
         res["sha"][h], res["shb"][h], res["shc"][h] = np.sqrt(ev / mt)
         res["icenter"][h] = ic
     if epot:

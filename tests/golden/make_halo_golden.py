@@ -11,6 +11,12 @@ potential (CHP:1413-1427); larger ones get its ellipsoid formula
 (CHP:1405-1412), which the batched kernel does not compute (it sums pairs for
 every size), so for those only the O(n) fields are compared.
 
+A second case (halo_case_stars.npz) runs the same chain in mode 'full' with
+H.cdm = True on halos that hold stars (particle indices at or above H.ndm) and
+contaminating heavy dark-matter members: det_mass_17's ndm, nstar, mdm, m*,
+mcontam (CHP:766-780), det_center_18's centre of mass and closest member
+(CHP:917-934) and its sigma_dm / sigma* (CHP:962-966).
+
 Usage (where the reference is mounted): python tests/golden/make_halo_golden.py /path/to/reference
 """
 import os
@@ -23,6 +29,7 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 
 FIELDS = ["m", "px", "py", "pz", "vx", "vy", "vz", "Lx", "Ly", "Lz", "r", "sha", "shb", "shc", "ek", "ep",
           "et", "spin", "sigma"]
+STAR_FIELDS = FIELDS + ["ndm", "nstar", "mdm", "m*", "mcontam", "sigma_dm", "sigma*"]
 
 
 def main(refroot):
@@ -79,11 +86,46 @@ def main(refroot):
         CHP.det_halo_energies_1b3(rec, member=member)
         CHP.compute_spin_parameter_1c(rec)
         out[h] = [rec[f] for f in FIELDS]
-    for name in list(H.mem.keys()):
-        H.deallocate(name)
     np.savez_compressed(os.path.join(HERE, "halo_case.npz"), off=off, pos=pos, vel=vel, mass=mass, dens=dens,
                         out=out, fields=np.array(FIELDS), Lbox=box, Hub_pt=70.0, gravconst=430.1)
     print("halo_case", nh, "halos", int(off[-1]), "members")
+
+    # stars and contamination, centre of mass (cdm)
+    H.cdm = True
+    H.massp = 0.8
+    ndm = 1_000_000
+    index = np.empty(len(mass), np.int64)
+    mass2 = mass.copy()
+    for h in range(nh):
+        a, b = off[h], off[h + 1]
+        k = b - a
+        star = rng.random(k) < 0.3
+        # particle ids: dark matter below ndm, stars at or above it (indexps < H.ndm is the mask)
+        index[a:b] = np.where(star, ndm + rng.integers(0, 10**6, k), rng.integers(0, ndm, k))
+        mass2[a:b] = np.where(star, 0.1 * mass[a:b], mass[a:b])
+    H.ndm = ndm
+    out2 = np.zeros((nh, len(STAR_FIELDS)))
+    for h in range(nh):
+        a, b = off[h], off[h + 1]
+        member = (np.int32(b - a), index[a:b].copy(), pos[a:b].copy(), vel[a:b].copy(), mass2[a:b].copy(),
+                  dens[a:b].copy())
+        rec = np.zeros(1, dtype=H.halo_dtype)[0]
+        rec["nmem"] = b - a
+        CHP.det_mass_17(rec, member=member)
+        CHP.det_center_18(rec, member=member)
+        CHP.refine_centers_1b(rec, member=member)
+        CHP.compute_ang_mom_19(rec, member=member)
+        CHP.r_halos_1a(rec, member=member)
+        CHP.det_main_axis_1b2(rec, member=member)
+        CHP.det_halo_energies_1b3(rec, member=member)
+        CHP.compute_spin_parameter_1c(rec)
+        out2[h] = [rec[f] for f in STAR_FIELDS]
+    for name in list(H.mem.keys()):
+        H.deallocate(name)
+    np.savez_compressed(os.path.join(HERE, "halo_case_stars.npz"), off=off, pos=pos, vel=vel, mass=mass2,
+                        dens=dens, index=index.astype(np.int32), ndm=ndm, massp=0.8, out=out2,
+                        fields=np.array(STAR_FIELDS), Lbox=box, Hub_pt=70.0, gravconst=430.1)
+    print("halo_case_stars", nh, "halos", int(off[-1]), "members", int((index >= ndm).sum()), "stars")
 
 
 if __name__ == "__main__":

@@ -106,3 +106,46 @@ def test_shrinking_sphere_centre():
     np.testing.assert_allclose(g["r"][same], r["r"][same], rtol=1e-12)
     with pytest.raises(Exception):
         halo_props.compute(off, pos, vel, mass, dens, 100.0, 70.0, sc=(1e-3, 0.0))
+
+
+def test_stars_and_centre_of_mass():
+    """Mode 'full' with stars and H.cdm: the reference's fixture
+    (halo_case_stars.npz: det_mass_17's ndm, nstar, mdm, m*, mcontam;
+    det_center_18's centre-of-mass member, sigma_dm, sigma*) through the host
+    entry point, and a larger catalogue with stars against the oracle through
+    the device entry point (member indices on the device)."""
+    import torch
+    from ahop_b200 import halo_props, synthetic
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "halo_case_stars.npz"))
+    kw = dict(cdm=True, index=d["index"], ndm=int(d["ndm"]), massp=float(d["massp"]))
+    g = halo_props.compute(d["off"], d["pos"], d["vel"], d["mass"], d["dens"], float(d["Lbox"]), float(d["Hub_pt"]),
+                           **kw)
+    f = list(d["fields"])
+    col = lambda n: d["out"][:, f.index(n)]
+    for name in ["ndm", "nstar"]:
+        assert np.array_equal(g[name], col(name)), name
+    for name in ["px", "py", "pz"]:
+        assert np.array_equal(g[name], col(name)), name
+    for name in ["m", "mdm", "m*", "mcontam", "vx", "vy", "vz", "r", "ek", "sigma", "sigma_dm", "sigma*"]:
+        np.testing.assert_allclose(g[name], col(name), rtol=1e-12, err_msg=name)
+    # a catalogue with 30 % stars, device arrays
+    off, pos, vel, mass, dens = synthetic.halo_catalogue(150, seed=61, nmin=20, nmax=40000, box=100.0)
+    rng = np.random.default_rng(5)
+    star = rng.random(len(mass)) < 0.3
+    ndm = 10_000_000
+    index = np.where(star, ndm + np.arange(len(mass)), np.arange(len(mass))).astype(np.int32)
+    mass = np.where(star, 0.1, 1.0) * rng.uniform(0.9, 1.2, len(mass))
+    r = halo_oracle.props(off, pos, vel, mass, dens, 100.0, 70.0, epot=False, cdm=True, index=index, ndm=ndm,
+                          massp=1.1)
+    dev = torch.device("cuda")
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    out = torch.zeros((len(off) - 1, halo_props.NF), dtype=torch.float64, device=dev)
+    halo_props.compute_device(t(off), t(pos), t(vel), t(mass), t(dens), out, 100.0, 70.0, cdm=True,
+                              d_index=t(index), ndm=ndm, massp=1.1)
+    torch.cuda.synchronize()
+    o = out.cpu().numpy()
+    gi = lambda n: o[:, halo_props.FIELDS.index(n)]
+    for name in ["ndm", "nstar", "icenter"]:
+        assert np.array_equal(gi(name), r[name]), name
+    for name in ["m", "mdm", "m*", "mcontam", "px", "py", "pz", "r", "sigma", "sigma_dm", "sigma*"]:
+        np.testing.assert_allclose(gi(name), r[name], rtol=1e-12, err_msg=name)

@@ -46,3 +46,41 @@ def test_device_pipeline_matches_host_steps():
         assert np.array_equal(res["props"], host, equal_nan=True)
     finally:
         halo_props.set_tiles(None)
+
+
+def test_pipeline_with_stars_centre_of_mass_and_virial_step():
+    """A box with 15 % stars (dark matter first, ndm), the centre-of-mass
+    centre and the virial step inside the snapshot pipeline, against the host
+    entry points on the host-gathered members with their particle indices:
+    every property row and every virial row bit for bit."""
+    from ahop_b200 import finder, halo_props, msm, pipeline, synthetic
+    ps = synthetic.clustered_box(100_000, 100, seed=37, nmax=8000, star_fraction=0.15)
+    assert ps.ndm is not None and 0 < ps.ndm < ps.n
+    halo_props.set_tiles([256] * halo_props.BUCKETS)
+    try:
+        kw = dict(ndm=ps.ndm, cdm=True, massp=1.5 / ps.n)
+        res = pipeline.run_snapshot(ps.pos, ps.vel, ps.mass, box=1.0, hub=70.0, epot=3, particle_views=True,
+                                    vir_overdens=178.0, rho_mean=1.0, **kw)
+        finder.configure(ps.n)
+        out = finder.run(ps.pos, ps.mass)
+        sel = msm.select()
+        w = sel["whereIam_parts"]
+        order = np.argsort(w, kind="stable")
+        ids, idxs, counts = np.unique(w[order], return_index=True, return_counts=True)
+        keep = ids > 0
+        idxs, counts = idxs[keep], counts[keep]
+        members = np.concatenate([order[i:i + c] for i, c in zip(idxs, counts)])
+        off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        g = halo_props.compute(off, ps.pos[members], ps.vel[members], ps.mass[members], out["density"][members],
+                               1.0, 70.0, epot=3, index=members.astype(np.int32), **kw)
+        host = np.stack([g[f] for f in halo_props.FIELDS], 1)
+        assert np.array_equal(res["props"], host, equal_nan=True)
+        assert g["nstar"].sum() > 0 and np.array_equal(g["ndm"] + g["nstar"], np.diff(off).astype(float))
+        v = halo_props.virial(off, ps.pos[members], ps.vel[members], ps.mass[members], g, 1.0, 70.0, 430.1, 178.0,
+                              1.0, ep="ep64")
+        vh = np.stack([v[f] for f in halo_props.VIR_FIELDS], 1)
+        assert res["virial"].shape == vh.shape
+        assert np.array_equal(res["virial"], vh, equal_nan=True)
+        assert np.isfinite(res["virial"][:, 0]).mean() > 0.5
+    finally:
+        halo_props.set_tiles(None)

@@ -33,6 +33,32 @@ def test_oracle_matches_reference_halo_functions():
     np.testing.assert_allclose(r["spin64"][small], col("spin")[small], rtol=1e-10)
 
 
+STARS = os.path.join(os.path.dirname(__file__), "golden", "halo_case_stars.npz")
+
+
+def test_oracle_matches_reference_with_stars_and_cdm():
+    """halo_case_stars.npz: mode 'full', H.cdm = True, stars above H.ndm and
+    heavy dark-matter members -- det_mass_17's split, det_center_18's
+    centre-of-mass member and sigma_dm / sigma*."""
+    g = np.load(STARS)
+    f = list(g["fields"])
+    ref = g["out"]
+    r = halo_oracle.props(g["off"], g["pos"], g["vel"], g["mass"], g["dens"], float(g["Lbox"]), float(g["Hub_pt"]),
+                          float(g["gravconst"]), nthreads=2, cdm=True, index=g["index"], ndm=int(g["ndm"]),
+                          massp=float(g["massp"]))
+    col = lambda n: ref[:, f.index(n)]
+    for name in ["ndm", "nstar"]:
+        assert np.array_equal(r[name], col(name)), name
+    for name in ["m", "mdm", "m*", "mcontam", "px", "py", "pz", "vx", "vy", "vz", "r", "ek", "sigma", "sigma_dm",
+                 "sigma*"]:
+        np.testing.assert_allclose(r[name], col(name), rtol=1e-12, atol=0, err_msg=name)
+    assert (col("nstar") > 0).all() and (col("mcontam") > 0).all()
+    # the centre-of-mass member differs from the densest one in most halos
+    d = halo_oracle.props(g["off"], g["pos"], g["vel"], g["mass"], g["dens"], float(g["Lbox"]), float(g["Hub_pt"]),
+                          float(g["gravconst"]), epot=False)
+    assert np.count_nonzero(d["px"] != r["px"]) >= len(r["px"]) - 1
+
+
 VIR = os.path.join(os.path.dirname(__file__), "golden", "virial_case.npz")
 
 
