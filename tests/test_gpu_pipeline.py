@@ -4,6 +4,8 @@ points: the reference's grouping (NumPy argsort/unique of whereIam_parts,
 NEI:107-119) and gather (CHP:497-506) on the host, then ahop_halo_props on
 host buffers.  Same kernels on the same members in the same order, so every
 property row must agree bit for bit."""
+import os
+
 import numpy as np
 import pytest
 
@@ -84,3 +86,41 @@ def test_pipeline_with_stars_centre_of_mass_and_virial_step():
         assert np.isfinite(res["virial"][:, 0]).mean() > 0.5
     finally:
         halo_props.set_tiles(None)
+
+
+def test_tree_brick_from_the_pipeline(tmp_path):
+    """The tree-brick catalogue of a pipeline run (ahop_b200.tree_bricks),
+    written through the recording h5py stand-in: one record per structure,
+    property fields equal to the pipeline's rows after the reference's unit
+    conversion, the tree fields from the selection, members as grouped."""
+    import json
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import h5py_record
+    from ahop_b200 import halo_props, pipeline, synthetic, tree_bricks as T
+    ps = synthetic.clustered_box(60_000, 60, seed=41, nmax=6000, star_fraction=0.15)
+    res = pipeline.run_snapshot(ps.pos * 100.0, ps.vel, ps.mass, box=100.0, hub=70.0, epot=3, particle_views=True,
+                                ndm=ps.ndm, rho_mean=1.0)
+    cat, idx, cnt, pids = T.from_snapshot(res, numstep=3)
+    assert len(cat) == res["nstruct"] and np.array_equal(cat["id"], np.arange(1, len(cat) + 1))
+    k = res["ids"] - 1
+    F = lambda f: res["props"][:, halo_props.FIELDS.index(f)]
+    assert np.array_equal(cat["nmem"][k], np.diff(res["offsets"]))
+    assert np.array_equal(cat["nstar"][k], F("nstar").astype(np.int32))
+    np.testing.assert_array_equal(cat["m"][k], F("m"))
+    assert cnt.sum() == ps.n and np.array_equal(np.sort(pids), np.arange(ps.n))
+    meta = dict(npart=ps.n, nusedpart=ps.n, ndm=ps.ndm, nstar=ps.n - ps.ndm, family="all", massp=1.0 / ps.n,
+                aexp=1.0, omega_t=0.3, age_univ=13.7, boxsize2=100.0, hubble=0.7, mboxp=1.0, numstep=3,
+                nb_of_halos=res["nb_of_halos"], nb_of_subhalos=res["nb_of_subhalos"], createtime="now",
+                omega_f=0.3, omega_lambda_f=0.7, af=1.0, Lf=100.0, H_f=70.0, FlagPeriod=1, nMembers=20, cdm=False,
+                method="MSM", b_init=0.2, nvoisins=32, nhop=16, rho_threshold=80.0, fudge=4.0, fudgepsilon=1e-5,
+                alphap=1.0, verbose=False, megaverbose=False, DPMMC=False, SC=False, dcell_min=0.005, eps_SC=0.05,
+                nsteps=1, photometry=False)
+    f = h5py_record.File(str(tmp_path / "tb.h5"), "w")
+    T.write(f, meta, cat, idx, cnt, pids)
+    log, arrays = h5py_record.record_of(f)
+    halo = [e for e in log if e["op"] == "dataset" and e["path"] == "/catalog/halo"][0]
+    written = arrays[halo["data"]]
+    np.testing.assert_array_equal(written["m"][k], F("m") * 1e11)
+    np.testing.assert_array_equal(written["px"][k], np.mod(F("px") / 100.0, 1.0))
+    assert json.loads([e for e in log if e.get("name") == "field_units"][0]["value"]["v"])["m"] == "Msun"
