@@ -341,6 +341,69 @@ def pipeline_section(args):
             "props_stages": t["props_stages"], "tile_rows_per_bucket": halo_props.tiles()["rows"]}
 
 
+def adjoint_section(args):
+    """Differentiation on the 2,097,152-particle box (2,000 NFW halos of up
+    to ~74,000 members, seed 4): forward and backward of the SPH density with
+    the finder's 32-neighbour lists held fixed, and of the per-halo
+    direct-sum potential over the generator's halos (members grouped by
+    halo); CUDA events around each call, W untimed + K timed repeats."""
+    import numpy as np
+    import torch
+    from ahop_b200 import autograd, build, finder, synthetic
+    build.build()
+    ps = synthetic.workload("c4_2m")
+    finder.configure(ps.n)
+    st = finder.run_stages(ps.pos, ps.mass, last_stage=2, store_neighbours=32)
+    dev = torch.device("cuda")
+    pos = torch.from_numpy(ps.pos).to(dev)
+    mass = torch.from_numpy(ps.mass).to(dev)
+    nei = torch.from_numpy(np.ascontiguousarray(st["neighbours"] - 1, np.int32)).to(dev)
+    order = np.argsort(ps.halo_id, kind="stable")
+    order = order[ps.halo_id[order] >= 0]
+    counts = np.bincount(ps.halo_id[order])
+    off = torch.from_numpy(np.concatenate([[0], np.cumsum(counts)]).astype(np.int64))
+    hpos = torch.from_numpy(np.ascontiguousarray(ps.pos[order])).to(dev)
+    hmass = torch.from_numpy(np.ascontiguousarray(ps.mass[order])).to(dev)
+    g = torch.randn(ps.n, dtype=torch.float64, device=dev)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms = []
+        for _ in range(max(1, args.steps)):
+            torch.cuda.synchronize()
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return statistics.mean(ms)
+
+    def dens_fwd():
+        autograd.density_fixed(pos, mass, nei, 1.0)
+
+    def dens_bwd():
+        p = pos.clone().requires_grad_(True)
+        (autograd.SPHDensity.apply(p, mass, nei, 1.0) * g).sum().backward()
+
+    def pot_fwd():
+        autograd.HaloPotential.apply(hpos, hmass, off, 1.0, 430.1)
+
+    def pot_bwd():
+        p = hpos.clone().requires_grad_(True)
+        autograd.HaloPotential.apply(p, hmass, off, 1.0, 430.1).sum().backward()
+
+    f_d, b_d, f_p, b_p = timed(dens_fwd), timed(dens_bwd), timed(pot_fwd), timed(pot_bwd)
+    pairs = float((counts.astype(np.float64) * (counts - 1) / 2).sum())
+    return {"mode": "adjoint", "workload": "c4_2m", "npart": ps.n, "nhalo": len(counts),
+            "halo_members": int(counts.sum()), "pairs": pairs, "density_forward_ms": f_d,
+            "density_forward_and_backward_ms": b_d, "potential_forward_ms": f_p,
+            "potential_forward_and_backward_ms": b_p,
+            "density_backward_Mpart_per_s": ps.n / ((b_d - f_d) / 1e3) / 1e6,
+            "potential_backward_pairs_per_s": pairs / ((b_p - f_p) / 1e3)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -360,6 +423,8 @@ def main():
     ap.add_argument("--reader", default="", metavar="WORKLOAD",
                     help="write a named synthetic workload as RAMSES Ra4 part files (64 files, in a temporary "
                          "directory) and time the device reader against the CPU restatement (not the bench line)")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="time the density and potential adjoints on the 2,097,152-particle box (not the bench line)")
     ap.add_argument("--pipeline", default="", metavar="WORKLOAD",
                     help="run whole snapshots (finder, MSM, member gather, FP32-compensated properties) on a named "
                          "synthetic workload (e.g. c5_512cubed) and print per-stage times (not the bench line)")
@@ -382,6 +447,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     if args.pipeline:
         print(json.dumps(pipeline_section(args)))
+        return
+    if args.adjoint:
+        print(json.dumps(adjoint_section(args)))
         return
     if args.reader:
         print(json.dumps(reader_section(args)))
