@@ -313,26 +313,48 @@ def reader_section(args):
 
 def pipeline_section(args):
     """Whole snapshots on one GPU: W untimed + K timed runs of
-    pipeline.run_snapshot; per-stage times of the last run and the mean
-    particles/s over the timed runs (host clock around the synchronised call,
-    pinned host arrays in, property rows out)."""
+    pipeline.run_snapshot (finder, MSM selection, member gather, properties,
+    virial step); per-stage times of the last run and the mean particles/s
+    over the timed runs (host clock around the synchronised call, pinned host
+    arrays in, property rows out).  With --check, the finder's outputs are
+    compared with the CPU restatement of the reference on the same particles,
+    which is timed beside."""
     import numpy as np
     from ahop_b200 import build, halo_props, pipeline, synthetic
     build.build()
     t0 = time.perf_counter()
     ps = synthetic.workload(args.pipeline)
     gen_s = time.perf_counter() - t0
+    kw = dict(box=ps.box, epot=2, ndm=ps.ndm)
     for _ in range(args.warmup):
-        pipeline.run_snapshot(ps.pos, ps.vel, ps.mass, box=ps.box, epot=2)
+        pipeline.run_snapshot(ps.pos, ps.vel, ps.mass, **kw)
     walls = []
     res = None
     for _ in range(max(1, args.steps)):
         t0 = time.perf_counter()
-        res = pipeline.run_snapshot(ps.pos, ps.vel, ps.mass, box=ps.box, epot=2)
+        res = pipeline.run_snapshot(ps.pos, ps.vel, ps.mass, **kw)
         walls.append(time.perf_counter() - t0)
     t = res["timings"]
     stars = int(np.count_nonzero(ps.mass < ps.mass.max() * 0.5)) if ps.n else 0
+    check = None
+    if args.check:
+        # the finder's outputs through the drop-in on the same particles
+        # against the CPU restatement of the reference (OpenMP, all host cores)
+        from ahop_b200 import finder
+        finder.configure(ps.n)
+        t0 = time.perf_counter()
+        out = finder.run(ps.pos, ps.mass)
+        gpu_s = time.perf_counter() - t0
+        rate, cpu_s, nth, ref = cpu_rate(ps)
+        check = {"density_equal": bool(np.array_equal(out["density"], ref["density"])),
+                 "liste_parts_equal": bool(np.array_equal(out["liste_parts"], ref["liste_parts"])),
+                 "integer_table_equal": bool(np.array_equal(out["integer_table"], ref["integer_table"])),
+                 "real_table_equal": bool(np.array_equal(out["real_table"], ref["real_table"])),
+                 "nnodes": int(out["nnodes"]), "oracle_nnodes": int(ref["nnodes"]),
+                 "gpu_finder_e2e_s": gpu_s, "cpu_finder_s": cpu_s, "cpu_Mpart_per_s": rate, "cpu_cores": nth,
+                 "cpu_kind": "port (C++/OpenMP restatement of the reference finder)"}
     return {"mode": "pipeline", "workload": args.pipeline, "npart": ps.n, "stars": stars, "generate_s": gen_s,
+            "check": check,
             "steps": len(walls), "warmup": args.warmup, "wall_s": walls, "Mpart_per_s": ps.n / min(walls) / 1e6,
             "nstruct": int(res["nstruct"]), "nb_of_halos": int(res["nb_of_halos"]),
             "structures_with_members": int(len(res["ids"])), "members": int(res["members"]),
@@ -423,6 +445,9 @@ def main():
     ap.add_argument("--reader", default="", metavar="WORKLOAD",
                     help="write a named synthetic workload as RAMSES Ra4 part files (64 files, in a temporary "
                          "directory) and time the device reader against the CPU restatement (not the bench line)")
+    ap.add_argument("--check", action="store_true",
+                    help="with --pipeline: compare the finder's outputs with the CPU restatement of the reference "
+                         "on the same particles and time it beside")
     ap.add_argument("--adjoint", action="store_true",
                     help="time the density and potential adjoints on the 2,097,152-particle box (not the bench line)")
     ap.add_argument("--pipeline", default="", metavar="WORKLOAD",
@@ -566,15 +591,18 @@ def main():
     dev_step()
     torch.cuda.synchronize()
     L.check(lib.ahop_debug_set_task_profile(0), "set_task_profile")
-    ts = (C.c_int64 * 13)()
-    lib.ahop_debug_tree_stats(ts, 13)
+    ts = (C.c_int64 * 30)()
+    lib.ahop_debug_tree_stats(ts, 30)
     tree_stats = {"structural_Mcycles": ts[0] / 1e6, "level_stats_Mcycles": ts[1] / 1e6,
                   "exact_Mcycles": ts[2] / 1e6, "levels": ts[3], "undecided_exact_passes": ts[4],
                   "max_levels_one_task": ts[5], "max_Mcycles_one_task": ts[6] / 1e6,
                   "structural_passes": ts[7]}
     nql = max(1, ts[8])
     knn_stats = {"query_leaves": ts[8], "cand_leaves_per_query_leaf": ts[9] / nql,
-                 "leaf_visits_per_query": ts[10] / n, "insertions_per_query": ts[11] / n, "overflow_leaves": ts[12]}
+                 "leaf_visits_per_query": ts[10] / n, "insertions_per_query": ts[11] / n, "overflow_leaves": ts[12],
+                 "ideal_visits_per_query": ts[18] / n, "chunks_per_query": ts[26] / n,
+                 "ballot_hits_per_query": ts[27] / n,
+                 "union_visits_per_query_leaf": ts[28] / max(1, ts[29])}
     mean_stage = {k: statistics.mean(s[k] for s in stage) for k in
                   ("tree", "knn_density", "hop_groups", "saddles", "nodes", "membership", "total")}
     line = {"metric": METRIC, "value": value, "unit": "Mpart/s", "n_gpus": world, "steps": args.steps,

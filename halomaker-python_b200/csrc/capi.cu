@@ -371,6 +371,7 @@ int ahop_debug_tree_stats(int64_t* out, int32_t n) {
   if (n > 17) out[17] = E.forest_edges;
   for (int i = 18; i < n && i < 21; ++i) out[i] = (int64_t)E.knn_stats[i - 13];
   for (int i = 21; i < n && i < 26; ++i) out[i] = (int64_t)E.knn_phase[i - 21];
+  for (int i = 26; i < n && i < 30; ++i) out[i] = (int64_t)E.knn_stats[i - 18];
   return AHOP_OK;
 }
 

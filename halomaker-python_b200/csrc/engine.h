@@ -95,7 +95,7 @@ struct Engine {
   int32_t launches = 0, cub_calls = 0, waves = 0, hop_passes = 0;  // counters of the current compute
   int32_t forest_rounds = 0, forest_edges = 0;                        // saddle forest of the current compute
   unsigned long long tree_stats[11] = {};                             // structure-tree kernel counters
-  unsigned long long knn_stats[8] = {};
+  unsigned long long knn_stats[12] = {};
   unsigned long long knn_phase[5] = {};                              // kNN kernel counters
   bool events_ready = false;
   AhopTimings timings{};

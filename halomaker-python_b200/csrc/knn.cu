@@ -573,6 +573,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
   __shared__ double s_bd[kWarpsPerBlock][kStack];
   __shared__ int32_t s_cand[kWarpsPerBlock][kMaxCand];
   __shared__ unsigned char s_list[kWarpsPerBlock][kLeaf][32];  // each query's seed order
+  __shared__ unsigned s_vis[kProf ? kWarpsPerBlock : 1][kMaxCand / 32];  // profiling: candidates any query visited
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
@@ -687,7 +688,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
     const long long t_b = kProf ? clock64() : 0;
     long long c_init = 0, c_scan = 0, c_fin = 0;
     // ---- C: per-query kNN over the candidates
-    unsigned nvis = 0, nins = 0, nideal = 0;
+    unsigned nvis = 0, nins = 0, nideal = 0, nchunk = 0, nbits = 0;
+    if (kProf) {
+      for (int i = lane; i < kMaxCand / 32; i += 32) s_vis[kProf ? wib : 0][i] = 0u;
+      __syncwarp();
+    }
     for (int q = 0; q < nq; ++q) {
       const int64_t s = s0 + q;
       const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
@@ -704,6 +709,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
           // least the current radius from that box (and all after it) is out
           const double lb = (double)__uint_as_float((kb[c0] >> 12) << 11);
           if (lb * (1.0 - 1e-9) >= L.r2) break;
+          if (kProf) ++nchunk;
           const int ci = c0 + lane;
           int32_t leaf = -1;
           double bd = CUDART_INF;
@@ -716,9 +722,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
           while (mask) {
             const int src = __ffs(mask) - 1;
             mask &= mask - 1;
+            if (kProf) ++nbits;
             const double sbd = __shfl_sync(0xffffffffu, bd, src);
             const int32_t sl = __shfl_sync(0xffffffffu, leaf, src);
-            if (sbd < L.r2) leaf_insert<C>(A, L, sl, s, qx, qy, qz, lane, nvis, nins);
+            if (sbd < L.r2) {
+              if (kProf && lane == 0 && c0 + src < kMaxCand)
+                atomicOr(&s_vis[kProf ? wib : 0][(c0 + src) >> 5], 1u << ((c0 + src) & 31));
+              leaf_insert<C>(A, L, sl, s, qx, qy, qz, lane, nvis, nins);
+            }
           }
         }
       }
@@ -750,6 +761,20 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
       }
       atomicAdd(&A.kstats[5], (unsigned long long)nideal);
       atomicAdd(&A.kstats[overflow ? 6 : 7], (unsigned long long)(clock64() - t_leaf));
+    }
+    if (kProf) {
+      __syncwarp();
+      unsigned u = 0;
+      if (!overflow && cap == kMaxCand)
+        for (int i = lane; i < kMaxCand / 32; i += 32) u += __popc(s_vis[kProf ? wib : 0][i]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) u += __shfl_xor_sync(0xffffffffu, u, o);
+      if (lane == 0) {
+        atomicAdd(&A.kstats[8], (unsigned long long)nchunk);
+        atomicAdd(&A.kstats[9], (unsigned long long)nbits);
+        atomicAdd(&A.kstats[10], (unsigned long long)u);
+        if (!overflow && cap == kMaxCand) atomicAdd(&A.kstats[11], 1ULL);
+      }
     }
     if (kProf && lane == 0) {
       atomicAdd(&A.kstats[0], 1ULL);
@@ -818,7 +843,7 @@ int stage_knn_density(Engine& E) {
   AHOP_CUDA_TRY(cudaGetLastError());
   int herr = 0;
   AHOP_CUDA_TRY(cudaMemcpyAsync(&herr, E.d_flags.p, 4, cudaMemcpyDeviceToHost, E.stream));
-  AHOP_CUDA_TRY(cudaMemcpyAsync(E.knn_stats, E.d_flags.as<char>() + 64, 8 * 8, cudaMemcpyDeviceToHost, E.stream));
+  AHOP_CUDA_TRY(cudaMemcpyAsync(E.knn_stats, E.d_flags.as<char>() + 64, 12 * 8, cudaMemcpyDeviceToHost, E.stream));
   AHOP_CUDA_TRY(cudaMemcpyAsync(E.knn_phase, E.d_flags.as<char>() + 64 + 24 * 8, 5 * 8, cudaMemcpyDeviceToHost,
                                 E.stream));
   AHOP_CUDA_TRY(cudaStreamSynchronize(E.stream));

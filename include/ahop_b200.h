@@ -144,7 +144,12 @@ int ahop_debug_compute_stages(const double* pos_in, const double* mass_in, int64
  * radius, cycles spent in leaves that fell back to per-query search and in
  * the other leaves (summed over warps), then [21..25] the cycles of those
  * other leaves by phase: radius bound, candidate list and its sort, seed
- * lists, candidate scan, density. */
+ * lists, candidate scan, density; [26..29] kNN, task profile on: candidate
+ * chunks examined, candidate leaves passing a query's box test at its ballot,
+ * candidate leaves visited by at least one query of their leaf (leaves whose
+ * list stayed in shared memory), and the number of such leaves.  The
+ * counters [8..12] and [18..29] come from the profiling instance of the kNN
+ * kernel, which runs only while the task profile is on. */
 int ahop_debug_tree_stats(int64_t* out, int32_t n);
 /* Per-task structure-tree profile (off by default; turning it on costs one
  * store per task).  Row k (16 int64) describes the task of node k: groups in
