@@ -573,7 +573,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
   __shared__ double s_bd[kWarpsPerBlock][kStack];
   __shared__ int32_t s_cand[kWarpsPerBlock][kMaxCand];
   __shared__ unsigned char s_list[kWarpsPerBlock][kLeaf][32];  // each query's seed order
-  __shared__ unsigned s_vis[kProf ? kWarpsPerBlock : 1][kMaxCand / 32];  // profiling: candidates any query visited
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
@@ -689,10 +688,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
     long long c_init = 0, c_scan = 0, c_fin = 0;
     // ---- C: per-query kNN over the candidates
     unsigned nvis = 0, nins = 0, nideal = 0, nchunk = 0, nbits = 0;
-    if (kProf) {
-      for (int i = lane; i < kMaxCand / 32; i += 32) s_vis[kProf ? wib : 0][i] = 0u;
-      __syncwarp();
-    }
+    unsigned visbits = 0;  // profiling: lane l holds candidates [32 l, 32 l + 32) visited by any query
     for (int q = 0; q < nq; ++q) {
       const int64_t s = s0 + q;
       const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
@@ -726,8 +722,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
             const double sbd = __shfl_sync(0xffffffffu, bd, src);
             const int32_t sl = __shfl_sync(0xffffffffu, leaf, src);
             if (sbd < L.r2) {
-              if (kProf && lane == 0 && c0 + src < kMaxCand)
-                atomicOr(&s_vis[kProf ? wib : 0][(c0 + src) >> 5], 1u << ((c0 + src) & 31));
+              if (kProf && lane == ((c0 + src) >> 5)) visbits |= 1u << ((c0 + src) & 31);
               leaf_insert<C>(A, L, sl, s, qx, qy, qz, lane, nvis, nins);
             }
           }
@@ -763,10 +758,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
       atomicAdd(&A.kstats[overflow ? 6 : 7], (unsigned long long)(clock64() - t_leaf));
     }
     if (kProf) {
-      __syncwarp();
-      unsigned u = 0;
-      if (!overflow && cap == kMaxCand)
-        for (int i = lane; i < kMaxCand / 32; i += 32) u += __popc(s_vis[kProf ? wib : 0][i]);
+      unsigned u = (!overflow && cap == kMaxCand) ? __popc(visbits) : 0u;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) u += __shfl_xor_sync(0xffffffffu, u, o);
       if (lane == 0) {
