@@ -39,7 +39,6 @@ import time
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(REPO, "halomaker-python_b200"))
 
-FP32_OPS_PER_PAIR = 13.5  # FP32 operations per pair in the compensated pair kernel
 METRIC = "Mpart/s end-to-end vs host CPU; halo Epot pairs/s FP32-comp vs FP64 at 1e-6"
 PARAMS = dict(nvoisins=32, nhop=16, rho_threshold=80.0, fudge=4.0, fudgepsilon=1e-5, alphap=1.0, nmembthresh=20)
 WORKLOAD = dict(name="c2_256cubed", npart=16_777_216, nhalo=19_200, seed=2, nmin=20, nmax=2_000_000)
@@ -240,22 +239,26 @@ def halo_section(args, torch, dist=None):
         pairs = float(pt.item())
     m64, m32 = statistics.mean(t64), statistics.mean(t32)
     nominal_fp32 = 148 * 128 * 2 * 1.965e9 / 1e12  # TFLOP/s, non-tensor FP32 at max clock
-    lane_peak = 148 * 128 * 1.965e9 / 1e12          # T FP32 lane operations/s
+    mufu_peak = 148 * 16 * 1.965e9 / 1e12           # T reciprocal square roots/s
+    rate32 = pairs / (m32 / 1e3)
     return {"workload": f"{nh_all} halos, counts n^-1.9 on [20, {args.halo_nmax:g}], seed {args.halo_seed}"
                         + (f", split over {world} ranks by cost" if world > 1 else ""),
             "pairs": pairs, "fp64_ms": m64, "fp32c_ms": m32,
-            "fp64_pairs_per_s": pairs / (m64 / 1e3), "fp32c_pairs_per_s": pairs / (m32 / 1e3),
+            "fp64_pairs_per_s": pairs / (m64 / 1e3), "fp32c_pairs_per_s": rate32,
             "fp32c_over_fp64": m64 / m32, "max_rel_err_fp32c_vs_fp64": rel, "tolerance": 1e-6,
-            # the FP32 pipes bound the compensated form: 13.5 FP32 operations per
-            # pair (9 hi/lo separation, 3 r^2, 1 mass-weighted accumulation, 0.5
-            # compensated fold), packed two per f32x2 instruction, against 128 FP32
-            # lanes per SM per cycle; the 20 flop/pair convention is kept beside it
-            "roofline": {"bound": "fp32 fma pipes", "fp32_ops_per_pair": FP32_OPS_PER_PAIR,
-                         "achieved": FP32_OPS_PER_PAIR * pairs / (m32 / 1e3) / 1e12, "peak": lane_peak,
-                         "unit": "T FP32 lane-ops/s",
-                         "frac": FP32_OPS_PER_PAIR * pairs / (m32 / 1e3) / 1e12 / lane_peak,
-                         "peak_source": "nominal (148 SMs x 128 FP32 lanes x 1.965 GHz)",
-                         "tflops_at_20_flop_per_pair": 20 * pairs / (m32 / 1e3) / 1e12,
+            # the compensated form takes one approximate reciprocal square root
+            # per pair on the MUFU pipe (16 results per SM per cycle) and, per
+            # pair, 7 FP32 lane operations for far pairs (3 separation, 3 r^2,
+            # 1 mass-weighted accumulation) or 13 for near ones (hi/lo
+            # separation), packed two per f32x2 instruction on 128 FP32 lanes
+            # per SM per cycle; far pairs are therefore MUFU-bound.  The fp32c
+            # time includes the Morton sort of the members.  The 20 flop/pair
+            # convention is kept beside it.
+            "roofline": {"bound": "MUFU pipe (rsqrt)", "rsqrt_per_pair": 1, "achieved": rate32 / 1e12,
+                         "peak": mufu_peak, "unit": "T rsqrt/s", "frac": rate32 / 1e12 / mufu_peak,
+                         "peak_source": "nominal (148 SMs x 16 MUFU results/clk x 1.965 GHz)",
+                         "fp32_lane_ops_per_pair": "7 far, 13 near",
+                         "tflops_at_20_flop_per_pair": 20 * rate32 / 1e12,
                          "tflops_peak_nominal": nominal_fp32},
             "moments_ms": tm["moments"], "items": int(tm["items"]), "tile_rows_per_bucket": halo_props.tiles()["rows"],
             "autotune_ms": tune_ms, "graph_replays": int(tm["graph_replays"]), "virial_ms": statistics.mean(tv),

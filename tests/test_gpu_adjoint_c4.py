@@ -8,9 +8,15 @@
   the sample).
 * Per-halo direct-sum potential over the generator's halos: dE/dx equals
   minus the direct-sum force (NumPy FP64, per sampled particle over its
-  halo) to 1e-10 on 1,000 random halo members, and matches central
-  differences of the halo's E through the forward kernel to 1e-6 of the
-  halo's largest gradient component.
+  halo) to 1e-10 on 1,000 random halo members, and matches FP64 central
+  differences of E to 1e-6 of the halo's largest gradient component.  E
+  depends on x_j only through the pairs (i, j), so the differences are taken
+  of those n - 1 terms (NumPy FP64); for halos of up to 5,000 members they
+  are also taken of the whole E through the forward kernel.  For larger
+  halos the kernel's E is a sum of up to 2.8e9 pair terms whose FP64
+  rounding, divided by 2h, exceeds 1e-6 of the gradient (measured: 3.6e-5
+  relative in the largest halo), so there only the pair-term differences
+  apply.
 The backward passes recompute the pair weights from positions; nothing is
 stored between forward and backward but positions and lists.
 """
@@ -102,11 +108,29 @@ def test_potential_adjoint_c4(c4):
         r2[j - a] = np.inf
         f = -G * hm[j] * (hm[a:b, None] * d / r2[:, None] ** 1.5).sum(0)
         np.testing.assert_allclose(grad[j], -f, rtol=1e-10, atol=1e-12 * np.abs(f).max())
+    # central differences of the pair terms of each sampled member
+    def pair_energy(x, j, a, b):
+        d = x - hp[a:b]
+        d[d > L / 2] -= L
+        d[d < -L / 2] += L
+        r = np.sqrt((d * d).sum(1))
+        r[j - a] = np.inf
+        return -G * hm[j] * np.sum(hm[a:b] / r)
+    for j, hh in zip(sample, halo):
+        a, b = off[hh], off[hh + 1]
+        gmax = np.abs(grad[a:b]).max()
+        for ax in range(3):
+            e = np.zeros(3)
+            e[ax] = H
+            fdv = (pair_energy(hp[j] + e, j, a, b) - pair_energy(hp[j] - e, j, a, b)) / (2 * H)
+            assert abs(fdv - grad[j, ax]) <= 1e-6 * max(abs(grad[j, ax]), gmax), (j, ax)
     # central differences of the halo's E through the forward kernel
     halo_props.set_graph(False)
     try:
         for hh in np.unique(halo):
             a, b = off[hh], off[hh + 1]
+            if b - a > 5000:
+                continue
             q0 = torch.from_numpy(hp[a:b].copy()).to(dev)
             q = q0.clone()
             mh = m_t[a:b]
