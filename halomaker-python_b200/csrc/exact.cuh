@@ -32,6 +32,15 @@ __device__ __forceinline__ double pdist2(double ax, double ay, double az, double
   return xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
 }
 
+// The same squared distance for a pair known to be less than half a period
+// apart on every axis: then |a - b| <= L/2 <= L - |a - b| (also after
+// rounding, which is monotone), so the periodic minimum and the clamp at 0
+// return |a - b|, and squaring drops the sign.  Same bits as pdist2.
+__device__ __forceinline__ double dist2_near(double ax, double ay, double az, double bx, double by, double bz) {
+  const double dx = xsub(ax, bx), dy = xsub(ay, by), dz = xsub(az, bz);
+  return xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
+}
+
 // Cubic-spline kernel of the reference (f90:3270-3287), same evaluation order.
 __device__ __forceinline__ double spline(double x) {
   if (x <= 1.0) {

@@ -231,6 +231,14 @@ __device__ __forceinline__ double box_dist2(const double* __restrict__ b, double
   return dx * dx + dy * dy + dz * dz;
 }
 
+// Squared distance from the query to particle p; wrap = false (uniform over
+// the warp) when every particle the caller passes lies within half a period
+// of the query on each axis (same bits, fewer operations: dist2_near).
+__device__ __forceinline__ double qdist2(const KnnArgs& A, bool wrap, double qx, double qy, double qz, int64_t p) {
+  return wrap ? pdist2(qx, qy, qz, A.x[p], A.y[p], A.z[p], A.Lx, A.Ly, A.Lz)
+              : dist2_near(qx, qy, qz, A.x[p], A.y[p], A.z[p]);
+}
+
 // The warp's running neighbour list: lane i holds the i-th nearest (ld, ls, lo):
 // squared distance, sorted slot, original index; empty slots hold +inf.
 struct WarpList {
@@ -246,13 +254,14 @@ struct WarpList {
 // such ties.
 template <int C>
 __device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int32_t leaf, int64_t self, double qx,
-                                            double qy, double qz, int lane, unsigned& nvis, unsigned& nins) {
+                                            double qy, double qz, int lane, unsigned& nvis, unsigned& nins,
+                                            bool wrap = true) {
   const int nvv = C ? C : A.nv;
   ++nvis;
   const int32_t p = leaf * kLeaf + lane;
   const bool v = ((int64_t)p < A.n) && ((int64_t)p != self);
   double d = CUDART_INF;
-  if (v) d = pdist2(qx, qy, qz, A.x[p], A.y[p], A.z[p], A.Lx, A.Ly, A.Lz);
+  if (v) d = qdist2(A, wrap, qx, qy, qz, p);
   unsigned mask = __ballot_sync(0xffffffffu, v && d <= L.r2);
   if (!mask) return;
   while (mask) {
@@ -288,12 +297,12 @@ __device__ __forceinline__ bool key_less(double da, int32_t oa, double db, int32
 // and element 32 + l (adjacent leaf jn, lane l).  Empty ones are
 // (+inf, INT_MAX) and order last.
 __device__ __forceinline__ void seed_candidate(const KnnArgs& A, int64_t jl, int64_t jn, int64_t self, double qx,
-                                               double qy, double qz, int e, double& d, int32_t& o) {
+                                               double qy, double qz, int e, double& d, int32_t& o, bool wrap) {
   const int64_t p = (e < 32) ? jl * kLeaf + e : jn * kLeaf + (e - 32);
   d = CUDART_INF;
   o = INT_MAX;
   if ((e < 32 || (jn >= 0 && jn != jl)) && p < A.n && p != self) {
-    d = pdist2(qx, qy, qz, A.x[p], A.y[p], A.z[p], A.Lx, A.Ly, A.Lz);
+    d = qdist2(A, wrap, qx, qy, qz, p);
     o = A.orig[p];
   }
 }
@@ -304,12 +313,12 @@ __device__ __forceinline__ void seed_candidate(const KnnArgs& A, int64_t jl, int
 // distance (+inf when fewer than nv exist) to every lane.
 template <int C>
 __device__ __forceinline__ double seed_sort(const KnnArgs& A, int64_t jl, int64_t jn, int64_t self, double qx,
-                                           double qy, double qz, int lane, unsigned char* list) {
+                                           double qy, double qz, int lane, unsigned char* list, bool wrap) {
   const int nvv = C ? C : A.nv;
   double d0, d1;
   int32_t o0, o1, s0 = lane, s1 = 32 + lane;
-  seed_candidate(A, jl, jn, self, qx, qy, qz, lane, d0, o0);
-  seed_candidate(A, jl, jn, self, qx, qy, qz, 32 + lane, d1, o1);
+  seed_candidate(A, jl, jn, self, qx, qy, qz, lane, d0, o0, wrap);
+  seed_candidate(A, jl, jn, self, qx, qy, qz, 32 + lane, d1, o1, wrap);
 #pragma unroll
   for (int size = 2; size <= 64; size <<= 1) {
     const bool asc = ((2 * lane) & size) == 0;  // same for both elements of the lane
@@ -350,21 +359,22 @@ __device__ __forceinline__ double seed_sort(const KnnArgs& A, int64_t jl, int64_
 // caller then sorts with the particle indices (seed_sort).  Empty candidates
 // (+inf) may tie among themselves: they are never list entries.
 __device__ __forceinline__ unsigned long long seed_key(const KnnArgs& A, int64_t jl, int64_t jn, int64_t self,
-                                                       double qx, double qy, double qz, int e) {
+                                                       double qx, double qy, double qz, int e, bool wrap) {
   const int64_t p = (e < 32) ? jl * kLeaf + e : jn * kLeaf + (e - 32);
   double d = CUDART_INF;
   if ((e < 32 || (jn >= 0 && jn != jl)) && p < A.n && p != self)
-    d = pdist2(qx, qy, qz, A.x[p], A.y[p], A.z[p], A.Lx, A.Ly, A.Lz);
+    d = qdist2(A, wrap, qx, qy, qz, p);
   return (unsigned long long)__double_as_longlong(d);
 }
 
 template <int C>
 __device__ __forceinline__ bool seed_sort_keys(const KnnArgs& A, int64_t jl, int64_t jn, int64_t self, double qx,
-                                               double qy, double qz, int lane, unsigned char* list, double& kth) {
+                                               double qy, double qz, int lane, unsigned char* list, double& kth,
+                                               bool wrap) {
   const int nvv = C ? C : A.nv;
   const unsigned long long kInf = 0x7FF0000000000000ull;
-  unsigned long long k0 = seed_key(A, jl, jn, self, qx, qy, qz, lane);
-  unsigned long long k1 = seed_key(A, jl, jn, self, qx, qy, qz, 32 + lane);
+  unsigned long long k0 = seed_key(A, jl, jn, self, qx, qy, qz, lane, wrap);
+  unsigned long long k1 = seed_key(A, jl, jn, self, qx, qy, qz, 32 + lane, wrap);
   int32_t s0 = lane, s1 = 32 + lane;
 #pragma unroll
   for (int size = 2; size <= 64; size <<= 1) {
@@ -406,10 +416,10 @@ __device__ __forceinline__ bool seed_sort_keys(const KnnArgs& A, int64_t jl, int
 template <int C>
 __device__ __forceinline__ void seed_list(const KnnArgs& A, WarpList& L, int64_t jl, int64_t jn, int64_t self,
                                           double qx, double qy, double qz, int lane, const unsigned char* list,
-                                          unsigned& nvis) {
+                                          unsigned& nvis, bool wrap) {
   const int nvv = C ? C : A.nv;
   const int e = list[lane];
-  const double d = __longlong_as_double((long long)seed_key(A, jl, jn, self, qx, qy, qz, e));
+  const double d = __longlong_as_double((long long)seed_key(A, jl, jn, self, qx, qy, qz, e, wrap));
   const int64_t p = (e < 32) ? jl * kLeaf + e : jn * kLeaf + (e - 32);
   L.ld = d;
   L.ls = (d < CUDART_INF) ? (int32_t)p : -1;
@@ -529,6 +539,18 @@ __device__ __forceinline__ float box_dist2_lb(const float4* __restrict__ b, floa
   return __fadd_rd(__fadd_rd(__fmul_rd(dx, dx), __fmul_rd(dy, dy)), __fmul_rd(dz, dz));
 }
 
+// True when every particle of the leaf with FP32 box b (which contains the
+// leaf's exact box) lies within half a period of the query on each axis, so
+// that dist2_near applies.  Evaluated in FP64 (float operands are exact
+// there) with a margin of 2^-30 L for its own roundings.
+__device__ __forceinline__ bool near_box(const float4* __restrict__ b, double qx, double qy, double qz, double Lx,
+                                         double Ly, double Lz) {
+  const float4 c = b[0], w = b[1];
+  return fabs((double)c.x - qx) + (double)w.x <= Lx * (0.5 - 0x1p-30) &&
+         fabs((double)c.y - qy) + (double)w.y <= Ly * (0.5 - 0x1p-30) &&
+         fabs((double)c.z - qz) + (double)w.z <= Lz * (0.5 - 0x1p-30);
+}
+
 // Periodic squared distance between two padded boxes (centre, half width).
 // Lower bound of the squared periodic distance between two widened FP32 boxes.
 __device__ __forceinline__ float boxbox_dist2_lb(const float4* __restrict__ a, const float4* __restrict__ b,
@@ -594,9 +616,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
     for (int q = 0; q < nq; ++q) {
       const int64_t s = s0 + q;
       const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
+      const bool wrap = !(near_box(A.box32 + 2 * jl, qx, qy, qz, A.Lx, A.Ly, A.Lz) &&
+                          near_box(A.box32 + 2 * jn, qx, qy, qz, A.Lx, A.Ly, A.Lz));
       double kth;
-      if (!seed_sort_keys<C>(A, jl, jn, s, qx, qy, qz, lane, s_list[wib][q], kth))
-        kth = seed_sort<C>(A, jl, jn, s, qx, qy, qz, lane, s_list[wib][q]);
+      if (!seed_sort_keys<C>(A, jl, jn, s, qx, qy, qz, lane, s_list[wib][q], kth, wrap))
+        kth = seed_sort<C>(A, jl, jn, s, qx, qy, qz, lane, s_list[wib][q], wrap);
       if (!(kth < CUDART_INF)) ok = false;  // fewer than nv others in the two leaves
       if (lane == q) Rq = kth;
     }
@@ -695,7 +719,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
       const float qxf = (float)qx, qyf = (float)qy, qzf = (float)qz;
       WarpList L;
       const long long tq0 = kProf ? clock64() : 0;
-      seed_list<C>(A, L, jl, jn, s, qx, qy, qz, lane, s_list[wib][q], nvis);
+      const bool swrap = !(near_box(A.box32 + 2 * jl, qx, qy, qz, A.Lx, A.Ly, A.Lz) &&
+                           near_box(A.box32 + 2 * jn, qx, qy, qz, A.Lx, A.Ly, A.Lz));
+      seed_list<C>(A, L, jl, jn, s, qx, qy, qz, lane, s_list[wib][q], nvis, swrap);
       const long long tq1 = kProf ? clock64() : 0;
       if (overflow) {
         query_dfs<C>(A, L, s, qx, qy, qz, lane, s_node[wib], s_bd[wib], jl, jn, nvis, nins);
@@ -709,10 +735,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
           const int ci = c0 + lane;
           int32_t leaf = -1;
           double bd = CUDART_INF;
+          bool lwrap = true;
           if (ci < ncand) {
             leaf = cb[kb[ci] & 4095u];
-            if (leaf != jl && leaf != jn)
+            if (leaf != jl && leaf != jn) {
               bd = (double)box_dist2_lb(A.box32 + 2 * (int64_t)leaf, qxf, qyf, qzf, Lxf, Lyf, Lzf);
+              lwrap = !near_box(A.box32 + 2 * (int64_t)leaf, qx, qy, qz, A.Lx, A.Ly, A.Lz);
+            }
           }
           unsigned mask = __ballot_sync(0xffffffffu, bd < L.r2);
           while (mask) {
@@ -721,9 +750,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
             if (kProf) ++nbits;
             const double sbd = __shfl_sync(0xffffffffu, bd, src);
             const int32_t sl = __shfl_sync(0xffffffffu, leaf, src);
+            const bool swl = __shfl_sync(0xffffffffu, (int)lwrap, src) != 0;
             if (sbd < L.r2) {
               if (kProf && lane == ((c0 + src) >> 5)) visbits |= 1u << ((c0 + src) & 31);
-              leaf_insert<C>(A, L, sl, s, qx, qy, qz, lane, nvis, nins);
+              leaf_insert<C>(A, L, sl, s, qx, qy, qz, lane, nvis, nins, swl);
             }
           }
         }
