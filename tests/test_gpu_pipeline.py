@@ -54,7 +54,9 @@ def test_pipeline_with_stars_centre_of_mass_and_virial_step():
     """A box with 15 % stars (dark matter first, ndm), the centre-of-mass
     centre and the virial step inside the snapshot pipeline, against the host
     entry points on the host-gathered members with their particle indices:
-    every property row and every virial row bit for bit."""
+    every property row bit for bit; the virial rows to 1e-9 (the virial
+    step's shell sums are shared-memory atomics, so their last bits depend on
+    the order in which members land)."""
     from ahop_b200 import finder, halo_props, msm, pipeline, synthetic
     ps = synthetic.clustered_box(100_000, 100, seed=37, nmax=8000, star_fraction=0.15)
     assert ps.ndm is not None and 0 < ps.ndm < ps.n
@@ -82,7 +84,8 @@ def test_pipeline_with_stars_centre_of_mass_and_virial_step():
                               1.0, ep="ep64")
         vh = np.stack([v[f] for f in halo_props.VIR_FIELDS], 1)
         assert res["virial"].shape == vh.shape
-        assert np.array_equal(res["virial"], vh, equal_nan=True)
+        assert np.array_equal(np.isnan(res["virial"]), np.isnan(vh))
+        np.testing.assert_allclose(res["virial"], vh, rtol=1e-9, equal_nan=True)
         assert np.isfinite(res["virial"][:, 0]).mean() > 0.5
     finally:
         halo_props.set_tiles(None)
