@@ -206,6 +206,7 @@ struct KnnArgs {
   int64_t lev_cnt[kMaxLevels];
   int nlev;
   int64_t n;
+  int32_t n32;  // n as int32 (n < 2^31 is checked at the boundary)
   double Lx, Ly, Lz, xyzlong;
   int nv;       // nvoisins (<= 32)
   int nstore;   // neighbours written per particle
@@ -259,7 +260,7 @@ __device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int32
   const int nvv = C ? C : A.nv;
   ++nvis;
   const int32_t p = leaf * kLeaf + lane;
-  const bool v = ((int64_t)p < A.n) && ((int64_t)p != self);
+  const bool v = (p < A.n32) && (p != (int32_t)self);
   double d = CUDART_INF;
   if (v) d = qdist2(A, wrap, qx, qy, qz, p);
   unsigned mask = __ballot_sync(0xffffffffu, v && d <= L.r2);
@@ -733,27 +734,32 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
           if (lb * (1.0 - 1e-9) >= L.r2) break;
           if (kProf) ++nchunk;
           const int ci = c0 + lane;
-          int32_t leaf = -1;
-          double bd = CUDART_INF;
-          bool lwrap = true;
+          // candidate leaf with bit 30 set when its particles need the periodic
+          // fold (leaf ids are below 2^26)
+          int32_t leafw = -1;
+          float bd = CUDART_INF_F;
           if (ci < ncand) {
-            leaf = cb[kb[ci] & 4095u];
+            const int32_t leaf = cb[kb[ci] & 4095u];
+            leafw = leaf;
             if (leaf != jl && leaf != jn) {
-              bd = (double)box_dist2_lb(A.box32 + 2 * (int64_t)leaf, qxf, qyf, qzf, Lxf, Lyf, Lzf);
-              lwrap = !near_box(A.box32 + 2 * (int64_t)leaf, qx, qy, qz, A.Lx, A.Ly, A.Lz);
+              bd = box_dist2_lb(A.box32 + 2 * (int64_t)leaf, qxf, qyf, qzf, Lxf, Lyf, Lzf);
+              if (!near_box(A.box32 + 2 * (int64_t)leaf, qx, qy, qz, A.Lx, A.Ly, A.Lz)) leafw |= 1 << 30;
             }
           }
-          unsigned mask = __ballot_sync(0xffffffffu, bd < L.r2);
+          // visit test in FP32 against the bound rounded up: a superset of the
+          // leaves whose lower bound is below the bound, so nothing is lost
+          float r2f = __double2float_ru(L.r2);
+          unsigned mask = __ballot_sync(0xffffffffu, bd < r2f);
           while (mask) {
             const int src = __ffs(mask) - 1;
             mask &= mask - 1;
             if (kProf) ++nbits;
-            const double sbd = __shfl_sync(0xffffffffu, bd, src);
-            const int32_t sl = __shfl_sync(0xffffffffu, leaf, src);
-            const bool swl = __shfl_sync(0xffffffffu, (int)lwrap, src) != 0;
-            if (sbd < L.r2) {
+            const float sbd = __shfl_sync(0xffffffffu, bd, src);
+            const int32_t slw = __shfl_sync(0xffffffffu, leafw, src);
+            if (sbd < r2f) {
               if (kProf && lane == ((c0 + src) >> 5)) visbits |= 1u << ((c0 + src) & 31);
-              leaf_insert<C>(A, L, sl, s, qx, qy, qz, lane, nvis, nins, swl);
+              leaf_insert<C>(A, L, slw & ~(1 << 30), s, qx, qy, qz, lane, nvis, nins, (slw >> 30) & 1);
+              r2f = __double2float_ru(L.r2);
             }
           }
         }
@@ -830,6 +836,7 @@ int stage_knn_density(Engine& E) {
   for (int l = 0; l < kMaxLevels; ++l) { A.lev_off[l] = E.lev_off[l]; A.lev_cnt[l] = E.lev_cnt[l]; }
   A.nlev = E.nlev;
   A.n = n;
+  A.n32 = (int32_t)n;
   A.Lx = P.xlong; A.Ly = P.ylong; A.Lz = P.zlong; A.xyzlong = P.xyzlong;
   A.nv = P.nvoisins;
   A.nstore = E.nstore;
