@@ -170,13 +170,15 @@ __global__ void __launch_bounds__(256) epot_grad_kernel(const int64_t* __restric
     __syncthreads();
     if (vi) {
       const int jend = min(256, n - j0);
+      // the member itself (r2 = 0) and coincident members drop out, as in
+      // the forward sum; one double reciprocal square root per pair
+#pragma unroll 4
       for (int jj = 0; jj < jend; ++jj) {
-        if (j0 + jj == i) continue;
         const double dx = xi - sx[jj], dy = yi - sy[jj], dz = zi - sz[jj];
         const double r2 = dx * dx + dy * dy + dz * dz;
         if (r2 > 0.0) {
-          const double inv = 1.0 / sqrt(r2);
-          const double f = sm[jj] * inv * inv * inv;
+          const double inv = rsqrt(r2);
+          const double f = sm[jj] * (inv * inv * inv);
           ax += f * dx; ay += f * dy; az += f * dz;
         }
       }
