@@ -354,11 +354,8 @@ __device__ __forceinline__ double seed_sort(const KnnArgs& A, int64_t jl, int64_
 }
 
 // The same sort on distances alone: a squared distance is non-negative, so
-// its bit pattern orders like its value and one 64-bit key stands for the
-// (distance, index) pair whenever no two finite distances among the 64 are
-// equal.  Returns false (list untouched) when such an exact tie exists; the
-// caller then sorts with the particle indices (seed_sort).  Empty candidates
-// (+inf) may tie among themselves: they are never list entries.
+// its bit pattern orders like its value.  seed_key gives those bits for
+// element e of a query's 64 seed candidates (+inf for none).
 __device__ __forceinline__ unsigned long long seed_key(const KnnArgs& A, int64_t jl, int64_t jn, int64_t self,
                                                        double qx, double qy, double qz, int e, bool wrap) {
   const int64_t p = (e < 32) ? jl * kLeaf + e : jn * kLeaf + (e - 32);
@@ -368,15 +365,21 @@ __device__ __forceinline__ unsigned long long seed_key(const KnnArgs& A, int64_t
   return (unsigned long long)__double_as_longlong(d);
 }
 
+// Sort keys carry the element number in their 6 lowest bits (the squared
+// distance's last mantissa bits are dropped), so one 64-bit value moves
+// through the network.  The order is exact between keys whose upper 58 bits
+// differ; keys sharing them (distances within 2^-46 relative, or exact ties)
+// sit next to each other after the sort, and then the function returns false
+// and the caller sorts again exactly with the particle indices (seed_sort).
+// Empty candidates (+inf) may share them: they are never list entries.
 template <int C>
 __device__ __forceinline__ bool seed_sort_keys(const KnnArgs& A, int64_t jl, int64_t jn, int64_t self, double qx,
                                                double qy, double qz, int lane, unsigned char* list, double& kth,
                                                bool wrap) {
   const int nvv = C ? C : A.nv;
-  const unsigned long long kInf = 0x7FF0000000000000ull;
-  unsigned long long k0 = seed_key(A, jl, jn, self, qx, qy, qz, lane, wrap);
-  unsigned long long k1 = seed_key(A, jl, jn, self, qx, qy, qz, 32 + lane, wrap);
-  int32_t s0 = lane, s1 = 32 + lane;
+  const unsigned long long kInfHi = 0x7FF0000000000000ull >> 6;
+  unsigned long long k0 = (seed_key(A, jl, jn, self, qx, qy, qz, lane, wrap) & ~63ull) | (unsigned)lane;
+  unsigned long long k1 = (seed_key(A, jl, jn, self, qx, qy, qz, 32 + lane, wrap) & ~63ull) | (unsigned)(32 + lane);
 #pragma unroll
   for (int size = 2; size <= 64; size <<= 1) {
     const bool asc = ((2 * lane) & size) == 0;
@@ -385,29 +388,31 @@ __device__ __forceinline__ bool seed_sort_keys(const KnnArgs& A, int64_t jl, int
       if (stride == 1) {
         if (asc ? (k1 < k0) : (k0 < k1)) {
           const unsigned long long tk = k0; k0 = k1; k1 = tk;
-          const int32_t ts = s0; s0 = s1; s1 = ts;
         }
       } else {
         const int ls = stride >> 1;
         const unsigned long long pk0 = __shfl_xor_sync(0xffffffffu, k0, ls), pk1 = __shfl_xor_sync(0xffffffffu, k1, ls);
-        const int32_t ps0 = __shfl_xor_sync(0xffffffffu, s0, ls), ps1 = __shfl_xor_sync(0xffffffffu, s1, ls);
         const bool kmin = (((lane & ls) == 0) == asc);
-        if (kmin ? (pk0 < k0) : (k0 < pk0)) { k0 = pk0; s0 = ps0; }
-        if (kmin ? (pk1 < k1) : (k1 < pk1)) { k1 = pk1; s1 = ps1; }
+        if (kmin ? (pk0 < k0) : (k0 < pk0)) k0 = pk0;
+        if (kmin ? (pk1 < k1) : (k1 < pk1)) k1 = pk1;
       }
     }
   }
-  // sorted element 2*lane + slot: look for equal finite neighbours
-  const unsigned long long nx = __shfl_down_sync(0xffffffffu, k0, 1);
-  const bool tie = (k0 == k1 && k0 != kInf) || (lane < 31 && k1 == nx && k1 != kInf);
+  // sorted element 2*lane + slot: look for finite neighbours sharing the upper bits
+  const unsigned long long h0 = k0 >> 6, h1 = k1 >> 6;
+  const unsigned long long nx = __shfl_down_sync(0xffffffffu, h0, 1);
+  const bool tie = (h0 == h1 && h0 != kInfHi) || (lane < 31 && h1 == nx && h1 != kInfHi);
   if (__any_sync(0xffffffffu, tie)) return false;
   if (lane < 16) {
-    list[2 * lane] = (unsigned char)s0;
-    list[2 * lane + 1] = (unsigned char)s1;
+    list[2 * lane] = (unsigned char)(k0 & 63u);
+    list[2 * lane + 1] = (unsigned char)(k1 & 63u);
   }
+  // the nv-th distance, rounded up in its dropped bits (a bound for the
+  // candidate search), +inf when fewer than nv candidates exist
   const int e = nvv - 1;
   const unsigned long long a = __shfl_sync(0xffffffffu, k0, e >> 1), b = __shfl_sync(0xffffffffu, k1, e >> 1);
-  kth = __longlong_as_double((long long)((e & 1) ? b : a));
+  const unsigned long long kk = (e & 1) ? b : a;
+  kth = (kk >> 6) == kInfHi ? CUDART_INF : __longlong_as_double((long long)(kk | 63ull));
   return true;
 }
 
