@@ -606,6 +606,10 @@ def main():
                  "ideal_visits_per_query": ts[18] / n, "chunks_per_query": ts[26] / n,
                  "ballot_hits_per_query": ts[27] / n,
                  "union_visits_per_query_leaf": ts[28] / max(1, ts[29])}
+    ph = [float(ts[21 + k]) for k in range(5)]
+    if sum(ph) > 0:
+        knn_stats["cycle_share"] = {k: v / sum(ph) for k, v in zip(
+            ("bound_and_seed_sort", "candidates_and_sort", "seed_lists", "scan", "density"), ph)}
     mean_stage = {k: statistics.mean(s[k] for s in stage) for k in
                   ("tree", "knn_density", "hop_groups", "saddles", "nodes", "membership", "total")}
     line = {"metric": METRIC, "value": value, "unit": "Mpart/s", "n_gpus": world, "steps": args.steps,
