@@ -219,6 +219,10 @@ struct SharedTask {
   int32_t inode, a, b, level, ncomp, nsurv, nsisters, done, nexact, inode1, kk;
   int32_t flag, nbig;
   long long iters;
+  // the task the block runs next (a child it continues), and its size at start
+  unsigned long long best;
+  Task cont;
+  int32_t has_cont, groups0;
 };
 
 template <int NT, class SortT, class ScanT, class MaxScanT>
@@ -940,17 +944,26 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
   __shared__ long long s_clk[6];  // structural, approx, exact cycles; levels; structural passes; max ncomp
   __shared__ long long s_ph[8];   // cycles per phase of the structural passes
   const int tid = threadIdx.x;
-  const long long t_start = clock64();
+  if (tid == 0) T.cont = tasks[blockIdx.x];
+  // A block runs its task and then, when the task branches, one of the new
+  // children itself (the one with the most groups) instead of leaving it to
+  // the next wave: the longest chains of the tree no longer wait at every
+  // wave boundary.  The children's work is independent, so this changes
+  // only the schedule, not the nodes (their ids are renumbered at the end).
+  for (;;) {
+  long long t_start = clock64();
   if (tid < 6) s_clk[tid] = 0;
   if (tid < 8) s_ph[tid] = 0;
   if (tid == 0) {
-    const Task t = tasks[blockIdx.x];
+    const Task t = T.cont;
     T.rhot = t.rhot; T.inode = t.inode; T.a = t.a; T.b = t.b; T.level = t.level;
+    T.groups0 = t.b - t.a;
     T.next_event = -DBL_MAX;  // force a structural pass first
     T.nsurv = 0;
     T.ncomp = 0;
     T.done = 0;
     T.iters = 0;
+    T.has_cont = 0;
   }
   __syncthreads();
   while (true) {
@@ -1027,6 +1040,18 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
     }
     __syncthreads();
     if (T.done) break;
+    // the child this block continues: the significant component with the
+    // most groups (ties: the first), packed as (groups, ~index) for atomicMax
+    if (tid == 0) T.best = 0ull;
+    __syncthreads();
+    for (int32_t k = tid; k < T.ncomp; k += NT) {
+      if (A.cs[12 * (size_t)(T.a + k) + 9] == 1.0) {
+        const unsigned long long ng_k = (unsigned long long)(comp_end(A, T, k) - A.cstart[T.a + k]);
+        atomicMax(&T.best, (ng_k << 32) | (unsigned long long)(0xffffffffu - (unsigned)k));
+      }
+    }
+    __syncthreads();
+    const int32_t kc = (int32_t)(0xffffffffu - (unsigned)(T.best & 0xffffffffull));
     {
       int32_t carry = 0;
       for (int32_t k0 = 0; k0 < T.ncomp; k0 += NT) {
@@ -1052,7 +1077,13 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
           if (nd.mass == 0) set_err(A, 15, io);  // f90:1506-1510
           // child task (f90:1543-1556)
           const double rc = xmul(T.rhot, xadd(1.0, xdiv(A.fudge, xsqrt(C[1]))));
-          push_task(A, Task{rc, io, A.cstart[T.a + k], comp_end(A, T, k), T.level + 1});
+          const Task child{rc, io, A.cstart[T.a + k], comp_end(A, T, k), T.level + 1};
+          if (k == kc) {
+            T.cont = child;
+            T.has_cont = 1;
+          } else {
+            push_task(A, child);
+          }
         }
         carry += tot;
       }
@@ -1076,9 +1107,8 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
     atomicMax(&A.stats[5], (unsigned long long)s_clk[3]);
     atomicMax(&A.stats[6], (unsigned long long)(s_clk[0] + s_clk[1] + s_clk[2]));
     if (A.tprof) {
-      const Task t = tasks[blockIdx.x];
-      long long* r = A.tprof + 16 * (size_t)t.inode;
-      r[0] = t.b - t.a;       // groups in the task's range
+      long long* r = A.tprof + 16 * (size_t)T.inode;
+      r[0] = T.groups0;       // groups in the task's range
       r[1] = s_clk[3];        // levels
       r[2] = s_clk[4];        // structural passes
       r[3] = s_clk[0];        // cycles: structural
@@ -1088,6 +1118,11 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
       r[7] = s_clk[5];        // largest component count at one level
       for (int k = 0; k < 8; ++k) r[8 + k] = s_ph[k];  // structural phases
     }
+  }
+  __syncthreads();
+  const bool more = T.has_cont != 0;
+  __syncthreads();  // thread 0 rewrites T for the next task
+  if (!more) break;
   }
 }
 
