@@ -37,6 +37,9 @@ CASES = [
     ("ahop_case_a", 3000, 8, 11, 600),
     ("ahop_case_b", 5000, 16, 12, 800),
     ("ahop_case_c", 4000, 3, 13, 1500),
+    # a larger box: halos of up to 12,000 particles with subhalos, so the
+    # structure tree has several levels of significance tests
+    ("ahop_case_d", 40000, 30, 15, 12000),
 ]
 
 
