@@ -107,19 +107,61 @@ struct TreeArgs {
   Task* next_big;         // next wave's tasks of more than big_task groups (kNTBig-thread blocks)
   int32_t big_task;
   int32_t* nnext_big;
+  // a slot of next / next_big is readable once its flag is set; ntaken /
+  // ntaken_big count the slots that blocks of the current wave took over
+  int32_t* qready;
+  int32_t* qready_big;
+  int32_t* ntaken;
+  int32_t* ntaken_big;
   int32_t* err;           // [0] code, [1] detail
   unsigned long long* stats;  // [11] counters (see the end of tree_wave_kernel; [8..10] undecided tests)
   long long* tprof;       // [nnodesmax+1][16] per-task profile row by node id, or null
 };
 
-__device__ __forceinline__ void push_task(const TreeArgs& A, const Task& t) {
-  if (t.b - t.a > A.big_task) A.next_big[atomicAdd(A.nnext_big, 1)] = t;
-  else A.next[atomicAdd(A.nnext, 1)] = t;
-}
-
 __device__ __forceinline__ void set_err(const TreeArgs& A, int code, int detail) {
   if (atomicCAS(A.err, 0, code) == 0) A.err[1] = detail;
 }
+
+__device__ __forceinline__ void push_task(const TreeArgs& A, const Task& t) {
+  const bool big = t.b - t.a > A.big_task;
+  const int32_t s = atomicAdd(big ? A.nnext_big : A.nnext, 1);
+  (big ? A.next_big : A.next)[s] = t;
+  __threadfence();
+  atomicExch((big ? A.qready_big : A.qready) + s, 1);
+}
+
+constexpr long long kTakeSpin = 1LL << 22;  // waits for a claimed slot's record (bounded; an error past it)
+
+// Take a queued task of the next wave, if one is there (one thread).  A slot
+// is claimed by advancing the taken counter past it while it is below the
+// pushed count; its record was claimed by a pusher that writes it at once,
+// so the wait for its flag is short.  Returns false when the queue is empty.
+__device__ bool take_task(const TreeArgs& A, bool big, Task& out) {
+  int32_t* taken = big ? A.ntaken_big : A.ntaken;
+  const int32_t* pushed = big ? A.nnext_big : A.nnext;
+  for (;;) {
+    const int32_t t = atomicAdd(taken, 0);
+    const int32_t n = atomicAdd(const_cast<int32_t*>(pushed), 0);
+    if (t >= n) return false;
+    if (atomicCAS(taken, t, t + 1) != t) continue;
+    int32_t* ready = (big ? A.qready_big : A.qready) + t;
+    long long it = 0;
+    while (atomicAdd(ready, 0) == 0) {
+      if (++it > kTakeSpin) { set_err(A, 18, t); return false; }
+      __nanosleep(64);
+    }
+    __threadfence();
+    // another SM wrote the record in this launch: read it past L1
+    const Task* r = (big ? A.next_big : A.next) + t;
+    out.rhot = __ldcg(&r->rhot);
+    out.inode = __ldcg(&r->inode);
+    out.a = __ldcg(&r->a);
+    out.b = __ldcg(&r->b);
+    out.level = __ldcg(&r->level);
+    return true;
+  }
+}
+
 
 __device__ __forceinline__ double wrapd(double d, double L, double h) {
   // f90:2359-2373 / 1516-1532
@@ -1119,6 +1161,15 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
       for (int k = 0; k < 8; ++k) r[8 + k] = s_ph[k];  // structural phases
     }
   }
+  // no child to continue: take a task that another block queued for the next
+  // wave (wide blocks take wide tasks first, then narrow ones)
+  if (tid == 0 && !T.has_cont) {
+    Task t;
+    if ((NT >= kNTBig && take_task(A, true, t)) || take_task(A, false, t)) {
+      T.cont = t;
+      T.has_cont = 1;
+    }
+  }
   __syncthreads();
   const bool more = T.has_cont != 0;
   __syncthreads();  // thread 0 rewrites T for the next task
@@ -1473,7 +1524,7 @@ int stage_nodes(Engine& E) {
   // every sub-array starts on a 256-byte boundary: size the buffer with the rounding
   auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
   const size_t need = r256(bytes_i) * 12 + r256(G * 8 * 8) + r256(G * 12 * 8) +
-                      r256((size_t)(nnodesmax + 1) * sizeof(Task)) * 4;
+                      r256((size_t)(nnodesmax + 1) * sizeof(Task)) * 4 + r256((size_t)(nnodesmax + 1) * 4) * 4;
   AHOP_CUDA_TRY(E.d_tree_scratch.ensure(need));
   char* p = static_cast<char*>(E.d_tree_scratch.p);
   auto take = [&](size_t b) { char* q = p; p += (b + 255) & ~size_t(255); return q; };
@@ -1499,11 +1550,19 @@ int stage_nodes(Engine& E) {
   tasks[1] = reinterpret_cast<Task*>(take((size_t)(nnodesmax + 1) * sizeof(Task)));
   tasksB[0] = reinterpret_cast<Task*>(take((size_t)(nnodesmax + 1) * sizeof(Task)));
   tasksB[1] = reinterpret_cast<Task*>(take((size_t)(nnodesmax + 1) * sizeof(Task)));
+  int32_t* ready[2];   // slot flags of tasks[k]
+  int32_t* readyB[2];  // ... of tasksB[k]
+  for (int k = 0; k < 2; ++k) {
+    ready[k] = reinterpret_cast<int32_t*>(take((size_t)(nnodesmax + 1) * 4));
+    readyB[k] = reinterpret_cast<int32_t*>(take((size_t)(nnodesmax + 1) * 4));
+  }
+  const size_t ready_bytes = (size_t)(nnodesmax + 1) * 4;
   AHOP_CUDA_TRY(E.d_nodes.ensure((size_t)(nnodesmax + 1) * sizeof(NodeRec)));
   AHOP_CUDA_TRY(cudaMemsetAsync(E.d_nodes.p, 0, (size_t)(nnodesmax + 1) * sizeof(NodeRec), st));
   AHOP_CUDA_TRY(E.d_flags.ensure(512));
   AHOP_CUDA_TRY(cudaMemsetAsync(E.d_flags.p, 0, 256, st));
-  int32_t* flags = E.d_flags.as<int32_t>();  // [0..1] err, [2] nnodes, [3] nnext, [4] nnext_big
+  // [0..1] err, [2] nnodes, [3] nnext, [4] nnext_big, [5] ntaken, [6] ntaken_big
+  int32_t* flags = E.d_flags.as<int32_t>();
   A.stats = reinterpret_cast<unsigned long long*>(E.d_flags.as<char>() + 128);
   A.tprof = nullptr;
   if (E.task_profile) {
@@ -1515,6 +1574,8 @@ int stage_nodes(Engine& E) {
   A.nnodes = flags + 2;
   A.nnext = flags + 3;
   A.nnext_big = flags + 4;
+  A.ntaken = flags + 5;
+  A.ntaken_big = flags + 6;
   A.x = E.d_x.as<double>(); A.y = E.d_y.as<double>(); A.z = E.d_z.as<double>(); A.m = E.d_m.as<double>();
   A.dens = E.d_dens.as<double>();
   A.orig = E.d_orig.as<int32_t>();
@@ -1537,6 +1598,7 @@ int stage_nodes(Engine& E) {
   AHOP_CUDA_TRY(cudaGetLastError());
   // root node 0 (f90:934-943): mass and truemass stay 0, densmax = max peak density
   int32_t nsmall = 0, nbig = 0;
+  int32_t off_s = 0, off_b = 0;  // first task of the launch lists not taken by blocks of the previous wave
   {
     const Task root{P.rho_threshold, 0, 0, ng, 0};
     const bool big = ng > A.big_task;
@@ -1599,7 +1661,9 @@ int stage_nodes(Engine& E) {
       // the root branches at once (the usual case): level-1 nodes 1..nsis
       A.next = tasks[1];
       A.next_big = tasksB[1];
-      AHOP_CUDA_TRY(cudaMemsetAsync(A.nnext, 0, 8, st));
+      A.qready = ready[1];
+      A.qready_big = readyB[1];
+      AHOP_CUDA_TRY(cudaMemsetAsync(A.nnext, 0, 16, st));
       E.launches++;
       root_nodes_kernel<<<(unsigned)((ncomp + T - 1) / T), T, 0, st>>>(A, ncomp, A.cnt, A.run, nsis, rhot);
       E.launches++;
@@ -1636,7 +1700,13 @@ int stage_nodes(Engine& E) {
     if (wave > 100000) { set_error("structure tree: too many waves"); return AHOP_ELIMIT; }
     A.next = tasks[cur ^ 1];
     A.next_big = tasksB[cur ^ 1];
-    AHOP_CUDA_TRY(cudaMemsetAsync(A.nnext, 0, 8, st));
+    A.qready = ready[cur ^ 1];
+    A.qready_big = readyB[cur ^ 1];
+    AHOP_CUDA_TRY(cudaMemsetAsync(ready[cur ^ 1], 0, ready_bytes, st));
+    AHOP_CUDA_TRY(cudaMemsetAsync(readyB[cur ^ 1], 0, ready_bytes, st));
+    AHOP_CUDA_TRY(cudaMemsetAsync(A.nnext, 0, 16, st));
+    Task* list_s = tasks[cur] + off_s;
+    Task* list_b = tasksB[cur] + off_b;
     if (nsmall > 2048) {
       const size_t nb = (size_t)nsmall;
       AHOP_CUDA_TRY(E.d_task_sort.ensure(nb * 16 + nb * sizeof(Task) + 256));
@@ -1646,7 +1716,7 @@ int stage_nodes(Engine& E) {
       int32_t* v1 = v0 + nb;
       Task* tmp = reinterpret_cast<Task*>(reinterpret_cast<char*>(E.d_task_sort.p) + ((nb * 16 + 255) & ~size_t(255)));
       E.launches += 2;
-      task_keys_kernel<<<(unsigned)((nb + T - 1) / T), T, 0, st>>>(tasks[cur], nsmall, k0, v0);
+      task_keys_kernel<<<(unsigned)((nb + T - 1) / T), T, 0, st>>>(list_s, nsmall, k0, v0);
       cub::DoubleBuffer<uint32_t> kb(k0, k1);
       cub::DoubleBuffer<int32_t> vb(v0, v1);
       size_t t1 = 0;
@@ -1654,8 +1724,8 @@ int stage_nodes(Engine& E) {
       AHOP_CUDA_TRY(E.d_cub.ensure(t1));
       E.cub_calls++;
       AHOP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(E.d_cub.p, t1, kb, vb, nsmall, 0, 32, st));
-      task_gather_kernel<<<(unsigned)((nb + T - 1) / T), T, 0, st>>>(tasks[cur], vb.Current(), nsmall, tmp);
-      AHOP_CUDA_TRY(cudaMemcpyAsync(tasks[cur], tmp, nb * sizeof(Task), cudaMemcpyDeviceToDevice, st));
+      task_gather_kernel<<<(unsigned)((nb + T - 1) / T), T, 0, st>>>(list_s, vb.Current(), nsmall, tmp);
+      AHOP_CUDA_TRY(cudaMemcpyAsync(list_s, tmp, nb * sizeof(Task), cudaMemcpyDeviceToDevice, st));
       AHOP_CUDA_TRY(cudaGetLastError());
     }
     const bool prof = E.task_profile && wave < kMaxProfiledWaves;
@@ -1667,7 +1737,7 @@ int stage_nodes(Engine& E) {
       AHOP_CUDA_TRY(cudaStreamWaitEvent(E.stream2, E.ev_fork, 0));
       if (prof) AHOP_CUDA_TRY(cudaEventRecord(E.wave_ev[2], E.stream2));
       E.launches++;
-      tree_wave_kernel<kNTBig><<<nbig, kNTBig, wave_dyn_smem(kNTBig), E.stream2>>>(A, tasksB[cur]);
+      tree_wave_kernel<kNTBig><<<nbig, kNTBig, wave_dyn_smem(kNTBig), E.stream2>>>(A, list_b);
       AHOP_CUDA_TRY(cudaGetLastError());
       if (prof) AHOP_CUDA_TRY(cudaEventRecord(E.wave_ev[3], E.stream2));
       AHOP_CUDA_TRY(cudaEventRecord(E.ev_join, E.stream2));
@@ -1675,12 +1745,12 @@ int stage_nodes(Engine& E) {
     if (prof) AHOP_CUDA_TRY(cudaEventRecord(E.wave_ev[0], st));
     if (nsmall > 0) {
       E.launches++;
-      tree_wave_kernel<kNT><<<nsmall, kNT, wave_dyn_smem(kNT), st>>>(A, tasks[cur]);
+      tree_wave_kernel<kNT><<<nsmall, kNT, wave_dyn_smem(kNT), st>>>(A, list_s);
       AHOP_CUDA_TRY(cudaGetLastError());
     }
     if (prof) AHOP_CUDA_TRY(cudaEventRecord(E.wave_ev[1], st));
     if (nbig > 0) AHOP_CUDA_TRY(cudaStreamWaitEvent(st, E.ev_join, 0));
-    AHOP_CUDA_TRY(cudaMemcpyAsync(h, flags, 20, cudaMemcpyDeviceToHost, st));
+    AHOP_CUDA_TRY(cudaMemcpyAsync(h, flags, 28, cudaMemcpyDeviceToHost, st));
     AHOP_CUDA_TRY(cudaStreamSynchronize(st));
     if (prof) {
       float ms_s = 0.f, ms_b = 0.f;
@@ -1693,10 +1763,13 @@ int stage_nodes(Engine& E) {
     if (h[0] != 0) {
       set_error("structure tree invariant failed (code " + std::to_string(h[0]) + ", detail " +
                 std::to_string(h[1]) + ")");
-      return h[0] == 12 ? AHOP_ELIMIT : AHOP_EINVARIANT;
+      return (h[0] == 12 || h[0] == 18) ? AHOP_ELIMIT : AHOP_EINVARIANT;
     }
-    nsmall = h[3];
-    nbig = h[4];
+    // tasks queued in this wave that no block took run in the next one
+    nsmall = h[3] - h[5];
+    nbig = h[4] - h[6];
+    off_s = h[5];
+    off_b = h[6];
     cur ^= 1;
     E.waves = wave + 1;
   }
