@@ -1124,7 +1124,14 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
             T.cont = child;
             T.has_cont = 1;
           } else {
-            push_task(A, child);
+            // queued only after this task's last reads of its range (below):
+            // a queued child may start at once in another block
+            double* Cw = A.cs + 12 * (size_t)(T.a + k);
+            Cw[3] = child.rhot;
+            Cw[4] = (double)child.inode;
+            Cw[5] = (double)child.a;
+            Cw[6] = (double)child.b;
+            Cw[7] = (double)child.level;
           }
         }
         carry += tot;
@@ -1136,6 +1143,12 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
     for (int32_t i = T.a + tid; i < T.b; i += NT) {
       const int32_t io = A.cnt[T.a + A.compidx[i]];
       if (io > 0) A.deepnode[A.GL[i]] = io;
+    }
+    __syncthreads();
+    for (int32_t k = tid; k < T.ncomp; k += NT) {
+      const double* C = A.cs + 12 * (size_t)(T.a + k);
+      if (C[9] == 1.0 && k != kc)
+        push_task(A, Task{C[3], (int32_t)C[4], (int32_t)C[5], (int32_t)C[6], (int32_t)C[7]});
     }
     break;
   }
