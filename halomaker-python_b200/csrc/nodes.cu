@@ -1705,7 +1705,12 @@ int stage_nodes(Engine& E) {
                                        (int)wave_dyn_smem(kNTBig)));
     AHOP_CUDA_TRY(cudaFuncSetAttribute(tree_wave_kernel<kNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)wave_dyn_smem(kNT)));
-    AHOP_CUDA_TRY(cudaStreamCreateWithFlags(&E.stream2, cudaStreamNonBlocking));
+    // the wide blocks run the largest tasks, the tree's critical path: their
+    // stream has the highest priority, so their blocks are scheduled first
+    // when SMs free up
+    int prio_lo = 0, prio_hi = 0;
+    AHOP_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    AHOP_CUDA_TRY(cudaStreamCreateWithPriority(&E.stream2, cudaStreamNonBlocking, prio_hi));
     AHOP_CUDA_TRY(cudaEventCreateWithFlags(&E.ev_fork, cudaEventDisableTiming));
     AHOP_CUDA_TRY(cudaEventCreateWithFlags(&E.ev_join, cudaEventDisableTiming));
   }
