@@ -245,7 +245,8 @@ __device__ __forceinline__ double qdist2(const KnnArgs& A, bool wrap, double qx,
 struct WarpList {
   double ld;
   int32_t ls;
-  double r2;  // squared distance of the nv-th entry (acceptance bound)
+  double r2;   // acceptance bound: the smaller of the nv-th entry and cap
+  double cap;  // an upper bound of the query's final nv-th distance known in advance (+inf: none)
 };
 
 // Insert the particles of one leaf that belong in the list.  Candidates at
@@ -287,7 +288,7 @@ __device__ __forceinline__ void leaf_insert(const KnnArgs& A, WarpList& L, int32
     // (pos = nv) and changes nothing
     mask &= ~(1u << src);
   }
-  L.r2 = __shfl_sync(0xffffffffu, L.ld, nvv - 1);
+  L.r2 = fmin(__shfl_sync(0xffffffffu, L.ld, nvv - 1), L.cap);
 }
 
 __device__ __forceinline__ bool key_less(double da, int32_t oa, double db, int32_t ob) {
@@ -430,7 +431,7 @@ __device__ __forceinline__ void seed_list(const KnnArgs& A, WarpList& L, int64_t
   L.ld = d;
   L.ls = (d < CUDART_INF) ? (int32_t)p : -1;
   if (lane >= nvv) { L.ld = CUDART_INF; L.ls = -1; }
-  L.r2 = __shfl_sync(0xffffffffu, L.ld, nvv - 1);
+  L.r2 = fmin(__shfl_sync(0xffffffffu, L.ld, nvv - 1), L.cap);
   nvis += (jn >= 0 && jn != jl) ? 2 : 1;
 }
 
@@ -719,12 +720,30 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
     // ---- C: per-query kNN over the candidates
     unsigned nvis = 0, nins = 0, nideal = 0, nchunk = 0, nbits = 0;
     unsigned visbits = 0;  // profiling: lane l holds candidates [32 l, 32 l + 32) visited by any query
+    int32_t prev_ls = -1;  // lane's entry of the previous query's final list
     for (int q = 0; q < nq; ++q) {
       const int64_t s = s0 + q;
       const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
       const float qxf = (float)qx, qyf = (float)qy, qzf = (float)qz;
       WarpList L;
       const long long tq0 = kProf ? clock64() : 0;
+      // A bound for this query from its predecessor in the leaf (a close
+      // particle): the previous query's nv neighbours, with this query
+      // replaced by the previous query itself, are nv distinct other
+      // particles, so the largest of their exact distances from this query
+      // bounds its nv-th distance.  It tightens the acceptance bound from the
+      // start (fewer visits and fewer insertions that later drop out).
+      L.cap = CUDART_INF;
+      if (q > 0) {
+        const int nvv = C ? C : A.nv;
+        int32_t ps = prev_ls;
+        if (ps == (int32_t)s) ps = (int32_t)s - 1;
+        double d = 0.0;
+        if (lane < nvv) d = ps >= 0 ? pdist2(qx, qy, qz, A.x[ps], A.y[ps], A.z[ps], A.Lx, A.Ly, A.Lz) : CUDART_INF;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
+        L.cap = d;
+      }
       const bool swrap = !(near_box(A.box32 + 2 * jl, qx, qy, qz, A.Lx, A.Ly, A.Lz) &&
                            near_box(A.box32 + 2 * jn, qx, qy, qz, A.Lx, A.Ly, A.Lz));
       seed_list<C>(A, L, jl, jn, s, qx, qy, qz, lane, s_list[wib][q], nvis, swrap);
@@ -782,6 +801,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
         }
       }
       const long long tq3 = kProf ? clock64() : 0;
+      prev_ls = L.ls;
       finish_query<C>(A, L, s, lane);
       __syncwarp();
       if (kProf) c_fin += clock64() - tq3;
