@@ -385,7 +385,7 @@ int ahop_debug_task_profile(int64_t* out, int32_t maxrows) {
   if (!E.task_profile || !E.d_tprof.p) { set_error("task profile not enabled"); return AHOP_ESTATE; }
   const int64_t rows = std::min<int64_t>((int64_t)maxrows, (int64_t)2 * E.ngroups + 1);
   if (rows <= 0) return AHOP_OK;
-  AHOP_CUDA_TRY(cudaMemcpy(out, E.d_tprof.p, (size_t)rows * 128, cudaMemcpyDeviceToHost));
+  AHOP_CUDA_TRY(cudaMemcpy(out, E.d_tprof.p, (size_t)rows * kProfRow * 8, cudaMemcpyDeviceToHost));
   return AHOP_OK;
 }
 

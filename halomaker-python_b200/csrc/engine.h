@@ -76,6 +76,7 @@ constexpr int kLeaf = 32;         // particles per leaf bucket
 constexpr int kFan = 32;          // children per internal node
 constexpr int kMaxLevels = 8;
 constexpr int kMaxProfiledWaves = 64;
+constexpr int kProfRow = 32;  // int64 entries per structure-tree task-profile row
 
 struct Engine {
   Params prm;

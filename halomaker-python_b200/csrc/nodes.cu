@@ -51,12 +51,14 @@ constexpr int kTermWarps = 8;   // warps that sum large groups in an exact pass
 constexpr int kSmallComp = 4;   // components of at most this many groups are decided by one thread
 constexpr int kIPT = 4;         // items per thread in the reorder sort (2 for 1024-thread blocks)
 __host__ __device__ constexpr int ipt_for(int nt) { return nt >= 1024 ? 2 : kIPT; }
-// groups whose union-find parents a task block keeps in shared memory
+// most groups whose union-find parents a task block keeps in shared memory
+// (a 1024-thread launch sizes its array to its largest task, up to this)
 __host__ __device__ constexpr int par_cap(int nt) { return nt >= 1024 ? 32768 : 1024; }
 constexpr int kBigGroup = 96;   // groups larger than this are summed by a warp
 constexpr int kRowWarp = 8;     // saddle-row prefixes longer than this are linked by a warp
 constexpr int kMaxBigRows = 512;
 constexpr long long kMaxTaskLevels = 4000000LL;  // cap on one task's threshold levels (error, never a hang)
+constexpr int kProfPhases = 16;  // phase cycle counters per task (structural 0..7, 12; statistics 8..11)
 
 struct Task {
   double rhot;
@@ -107,6 +109,8 @@ struct TreeArgs {
   Task* next_big;         // next wave's tasks of more than big_task groups (kNTBig-thread blocks)
   int32_t big_task;
   int32_t* nnext_big;
+  int32_t* max_big;       // largest task pushed to next_big (bounds every task a wide launch runs)
+  int32_t par_cap_big;    // union-find parents in shared memory for wide tasks of at most this many groups
   // a slot of next / next_big is readable once its flag is set; ntaken /
   // ntaken_big count the slots that blocks of the current wave took over
   int32_t* qready;
@@ -115,7 +119,7 @@ struct TreeArgs {
   int32_t* ntaken_big;
   int32_t* err;           // [0] code, [1] detail
   unsigned long long* stats;  // [11] counters (see the end of tree_wave_kernel; [8..10] undecided tests)
-  long long* tprof;       // [nnodesmax+1][16] per-task profile row by node id, or null
+  long long* tprof;       // [nnodesmax+1][kProfRow] per-task profile row by node id, or null
 };
 
 __device__ __forceinline__ void set_err(const TreeArgs& A, int code, int detail) {
@@ -124,6 +128,7 @@ __device__ __forceinline__ void set_err(const TreeArgs& A, int code, int detail)
 
 __device__ __forceinline__ void push_task(const TreeArgs& A, const Task& t) {
   const bool big = t.b - t.a > A.big_task;
+  if (big) atomicMax(A.max_big, t.b - t.a);
   const int32_t s = atomicAdd(big ? A.nnext_big : A.nnext, 1);
   (big ? A.next_big : A.next)[s] = t;
   __threadfence();
@@ -173,11 +178,13 @@ __device__ __forceinline__ double wrapd(double d, double L, double h) {
 // number of members of group g with density > rhot (members sorted by
 // decreasing density).  A group's threshold only rises (a task's rhot grows
 // and children start above their parent), so the count is searched downward
-// from the group's previous count: a galloping step then a binary search.
-__device__ __forceinline__ int32_t count_above(const TreeArgs& A, int32_t g, double rhot) {
-  const double* r = A.rdesc + A.goff[g];
-  const int32_t hi = A.gcur[g];  // members [0, hi) were above the group's previous threshold
-  if (hi == 0 || r[hi - 1] > rhot) return hi;
+// from the group's previous count hi (members [0, hi) were above the group's
+// previous threshold; rlast = the density of member hi - 1, off = goff[g]):
+// a galloping step then a binary search.
+__device__ __forceinline__ int32_t count_above_at(const TreeArgs& A, int32_t g, int32_t off, int32_t hi, double rlast,
+                                                  double rhot) {
+  if (hi == 0 || rlast > rhot) return hi;
+  const double* r = A.rdesc + off;
   // r[j] <= rhot; gallop down until an index above rhot (or 0) brackets the answer
   int32_t j = hi - 1, lo = 0, step = 1;
   while (true) {
@@ -196,13 +203,18 @@ __device__ __forceinline__ int32_t count_above(const TreeArgs& A, int32_t g, dou
   return a2;
 }
 
+__device__ __forceinline__ int32_t count_above(const TreeArgs& A, int32_t g, double rhot) {
+  const int32_t off = A.goff[g], hi = A.gcur[g];
+  return count_above_at(A, g, off, hi, hi > 0 ? A.rdesc[off + hi - 1] : 0.0, rhot);
+}
+
 // number of saddle-row entries of group g above rhot (the row is sorted by
-// decreasing saddle), searched downward from the previous count like
-// count_above.
-__device__ __forceinline__ int32_t edges_above(const TreeArgs& A, int32_t g, double rhot) {
-  const double* r = A.srho + A.soff[g - 1];
-  const int32_t hi = A.ecur[g];
-  if (hi == 0 || r[hi - 1] > rhot) return hi;
+// decreasing saddle), searched downward from the previous count hi like
+// count_above (e0 = the row's start, rlast = the saddle of entry hi - 1).
+__device__ __forceinline__ int32_t edges_above_at(const TreeArgs& A, int32_t g, int32_t e0, int32_t hi, double rlast,
+                                                  double rhot) {
+  if (hi == 0 || rlast > rhot) return hi;
+  const double* r = A.srho + e0;
   int32_t j = hi - 1, lo = 0, step = 1;
   while (true) {
     const int32_t k = j - step;
@@ -276,7 +288,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   const int32_t a = T.a, b = T.b;
   // union-find parents: in shared memory when the task fits (entries relative
   // to a), else the global array (absolute positions)
-  const bool local = (b - a) <= par_cap(NT);
+  const bool local = (b - a) <= (NT >= 1024 ? A.par_cap_big : par_cap(NT));
   int32_t* par = local ? s_par : A.par;
   const int32_t poff = local ? a : 0;
   const double rhot = T.rhot;
@@ -305,7 +317,8 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
     if (!(dg > rhot)) continue;
     ev = fmin(ev, dg);
     const int32_t e0 = A.soff[g - 1];
-    const int32_t ne = edges_above(A, g, rhot);
+    const int32_t c = A.ecur[g];
+    const int32_t ne = edges_above_at(A, g, e0, c, c > 0 ? A.srho[e0 + c - 1] : 0.0, rhot);
     if (ne == 0) continue;
     ev = fmin(ev, A.srho[e0 + ne - 1]);
     if (ne > kRowWarp) {
@@ -323,6 +336,7 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   for (int o = 16; o > 0; o >>= 1) ev = fmin(ev, __shfl_xor_sync(0xffffffffu, ev, o));
   if ((tid & 31) == 0 && ev < DBL_MAX) atomic_min_pos(&T.next_event, ev);
   __syncthreads();
+  mark(12);
   {
     const int lane = tid & 31;
     const int32_t nbig = min(T.nbig, kMaxBigRows);
@@ -487,18 +501,13 @@ __device__ __forceinline__ int tri_gt(double v, double t, double e) {
 // 0 densg, 1 sum rho, 2 mass, 3..5 first moments about the anchor, 6 second
 // moment, 7 tri-state test "mean density of the group above rhot";
 // gn[i] = members above rhot (exact).
-__device__ __forceinline__ void position_terms(const TreeArgs& A, int32_t i, double rhot, const double* a) {
+__device__ __forceinline__ void store_terms(const TreeArgs& A, int32_t i, int32_t ng, double dg, const double* P,
+                                            double dx, double dy, double dz, double rhot) {
   const double u = 1.1102230246251565e-16;
-  const int32_t g = A.GL[i];
-  const int32_t ng = count_above(A, g, rhot);
   double* G = A.gs + 8 * (size_t)i;
   A.gn[i] = ng;
   double t[7] = {0, 0, 0, 0, 0, 0, (double)kFalse};
   if (ng > 0) {
-    const double* P = A.pref + 6 * (size_t)(A.goff[g] + ng - 1);
-    const int32_t pg = A.gpeak[g];
-    const double dx = wrapd(A.x[pg] - a[0], A.Lx, A.hx), dy = wrapd(A.y[pg] - a[1], A.Ly, A.hy),
-                 dz = wrapd(A.z[pg] - a[2], A.Lz, A.hz);
     const double sg = P[0], mg = P[1];
     t[0] = sg;
     t[1] = mg;
@@ -510,9 +519,26 @@ __device__ __forceinline__ void position_terms(const TreeArgs& A, int32_t i, dou
     const double vg = (sg / dn) / (1.0 + A.fudge / sqrt(dn));
     t[6] = (double)tri_gt(vg, rhot, (2.0 * dn + 8.0) * u * fabs(vg) * 1.01);
   }
-  G[0] = A.densg[g];
+  G[0] = dg;
 #pragma unroll
   for (int c = 0; c < 7; ++c) G[1 + c] = t[c];
+}
+
+__device__ __forceinline__ void position_terms(const TreeArgs& A, int32_t i, double rhot, const double* a) {
+  const int32_t g = A.GL[i];
+  const int32_t ng = count_above(A, g, rhot);
+  double P[6] = {0, 0, 0, 0, 0, 0};
+  double dx = 0, dy = 0, dz = 0;
+  if (ng > 0) {
+    const double* Pp = A.pref + 6 * (size_t)(A.goff[g] + ng - 1);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) P[c] = Pp[c];
+    const int32_t pg = A.gpeak[g];
+    dx = wrapd(A.x[pg] - a[0], A.Lx, A.hx);
+    dy = wrapd(A.y[pg] - a[1], A.Ly, A.hy);
+    dz = wrapd(A.z[pg] - a[2], A.Lz, A.hz);
+  }
+  store_terms(A, i, ng, A.densg[g], P, dx, dy, dz, rhot);
 }
 
 // Sum the gs rows of positions [c0, c1) over one warp and decide the
@@ -620,14 +646,83 @@ __device__ void component_decide(const TreeArgs& A, int32_t c0, int32_t c1, doub
   decide_from_sums(A, rhot, nl, nmax, dmax, S, M, Sx, Sy, Sz, Q, triB, C);
 }
 
-// Approximate statistics of every component of the task: anchors, then the
-// groups' terms position-parallel over the whole block, then a warp per
-// component sums them and decides.
+// component_decide for a large component on the whole block: every thread
+// sums a strided share of its rows, warps fold their lanes, warp 0 folds the
+// warps.  (The three-state test's bounds hold for any summation order.)
+struct CompSums {
+  long long nl;
+  int32_t nmax, triB;
+  double dmax, S, M, Sx, Sy, Sz, Q;
+};
+
 template <int NT>
-__device__ void approx_stats(const TreeArgs& A, SharedTask& T) {
+__device__ void component_decide_block(const TreeArgs& A, int32_t c0, int32_t c1, double rhot, double* C,
+                                       CompSums* red) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  CompSums s{0, 0, kFalse, -1.0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 4
+  for (int32_t i = c0 + tid; i < c1; i += NT) {
+    const double* G = A.gs + 8 * (size_t)i;
+    const int32_t ng = A.gn[i];
+    s.nl += ng;
+    s.nmax = max(s.nmax, ng);
+    s.dmax = fmax(s.dmax, G[0]);
+    s.S += G[1];
+    s.M += G[2];
+    s.Sx += G[3];
+    s.Sy += G[4];
+    s.Sz += G[5];
+    s.Q += G[6];
+    s.triB = tri_or(s.triB, (int)G[7]);
+  }
+  auto fold = [&](CompSums& v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      v.nl += __shfl_xor_sync(0xffffffffu, v.nl, o);
+      v.nmax = max(v.nmax, __shfl_xor_sync(0xffffffffu, v.nmax, o));
+      v.dmax = fmax(v.dmax, __shfl_xor_sync(0xffffffffu, v.dmax, o));
+      v.S += __shfl_xor_sync(0xffffffffu, v.S, o);
+      v.M += __shfl_xor_sync(0xffffffffu, v.M, o);
+      v.Sx += __shfl_xor_sync(0xffffffffu, v.Sx, o);
+      v.Sy += __shfl_xor_sync(0xffffffffu, v.Sy, o);
+      v.Sz += __shfl_xor_sync(0xffffffffu, v.Sz, o);
+      v.Q += __shfl_xor_sync(0xffffffffu, v.Q, o);
+      v.triB = tri_or(v.triB, __shfl_xor_sync(0xffffffffu, v.triB, o));
+    }
+  };
+  fold(s);
+  if (lane == 0) red[warp] = s;
+  __syncthreads();
+  if (warp == 0) {
+    CompSums w = (lane < NT / 32) ? red[lane] : CompSums{0, 0, kFalse, -1.0, 0, 0, 0, 0, 0, 0};
+    fold(w);
+    if (lane == 0) decide_from_sums(A, rhot, w.nl, w.nmax, w.dmax, w.S, w.M, w.Sx, w.Sy, w.Sz, w.Q, w.triB, C);
+  }
+  __syncthreads();  // red is reused by the next component
+}
+
+// components of more groups than this are summed by the whole block
+__host__ __device__ constexpr int block_comp_for(int nt) { return nt >= 1024 ? 512 : 1024; }
+constexpr int kMaxBlockComps = 32;
+
+// Approximate statistics of every component of the task: anchors, then the
+// groups' terms position-parallel over the whole block, then a thread per
+// small component, a warp per mid-sized one and the whole block per large
+// one sums them and decides.
+// s_bc (kMaxBlockComps entries) and s_red (NT / 32) are scratch that the
+// block's other phases own (no extra shared memory: that would shrink L1);
+// T.nbig counts the large components here.
+template <int NT>
+__device__ void approx_stats(const TreeArgs& A, SharedTask& T, long long* ph, int32_t* s_bc, CompSums* s_red) {
+  int32_t& s_nbc = T.nbig;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const double rhot = T.rhot;
   const int32_t a = T.a, b = T.b, ncomp = T.ncomp;
+  long long tl = clock64();
+  auto mark = [&](int k) {
+    if (tid == 0) { const long long t = clock64(); ph[k] += t - tl; tl = t; }
+  };
+  if (tid == 0) s_nbc = 0;
   for (int32_t k = tid; k < ncomp; k += NT) {
     const int32_t p0 = A.gpeak[A.GL[A.cstart[a + k]]];
     double* C = A.cs + 12 * (size_t)(a + k);
@@ -636,18 +731,37 @@ __device__ void approx_stats(const TreeArgs& A, SharedTask& T) {
     C[11] = A.z[p0];
   }
   __syncthreads();
+  mark(8);
   for (int32_t i = a + tid; i < b; i += NT) position_terms(A, i, rhot, A.cs + 12 * (size_t)(a + A.compidx[i]) + 9);
   __syncthreads();
-  // components of a few groups on one thread each, larger ones a warp each
+  mark(9);
   for (int32_t k = tid; k < ncomp; k += NT) {
     const int32_t c0 = A.cstart[a + k], c1 = comp_end(A, T, k);
-    if (c1 - c0 <= kSmallComp) component_decide_thread(A, c0, c1, rhot, A.cs + 12 * (size_t)(a + k));
-  }
-  for (int32_t k = warp; k < ncomp; k += NT / 32) {
-    const int32_t c0 = A.cstart[a + k], c1 = comp_end(A, T, k);
-    if (c1 - c0 > kSmallComp) component_decide(A, c0, c1, rhot, A.cs + 12 * (size_t)(a + k), lane);
+    if (c1 - c0 <= kSmallComp) {
+      component_decide_thread(A, c0, c1, rhot, A.cs + 12 * (size_t)(a + k));
+    } else if (c1 - c0 > block_comp_for(NT)) {
+      const int32_t slot = atomicAdd(&s_nbc, 1);
+      if (slot < kMaxBlockComps) s_bc[slot] = k;
+    }
   }
   __syncthreads();
+  mark(10);
+  // more large components than the list holds: warps take all of them
+  const int32_t nbc = s_nbc;
+  const bool by_block = nbc <= kMaxBlockComps;
+  for (int32_t k = warp; k < ncomp; k += NT / 32) {
+    const int32_t c0 = A.cstart[a + k], c1 = comp_end(A, T, k);
+    if (c1 - c0 > kSmallComp && !(by_block && c1 - c0 > block_comp_for(NT)))
+      component_decide(A, c0, c1, rhot, A.cs + 12 * (size_t)(a + k), lane);
+  }
+  if (by_block) {
+    for (int32_t j = 0; j < nbc; ++j) {
+      const int32_t k = s_bc[j];
+      component_decide_block<NT>(A, A.cstart[a + k], comp_end(A, T, k), rhot, A.cs + 12 * (size_t)(a + k), s_red);
+    }
+  }
+  __syncthreads();
+  mark(11);
 }
 
 // Exact per-group sums in the reference order (treat_particles f90:2317-2401):
@@ -961,13 +1075,17 @@ __global__ void task_gather_kernel(const Task* __restrict__ in, const int32_t* _
   if (i < n) out[i] = in[idx[i]];
 }
 
-// Dynamic shared memory of a task block: exact-sum staging (kTermWarps warps),
-// reorder keys, warp-linked row positions, union-find parents of tasks of at
-// most par_cap groups.
-__host__ __device__ constexpr size_t wave_dyn_smem(int nt) {
+// Dynamic shared memory of a task block: exact-sum staging (kTermWarps warps;
+// also the block fold of approx_stats), reorder keys, warp-linked row
+// positions (also approx_stats' list of large components), union-find
+// parents of tasks of at most pcap groups.  What the block does not take
+// stays L1, which the per-group loads of every level hit.
+__host__ __device__ constexpr size_t wave_dyn_smem(int nt, int pcap) {
   return (size_t)kTermWarps * 32 * 6 * 8 + (size_t)nt * ipt_for(nt) * 4 + (size_t)kMaxBigRows * 4 +
-         (size_t)par_cap(nt) * 4;
+         (size_t)pcap * 4;
 }
+static_assert(kTermWarps * 32 * 6 * 8 >= 32 * (int)sizeof(CompSums) && kMaxBigRows >= kMaxBlockComps,
+              "approx_stats scratch must fit the regions it borrows");
 
 template <int NT>
 __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeArgs A, const Task* __restrict__ tasks) {
@@ -984,7 +1102,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
   int32_t* s_par = s_big + kMaxBigRows;
   __shared__ SharedTask T;
   __shared__ long long s_clk[6];  // structural, approx, exact cycles; levels; structural passes; max ncomp
-  __shared__ long long s_ph[8];   // cycles per phase of the structural passes
+  __shared__ long long s_ph[kProfPhases];  // cycles per phase of the structural passes and statistics
   const int tid = threadIdx.x;
   if (tid == 0) T.cont = tasks[blockIdx.x];
   // A block runs its task and then, when the task branches, one of the new
@@ -995,7 +1113,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
   for (;;) {
   long long t_start = clock64();
   if (tid < 6) s_clk[tid] = 0;
-  if (tid < 8) s_ph[tid] = 0;
+  if (tid < kProfPhases) s_ph[tid] = 0;
   if (tid == 0) {
     const Task t = T.cont;
     T.rhot = t.rhot; T.inode = t.inode; T.a = t.a; T.b = t.b; T.level = t.level;
@@ -1024,7 +1142,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
       if (tid == 0) A.node[T.inode].firstchild = 0;
       break;
     }
-    approx_stats<NT>(A, T);
+    approx_stats<NT>(A, T, s_ph, s_big, reinterpret_cast<CompSums*>(s_terms));
     if (tid == 0) {
       s_clk[1] += clock64() - c1;
       T.nexact = 0;
@@ -1162,7 +1280,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
     atomicMax(&A.stats[5], (unsigned long long)s_clk[3]);
     atomicMax(&A.stats[6], (unsigned long long)(s_clk[0] + s_clk[1] + s_clk[2]));
     if (A.tprof) {
-      long long* r = A.tprof + 16 * (size_t)T.inode;
+      long long* r = A.tprof + kProfRow * (size_t)T.inode;
       r[0] = T.groups0;       // groups in the task's range
       r[1] = s_clk[3];        // levels
       r[2] = s_clk[4];        // structural passes
@@ -1171,7 +1289,8 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
       r[5] = s_clk[2];        // cycles: exact sums
       r[6] = clock64() - t_start;  // cycles: whole task
       r[7] = s_clk[5];        // largest component count at one level
-      for (int k = 0; k < 8; ++k) r[8 + k] = s_ph[k];  // structural phases
+      for (int k = 0; k < kProfPhases; ++k) r[8 + k] = s_ph[k];  // phases
+      r[24] = A.node[T.inode].mother;  // creation-time node id of the mother
     }
   }
   // no child to continue: take a task that another block queued for the next
@@ -1574,13 +1693,13 @@ int stage_nodes(Engine& E) {
   AHOP_CUDA_TRY(cudaMemsetAsync(E.d_nodes.p, 0, (size_t)(nnodesmax + 1) * sizeof(NodeRec), st));
   AHOP_CUDA_TRY(E.d_flags.ensure(512));
   AHOP_CUDA_TRY(cudaMemsetAsync(E.d_flags.p, 0, 256, st));
-  // [0..1] err, [2] nnodes, [3] nnext, [4] nnext_big, [5] ntaken, [6] ntaken_big
+  // [0..1] err, [2] nnodes, [3] nnext, [4] nnext_big, [5] ntaken, [6] ntaken_big, [7] max_big
   int32_t* flags = E.d_flags.as<int32_t>();
   A.stats = reinterpret_cast<unsigned long long*>(E.d_flags.as<char>() + 128);
   A.tprof = nullptr;
   if (E.task_profile) {
-    AHOP_CUDA_TRY(E.d_tprof.ensure((size_t)(nnodesmax + 1) * 128));
-    AHOP_CUDA_TRY(cudaMemsetAsync(E.d_tprof.p, 0, (size_t)(nnodesmax + 1) * 128, st));
+    AHOP_CUDA_TRY(E.d_tprof.ensure((size_t)(nnodesmax + 1) * kProfRow * 8));
+    AHOP_CUDA_TRY(cudaMemsetAsync(E.d_tprof.p, 0, (size_t)(nnodesmax + 1) * kProfRow * 8, st));
     A.tprof = E.d_tprof.as<long long>();
   }
   A.err = flags;
@@ -1589,6 +1708,8 @@ int stage_nodes(Engine& E) {
   A.nnext_big = flags + 4;
   A.ntaken = flags + 5;
   A.ntaken_big = flags + 6;
+  A.max_big = flags + 7;
+  A.par_cap_big = par_cap(kNTBig);
   A.x = E.d_x.as<double>(); A.y = E.d_y.as<double>(); A.z = E.d_z.as<double>(); A.m = E.d_m.as<double>();
   A.dens = E.d_dens.as<double>();
   A.orig = E.d_orig.as<int32_t>();
@@ -1611,6 +1732,7 @@ int stage_nodes(Engine& E) {
   AHOP_CUDA_TRY(cudaGetLastError());
   // root node 0 (f90:934-943): mass and truemass stay 0, densmax = max peak density
   int32_t nsmall = 0, nbig = 0;
+  int32_t max_big = ng;  // largest task of the next wide launch (every task its blocks take is smaller)
   int32_t off_s = 0, off_b = 0;  // first task of the launch lists not taken by blocks of the previous wave
   {
     const Task root{P.rho_threshold, 0, 0, ng, 0};
@@ -1676,7 +1798,7 @@ int stage_nodes(Engine& E) {
       A.next_big = tasksB[1];
       A.qready = ready[1];
       A.qready_big = readyB[1];
-      AHOP_CUDA_TRY(cudaMemsetAsync(A.nnext, 0, 16, st));
+      AHOP_CUDA_TRY(cudaMemsetAsync(A.nnext, 0, 20, st));
       E.launches++;
       root_nodes_kernel<<<(unsigned)((ncomp + T - 1) / T), T, 0, st>>>(A, ncomp, A.cnt, A.run, nsis, rhot);
       E.launches++;
@@ -1684,10 +1806,11 @@ int stage_nodes(Engine& E) {
       AHOP_CUDA_TRY(cudaGetLastError());
       h[5] = nsis;
       AHOP_CUDA_TRY(cudaMemcpyAsync(A.nnodes, h + 5, 4, cudaMemcpyHostToDevice, st));
-      AHOP_CUDA_TRY(cudaMemcpyAsync(h, flags, 20, cudaMemcpyDeviceToHost, st));
+      AHOP_CUDA_TRY(cudaMemcpyAsync(h, flags, 32, cudaMemcpyDeviceToHost, st));
       AHOP_CUDA_TRY(cudaStreamSynchronize(st));
       nsmall = h[3];
       nbig = h[4];
+      max_big = h[7];
       cur = 1;
     } else {
       // zero or one significant colour: the root task continues (f90:1577-1626)
@@ -1702,9 +1825,9 @@ int stage_nodes(Engine& E) {
   // in wider blocks on a second stream at the same time.
   if (!E.stream2) {
     AHOP_CUDA_TRY(cudaFuncSetAttribute(tree_wave_kernel<kNTBig>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)wave_dyn_smem(kNTBig)));
+                                       (int)wave_dyn_smem(kNTBig, par_cap(kNTBig))));
     AHOP_CUDA_TRY(cudaFuncSetAttribute(tree_wave_kernel<kNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)wave_dyn_smem(kNT)));
+                                       (int)wave_dyn_smem(kNT, par_cap(kNT))));
     // the wide blocks run the largest tasks, the tree's critical path: their
     // stream has the highest priority, so their blocks are scheduled first
     // when SMs free up
@@ -1722,7 +1845,7 @@ int stage_nodes(Engine& E) {
     A.qready_big = readyB[cur ^ 1];
     AHOP_CUDA_TRY(cudaMemsetAsync(ready[cur ^ 1], 0, ready_bytes, st));
     AHOP_CUDA_TRY(cudaMemsetAsync(readyB[cur ^ 1], 0, ready_bytes, st));
-    AHOP_CUDA_TRY(cudaMemsetAsync(A.nnext, 0, 16, st));
+    AHOP_CUDA_TRY(cudaMemsetAsync(A.nnext, 0, 20, st));
     Task* list_s = tasks[cur] + off_s;
     Task* list_b = tasksB[cur] + off_b;
     if (nsmall > 2048) {
@@ -1755,7 +1878,10 @@ int stage_nodes(Engine& E) {
       AHOP_CUDA_TRY(cudaStreamWaitEvent(E.stream2, E.ev_fork, 0));
       if (prof) AHOP_CUDA_TRY(cudaEventRecord(E.wave_ev[2], E.stream2));
       E.launches++;
-      tree_wave_kernel<kNTBig><<<nbig, kNTBig, wave_dyn_smem(kNTBig), E.stream2>>>(A, list_b);
+      // union-find parents sized to the launch's largest task: the rest of the
+      // shared-memory carveout stays L1
+      A.par_cap_big = std::min(par_cap(kNTBig), std::max(max_big, 1));
+      tree_wave_kernel<kNTBig><<<nbig, kNTBig, wave_dyn_smem(kNTBig, A.par_cap_big), E.stream2>>>(A, list_b);
       AHOP_CUDA_TRY(cudaGetLastError());
       if (prof) AHOP_CUDA_TRY(cudaEventRecord(E.wave_ev[3], E.stream2));
       AHOP_CUDA_TRY(cudaEventRecord(E.ev_join, E.stream2));
@@ -1763,12 +1889,12 @@ int stage_nodes(Engine& E) {
     if (prof) AHOP_CUDA_TRY(cudaEventRecord(E.wave_ev[0], st));
     if (nsmall > 0) {
       E.launches++;
-      tree_wave_kernel<kNT><<<nsmall, kNT, wave_dyn_smem(kNT), st>>>(A, list_s);
+      tree_wave_kernel<kNT><<<nsmall, kNT, wave_dyn_smem(kNT, par_cap(kNT)), st>>>(A, list_s);
       AHOP_CUDA_TRY(cudaGetLastError());
     }
     if (prof) AHOP_CUDA_TRY(cudaEventRecord(E.wave_ev[1], st));
     if (nbig > 0) AHOP_CUDA_TRY(cudaStreamWaitEvent(st, E.ev_join, 0));
-    AHOP_CUDA_TRY(cudaMemcpyAsync(h, flags, 28, cudaMemcpyDeviceToHost, st));
+    AHOP_CUDA_TRY(cudaMemcpyAsync(h, flags, 32, cudaMemcpyDeviceToHost, st));
     AHOP_CUDA_TRY(cudaStreamSynchronize(st));
     if (prof) {
       float ms_s = 0.f, ms_b = 0.f;
@@ -1788,6 +1914,7 @@ int stage_nodes(Engine& E) {
     nbig = h[4] - h[6];
     off_s = h[5];
     off_b = h[6];
+    max_big = h[7];
     cur ^= 1;
     E.waves = wave + 1;
   }

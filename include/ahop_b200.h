@@ -152,12 +152,15 @@ int ahop_debug_compute_stages(const double* pos_in, const double* mass_in, int64
  * kernel, which runs only while the task profile is on. */
 int ahop_debug_tree_stats(int64_t* out, int32_t n);
 /* Per-task structure-tree profile (off by default; turning it on costs one
- * store per task).  Row k (16 int64) describes the task of node k: groups in
- * its range, levels, structural passes, cycles in structural passes, in
- * approximate statistics, in exact sums, in the whole task, the largest
- * component count at one level, then the cycles of the eight phases of the
- * structural passes (reset, union, find, offsets, reorder, copy, starts,
- * component index).  Rows of nodes without a task stay 0. */
+ * store per task).  Row k (32 int64) describes the task of node k (node ids
+ * as created, before the final renumbering): [0] groups in its range, [1]
+ * levels, [2] structural passes, cycles [3] in structural passes, [4] in
+ * approximate statistics, [5] in exact sums, [6] in the whole task, [7] the
+ * largest component count at one level, then phase cycles: [8..15] structural
+ * (reset, union of long saddle rows, find, offsets, reorder, copy, starts,
+ * component index), [16..19] statistics (anchors, group terms, small
+ * components, large components), [20] structural union of short rows, [24]
+ * the mother's node id as created.  Rows of nodes without a task stay 0. */
 int ahop_debug_set_task_profile(int32_t on);
 /* Structure-tree waves of the last compute while the task profile is on (at
  * most 64): per wave the number of small tasks, their launch's milliseconds,
