@@ -1075,16 +1075,20 @@ __global__ void task_gather_kernel(const Task* __restrict__ in, const int32_t* _
   if (i < n) out[i] = in[idx[i]];
 }
 
-// Dynamic shared memory of a task block: exact-sum staging (kTermWarps warps;
-// also the block fold of approx_stats), reorder keys, warp-linked row
-// positions (also approx_stats' list of large components), union-find
-// parents of tasks of at most pcap groups.  What the block does not take
-// stays L1, which the per-group loads of every level hit.
+// Dynamic shared memory of a task block: reorder keys, warp-linked row
+// positions (also approx_stats' list of large components) and the union-find
+// parents of tasks of at most pcap groups, all scratch of a structural pass;
+// the exact-sum staging (kTermWarps warps; also approx_stats' block fold),
+// used only after the pass, lies over the same bytes.  What the block does
+// not take stays L1, which the per-group loads of every level hit.
 __host__ __device__ constexpr size_t wave_dyn_smem(int nt, int pcap) {
-  return (size_t)kTermWarps * 32 * 6 * 8 + (size_t)nt * ipt_for(nt) * 4 + (size_t)kMaxBigRows * 4 +
-         (size_t)pcap * 4;
+  const size_t pass = (size_t)nt * ipt_for(nt) * 4 + (size_t)kMaxBigRows * 4 + (size_t)pcap * 4;
+  const size_t terms = (size_t)kTermWarps * 32 * 6 * 8;
+  return pass > terms ? pass : terms;
 }
-static_assert(kTermWarps * 32 * 6 * 8 >= 32 * (int)sizeof(CompSums) && kMaxBigRows >= kMaxBlockComps,
+// the block fold (over the reorder keys) must end before the large-component list
+static_assert(kNT * kIPT * 4 >= (kNT / 32) * (int)sizeof(CompSums) &&
+              kNTBig * 2 * 4 >= (kNTBig / 32) * (int)sizeof(CompSums) && kMaxBigRows >= kMaxBlockComps,
               "approx_stats scratch must fit the regions it borrows");
 
 template <int NT>
@@ -1096,8 +1100,8 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
   __shared__ typename ScanT::TempStorage scan_tmp;
   __shared__ typename MaxScanT::TempStorage maxscan_tmp;
   extern __shared__ __align__(16) unsigned char wave_dyn[];
-  double* s_terms = reinterpret_cast<double*>(wave_dyn);
-  int32_t* s_keys = reinterpret_cast<int32_t*>(wave_dyn + (size_t)kTermWarps * 32 * 6 * 8);
+  double* s_terms = reinterpret_cast<double*>(wave_dyn);  // over s_keys, s_big, s_par
+  int32_t* s_keys = reinterpret_cast<int32_t*>(wave_dyn);
   int32_t* s_big = s_keys + NT * ipt_for(NT);
   int32_t* s_par = s_big + kMaxBigRows;
   __shared__ SharedTask T;
