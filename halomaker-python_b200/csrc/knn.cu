@@ -771,20 +771,24 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
             }
           }
           // visit test in FP32 against the bound rounded up: a superset of the
-          // leaves whose lower bound is below the bound, so nothing is lost
+          // leaves whose lower bound is below the bound, so nothing is lost.
+          // The chunk's leaves are visited nearest-first by that lower bound
+          // (its bits with the lane in the 5 lowest: non-negative floats order
+          // like their bits, and clearing bits rounds the bound down), so the
+          // list tightens sooner and the visits stop at the first leaf at or
+          // beyond the bound.
           float r2f = __double2float_ru(L.r2);
-          unsigned mask = __ballot_sync(0xffffffffu, bd < r2f);
-          while (mask) {
-            const int src = __ffs(mask) - 1;
-            mask &= mask - 1;
+          unsigned key = (bd < r2f) ? ((__float_as_uint(bd) & ~31u) | (unsigned)lane) : 0xffffffffu;
+          for (;;) {
+            const unsigned m = __reduce_min_sync(0xffffffffu, key);
+            if (!(__uint_as_float(m & ~31u) < r2f)) break;  // none left, or all at or beyond the bound
+            const int src = (int)(m & 31u);
+            if (lane == src) key = 0xffffffffu;
             if (kProf) ++nbits;
-            const float sbd = __shfl_sync(0xffffffffu, bd, src);
             const int32_t slw = __shfl_sync(0xffffffffu, leafw, src);
-            if (sbd < r2f) {
-              if (kProf && lane == ((c0 + src) >> 5)) visbits |= 1u << ((c0 + src) & 31);
-              leaf_insert<C>(A, L, slw & ~(1 << 30), s, qx, qy, qz, lane, nvis, nins, (slw >> 30) & 1);
-              r2f = __double2float_ru(L.r2);
-            }
+            if (kProf && lane == ((c0 + src) >> 5)) visbits |= 1u << ((c0 + src) & 31);
+            leaf_insert<C>(A, L, slw & ~(1 << 30), s, qx, qy, qz, lane, nvis, nins, (slw >> 30) & 1);
+            r2f = __double2float_ru(L.r2);
           }
         }
       }
