@@ -277,6 +277,10 @@ struct SharedTask {
   unsigned long long best;
   Task cont;
   int32_t has_cont, groups0;
+  // groups dropped from the range as below the member threshold for good:
+  // how many, and the bits of their largest peak density (0: none)
+  int32_t npruned;
+  unsigned long long pruned_max_bits;
 };
 
 template <int NT, class SortT, class ScanT, class MaxScanT>
@@ -1091,6 +1095,65 @@ static_assert(kNT * kIPT * 4 >= (kNT / 32) * (int)sizeof(CompSums) &&
               kNTBig * 2 * 4 >= (kNTBig / 32) * (int)sizeof(CompSums) && kMaxBigRows >= kMaxBlockComps,
               "approx_stats scratch must fit the regions it borrows");
 
+// Components whose member count above the threshold is below nmembthresh
+// fail the mass test (f90:1459) at this level and at every later one: the
+// count only falls as the threshold rises, and a later sub-component holds
+// fewer members still.  They make no node, and they never rejoin another
+// component (components only split as the threshold rises), so a task that
+// continues drops them from its range at a level where a structural pass
+// follows anyway.  The kept groups keep their relative order, hence the
+// reference's colour order; the dropped groups keep the task's node as their
+// deepest node, which is what the reference gives them.  Their largest peak
+// density is kept for the continuation test, which counts every surviving
+// group.  Worth it only when a good share of the range goes.
+constexpr int32_t kMinPrune = 64;
+
+template <int NT, class ScanT>
+__device__ void prune_low_components(const TreeArgs& A, SharedTask& T, typename ScanT::TempStorage& scan_tmp) {
+  const int tid = threadIdx.x;
+  const int32_t a = T.a, b = T.b, ncomp = T.ncomp;
+  const double thr = (double)A.nmembthresh;
+  // new start of every kept component (cnt is free until the next pass)
+  int32_t carry = 0;
+  for (int32_t k0 = 0; k0 < ncomp; k0 += NT) {
+    const int32_t k = k0 + tid;
+    int32_t v = 0;
+    if (k < ncomp && !(A.cs[12 * (size_t)(a + k)] < thr)) v = comp_end(A, T, k) - A.cstart[a + k];
+    int32_t ex, tot;
+    ScanT(scan_tmp).ExclusiveSum(v, ex, tot);
+    __syncthreads();
+    if (k < ncomp) A.cnt[a + k] = carry + ex;
+    carry += tot;
+  }
+  const int32_t nkeep = carry, ndrop = b - a - carry;  // the same in every thread
+  if (ndrop < kMinPrune || ndrop < (b - a) / 16) return;
+  __syncthreads();
+  unsigned long long mx = 0ull;  // peak densities are positive: their bits order like them
+  for (int32_t i = a + tid; i < b; i += NT) {
+    const int32_t k = A.compidx[i];
+    const int32_t g = A.GL[i];
+    if (A.cs[12 * (size_t)(a + k)] < thr)
+      mx = max(mx, (unsigned long long)__double_as_longlong(A.densg[g]));
+    else
+      A.GL2[a + A.cnt[a + k] + (i - A.cstart[a + k])] = g;
+  }
+  if (mx) atomicMax(&T.pruned_max_bits, mx);
+  __syncthreads();
+  for (int32_t i = a + tid; i < a + nkeep; i += NT) {
+    const int32_t g = A.GL2[i];
+    A.GL[i] = g;
+    A.pos_of[g] = i;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    T.b = a + nkeep;
+    T.nsurv = nkeep;
+    T.npruned += ndrop;
+    T.next_event = -DBL_MAX;  // components, starts and indices are rebuilt by the pass
+  }
+  __syncthreads();
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeArgs A, const Task* __restrict__ tasks) {
   using SortT = cub::BlockRadixSort<int32_t, NT, ipt_for(NT), int32_t>;
@@ -1128,6 +1191,8 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
     T.done = 0;
     T.iters = 0;
     T.has_cont = 0;
+    T.npruned = 0;
+    T.pruned_max_bits = 0ull;
   }
   __syncthreads();
   while (true) {
@@ -1178,7 +1243,8 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
       if (tid == 0) {
         const double mc = A.cs[12 * (size_t)(T.a + T.kk) + 1];
         const double rnew = xmul(T.rhot, xadd(1.0, xdiv(A.fudge, xsqrt(mc))));
-        if (T.nsurv > 1) {
+        // more than one surviving group (f90:1595), those pruned from the range included
+        if (T.nsurv > 1 || __longlong_as_double((long long)T.pruned_max_bits) > T.rhot) {
           T.rhot = rnew;
           T.done = 0;
         } else {
@@ -1190,6 +1256,8 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
       }
       __syncthreads();
       if (T.done) break;
+      // the next level restructures anyway: drop what can never be a node
+      if (T.rhot >= T.next_event) prune_low_components<NT, ScanT>(A, T, scan_tmp);
       continue;
     }
     // ---- branching (f90:1484-1571): one node per significant component in
@@ -1295,6 +1363,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
       r[7] = s_clk[5];        // largest component count at one level
       for (int k = 0; k < kProfPhases; ++k) r[8 + k] = s_ph[k];  // phases
       r[24] = A.node[T.inode].mother;  // creation-time node id of the mother
+      r[25] = T.npruned;               // groups dropped below the member threshold
     }
   }
   // no child to continue: take a task that another block queued for the next

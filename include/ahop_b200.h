@@ -160,7 +160,9 @@ int ahop_debug_tree_stats(int64_t* out, int32_t n);
  * (reset, union of long saddle rows, find, offsets, reorder, copy, starts,
  * component index), [16..19] statistics (anchors, group terms, small
  * components, large components), [20] structural union of short rows, [24]
- * the mother's node id as created.  Rows of nodes without a task stay 0. */
+ * the mother's node id as created, [25] groups the task dropped from its
+ * range as below the member threshold for good.  Rows of nodes without a
+ * task stay 0. */
 int ahop_debug_set_task_profile(int32_t on);
 /* Structure-tree waves of the last compute while the task profile is on (at
  * most 64): per wave the number of small tasks, their launch's milliseconds,
