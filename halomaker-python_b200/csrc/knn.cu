@@ -366,21 +366,26 @@ __device__ __forceinline__ unsigned long long seed_key(const KnnArgs& A, int64_t
   return (unsigned long long)__double_as_longlong(d);
 }
 
-// Sort keys carry the element number in their 6 lowest bits (the squared
-// distance's last mantissa bits are dropped), so one 64-bit value moves
-// through the network.  The order is exact between keys whose upper 58 bits
-// differ; keys sharing them (distances within 2^-46 relative, or exact ties)
-// sit next to each other after the sort, and then the function returns false
-// and the caller sorts again exactly with the particle indices (seed_sort).
+// The same sort on 32-bit keys: the squared distance rounded up to float
+// (rounding is monotone and non-negative floats order like their bits), its
+// 6 lowest bits replaced by the element number, so one 32-bit value moves
+// through the network.  The order is exact between keys whose upper 26 bits
+// differ; the list needs the first 33 elements in exact (distance, index)
+// order, so when two neighbours among them share those bits (distances
+// within about 2^-17 relative, or exact ties) the function returns false and
+// the caller sorts again exactly with the particle indices (seed_sort).
 // Empty candidates (+inf) may share them: they are never list entries.
 template <int C>
 __device__ __forceinline__ bool seed_sort_keys(const KnnArgs& A, int64_t jl, int64_t jn, int64_t self, double qx,
                                                double qy, double qz, int lane, unsigned char* list, double& kth,
                                                bool wrap) {
   const int nvv = C ? C : A.nv;
-  const unsigned long long kInfHi = 0x7FF0000000000000ull >> 6;
-  unsigned long long k0 = (seed_key(A, jl, jn, self, qx, qy, qz, lane, wrap) & ~63ull) | (unsigned)lane;
-  unsigned long long k1 = (seed_key(A, jl, jn, self, qx, qy, qz, 32 + lane, wrap) & ~63ull) | (unsigned)(32 + lane);
+  const unsigned kInfHi = 0x7F800000u >> 6;
+  auto key32 = [&](int e) {
+    const double d = __longlong_as_double((long long)seed_key(A, jl, jn, self, qx, qy, qz, e, wrap));
+    return (__float_as_uint(__double2float_ru(d)) & ~63u) | (unsigned)e;
+  };
+  unsigned k0 = key32(lane), k1 = key32(32 + lane);
 #pragma unroll
   for (int size = 2; size <= 64; size <<= 1) {
     const bool asc = ((2 * lane) & size) == 0;
@@ -388,32 +393,32 @@ __device__ __forceinline__ bool seed_sort_keys(const KnnArgs& A, int64_t jl, int
     for (int stride = size >> 1; stride >= 1; stride >>= 1) {
       if (stride == 1) {
         if (asc ? (k1 < k0) : (k0 < k1)) {
-          const unsigned long long tk = k0; k0 = k1; k1 = tk;
+          const unsigned tk = k0; k0 = k1; k1 = tk;
         }
       } else {
         const int ls = stride >> 1;
-        const unsigned long long pk0 = __shfl_xor_sync(0xffffffffu, k0, ls), pk1 = __shfl_xor_sync(0xffffffffu, k1, ls);
+        const unsigned pk0 = __shfl_xor_sync(0xffffffffu, k0, ls), pk1 = __shfl_xor_sync(0xffffffffu, k1, ls);
         const bool kmin = (((lane & ls) == 0) == asc);
         if (kmin ? (pk0 < k0) : (k0 < pk0)) k0 = pk0;
         if (kmin ? (pk1 < k1) : (k1 < pk1)) k1 = pk1;
       }
     }
   }
-  // sorted element 2*lane + slot: look for finite neighbours sharing the upper bits
-  const unsigned long long h0 = k0 >> 6, h1 = k1 >> 6;
-  const unsigned long long nx = __shfl_down_sync(0xffffffffu, h0, 1);
-  const bool tie = (h0 == h1 && h0 != kInfHi) || (lane < 31 && h1 == nx && h1 != kInfHi);
+  // sorted element 2*lane + slot: neighbours (e, e + 1), e < 32, sharing the upper bits
+  const unsigned h0 = k0 >> 6, h1 = k1 >> 6;
+  const unsigned nx = __shfl_down_sync(0xffffffffu, h0, 1);
+  const bool tie = lane < 16 && ((h0 == h1 && h0 != kInfHi) || (h1 == nx && h1 != kInfHi));
   if (__any_sync(0xffffffffu, tie)) return false;
   if (lane < 16) {
     list[2 * lane] = (unsigned char)(k0 & 63u);
     list[2 * lane + 1] = (unsigned char)(k1 & 63u);
   }
-  // the nv-th distance, rounded up in its dropped bits (a bound for the
-  // candidate search), +inf when fewer than nv candidates exist
+  // the nv-th distance, rounded up (a bound for the candidate search), +inf
+  // when fewer than nv candidates exist
   const int e = nvv - 1;
-  const unsigned long long a = __shfl_sync(0xffffffffu, k0, e >> 1), b = __shfl_sync(0xffffffffu, k1, e >> 1);
-  const unsigned long long kk = (e & 1) ? b : a;
-  kth = (kk >> 6) == kInfHi ? CUDART_INF : __longlong_as_double((long long)(kk | 63ull));
+  const unsigned a = __shfl_sync(0xffffffffu, k0, e >> 1), b = __shfl_sync(0xffffffffu, k1, e >> 1);
+  const unsigned kk = (e & 1) ? b : a;
+  kth = (kk >> 6) == kInfHi ? CUDART_INF : (double)__uint_as_float(kk | 63u);
   return true;
 }
 
@@ -496,9 +501,11 @@ __device__ void query_dfs(const KnnArgs& A, WarpList& L, int64_t s, double qx, d
 }
 
 // SPH density (f90:2816-2838) in the exact evaluation order, and the stored
-// neighbour slots.
+// neighbour slots.  The nv - 1 terms are summed in list order by lane 0 from
+// the warp's scratch st (32 doubles of shared memory), not with a shuffle per
+// term.
 template <int C>
-__device__ __forceinline__ void finish_query(const KnnArgs& A, const WarpList& L, int64_t s, int lane) {
+__device__ __forceinline__ void finish_query(const KnnArgs& A, const WarpList& L, int64_t s, int lane, double* st) {
   const int nv = C ? C : A.nv;
   const double dlast = __shfl_sync(0xffffffffu, L.ld, nv - 1);
   const double r = xmul(xsqrt(dlast), 0.5);
@@ -506,13 +513,16 @@ __device__ __forceinline__ void finish_query(const KnnArgs& A, const WarpList& L
   const double unsr = xdiv(1.0, r);
   double term = 0.0;
   if (lane < nv - 1) term = xmul(A.m[L.ls], spline(xmul(xsqrt(L.ld), unsr)));
-  double contrib = 0.0;
-  for (int i = 0; i < nv - 1; ++i) contrib = xadd(contrib, __shfl_sync(0xffffffffu, term, i));
+  st[lane] = term;
+  __syncwarp();
   if (lane == 0) {
+    double contrib = 0.0;
+    for (int i = 0; i < nv - 1; ++i) contrib = xadd(contrib, st[i]);
     const double pi_f = (double)3.141592654f;  // f90:58 single-precision literal
     A.dens[s] = xdiv(xmul(A.xyzlong, xadd(contrib, A.m[s])), xmul(pi_f, r3));
   }
   if (lane < A.nstore) A.nei[s * A.nstore + lane] = L.ls;
+  __syncwarp();  // st is the fallback search stack of the next query
 }
 
 // Boxes in FP32 for the candidate tests: centre rounded to
@@ -598,7 +608,7 @@ static_assert((kMaxCand & (kMaxCand - 1)) == 0 && (kMaxCandSpill & (kMaxCandSpil
 // production instances, so they cost nothing there).
 template <int C, bool kProf>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArgs A) {
-  __shared__ int32_t s_node[kWarpsPerBlock][kStack];
+  __shared__ __align__(16) int32_t s_node[kWarpsPerBlock][kStack];
   __shared__ double s_bd[kWarpsPerBlock][kStack];
   __shared__ int32_t s_cand[kWarpsPerBlock][kMaxCand];
   __shared__ unsigned char s_list[kWarpsPerBlock][kLeaf][32];  // each query's seed order
@@ -620,11 +630,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
     // ---- A: per-query bound from the two leaves
     double Rq = 0.0;
     bool ok = true;
+    unsigned wrapmask = 0u;  // bit q: query q needs the periodic fold for its two seed leaves
     for (int q = 0; q < nq; ++q) {
       const int64_t s = s0 + q;
       const double qx = A.x[s], qy = A.y[s], qz = A.z[s];
       const bool wrap = !(near_box(A.box32 + 2 * jl, qx, qy, qz, A.Lx, A.Ly, A.Lz) &&
                           near_box(A.box32 + 2 * jn, qx, qy, qz, A.Lx, A.Ly, A.Lz));
+      if (wrap) wrapmask |= 1u << q;
       double kth;
       if (!seed_sort_keys<C>(A, jl, jn, s, qx, qy, qz, lane, s_list[wib][q], kth, wrap))
         kth = seed_sort<C>(A, jl, jn, s, qx, qy, qz, lane, s_list[wib][q], wrap);
@@ -744,8 +756,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
         for (int o = 16; o > 0; o >>= 1) d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
         L.cap = d;
       }
-      const bool swrap = !(near_box(A.box32 + 2 * jl, qx, qy, qz, A.Lx, A.Ly, A.Lz) &&
-                           near_box(A.box32 + 2 * jn, qx, qy, qz, A.Lx, A.Ly, A.Lz));
+      const bool swrap = (wrapmask >> q) & 1u;
       seed_list<C>(A, L, jl, jn, s, qx, qy, qz, lane, s_list[wib][q], nvis, swrap);
       const long long tq1 = kProf ? clock64() : 0;
       if (overflow) {
@@ -806,7 +817,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
       }
       const long long tq3 = kProf ? clock64() : 0;
       prev_ls = L.ls;
-      finish_query<C>(A, L, s, lane);
+      // the traversal stack is free once the query's search is done
+      finish_query<C>(A, L, s, lane, reinterpret_cast<double*>(s_node[wib]));
       __syncwarp();
       if (kProf) c_fin += clock64() - tq3;
     }
