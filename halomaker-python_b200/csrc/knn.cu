@@ -568,6 +568,20 @@ __device__ __forceinline__ bool near_box(const float4* __restrict__ b, double qx
          fabs((double)c.z - qz) + (double)w.z <= Lz * (0.5 - 0x1p-30);
 }
 
+// near_box in FP32 for a query (qx, qy, qz) rounded to float (|q - qf| <=
+// 2^-25 L for |q| <= L/2): |c - qf| rounded up, plus w rounded up, against
+// lim = L (1/2 - 2^-22) rounded down, a margin far above those roundings.
+// False more often than near_box only within that margin (the periodic path
+// is then taken, which is exact too).
+__device__ __forceinline__ bool near_box32(const float4* __restrict__ b, float qx, float qy, float qz, float limx,
+                                           float limy, float limz) {
+  const float4 c = b[0], w = b[1];
+  const float ux = __fadd_ru(__fsub_ru(fmaxf(c.x, qx), fminf(c.x, qx)), w.x);
+  const float uy = __fadd_ru(__fsub_ru(fmaxf(c.y, qy), fminf(c.y, qy)), w.y);
+  const float uz = __fadd_ru(__fsub_ru(fmaxf(c.z, qz), fminf(c.z, qz)), w.z);
+  return ux <= limx && uy <= limy && uz <= limz;
+}
+
 // Periodic squared distance between two padded boxes (centre, half width).
 // Lower bound of the squared periodic distance between two widened FP32 boxes.
 __device__ __forceinline__ float boxbox_dist2_lb(const float4* __restrict__ a, const float4* __restrict__ b,
@@ -618,6 +632,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
   const int64_t nleaf = A.lev_cnt[0];
   const int top = A.nlev - 1;
   const float Lxf = (float)A.Lx, Lyf = (float)A.Ly, Lzf = (float)A.Lz;
+  const float hlx = __double2float_rd(A.Lx * (0.5 - 0x1p-22)), hly = __double2float_rd(A.Ly * (0.5 - 0x1p-22)),
+              hlz = __double2float_rd(A.Lz * (0.5 - 0x1p-22));
   // candidate sort keys; s_bd is only used by the per-query fallback, which
   // runs exactly when there is no candidate list
   unsigned* s_key = reinterpret_cast<unsigned*>(s_bd[wib]);
@@ -750,11 +766,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
         const int nvv = C ? C : A.nv;
         int32_t ps = prev_ls;
         if (ps == (int32_t)s) ps = (int32_t)s - 1;
-        double d = 0.0;
-        if (lane < nvv) d = ps >= 0 ? pdist2(qx, qy, qz, A.x[ps], A.y[ps], A.z[ps], A.Lx, A.Ly, A.Lz) : CUDART_INF;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
-        L.cap = d;
+        // Only an upper bound is needed: the distance without the periodic fold
+        // is at least the folded one (equal bits within half a period), and
+        // the warp maximum is taken over the high words rounded up (one
+        // reduction; non-negative doubles order like their bits).
+        unsigned hk = 0u;
+        if (lane < nvv)
+          hk = ps >= 0 ? (unsigned)(__double_as_longlong(dist2_near(qx, qy, qz, A.x[ps], A.y[ps], A.z[ps])) >> 32) + 1u
+                       : 0x7FF00000u;  // +inf
+        hk = __reduce_max_sync(0xffffffffu, hk);
+        L.cap = __longlong_as_double((long long)((unsigned long long)hk << 32));
       }
       const bool swrap = (wrapmask >> q) & 1u;
       seed_list<C>(A, L, jl, jn, s, qx, qy, qz, lane, s_list[wib][q], nvis, swrap);
@@ -778,7 +799,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
             leafw = leaf;
             if (leaf != jl && leaf != jn) {
               bd = box_dist2_lb(A.box32 + 2 * (int64_t)leaf, qxf, qyf, qzf, Lxf, Lyf, Lzf);
-              if (!near_box(A.box32 + 2 * (int64_t)leaf, qx, qy, qz, A.Lx, A.Ly, A.Lz)) leafw |= 1 << 30;
+              if (!near_box32(A.box32 + 2 * (int64_t)leaf, qxf, qyf, qzf, hlx, hly, hlz)) leafw |= 1 << 30;
             }
           }
           // visit test in FP32 against the bound rounded up: a superset of the
