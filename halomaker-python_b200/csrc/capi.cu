@@ -389,6 +389,14 @@ int ahop_debug_task_profile(int64_t* out, int32_t maxrows) {
   return AHOP_OK;
 }
 
+int ahop_debug_set_tree_cluster(int32_t ctas) {
+  if (ctas != 1 && ctas != 4) { set_error("tree cluster size must be 1 or 4"); return AHOP_EINVAL; }
+  engine().tree_cluster_req = ctas;
+  return AHOP_OK;
+}
+
+int ahop_debug_get_tree_cluster(void) { return engine().tree_cluster; }
+
 int ahop_debug_set_big_task(int32_t groups) {
   if (groups < 1) { set_error("big-task threshold must be positive"); return AHOP_EINVAL; }
   engine().big_task = groups;

@@ -84,6 +84,9 @@ struct Engine {
   cudaStream_t stream = nullptr;  // stream of the current call
   cudaStream_t stream2 = nullptr; // structure tree: large tasks run here beside the small ones
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  int tree_cluster = 1;           // CTAs per wide structure-tree task in use (1: no clusters)
+  int tree_cluster_req = 4;       // CTAs asked for (debug API: 4 or 1)
+  int tree_cluster_for = 0;       // the request tree_cluster was chosen for (0: none yet)
   cudaStream_t stream_copy = nullptr;   // host path: density copy-out during the later stages
   cudaEvent_t ev_dens = nullptr, ev_copied = nullptr;
   cudaEvent_t ev_mass = nullptr;        // host path: masses uploaded on the copy stream

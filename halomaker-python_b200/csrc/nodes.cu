@@ -36,6 +36,7 @@
 // final node of a particle is therefore the deepest node containing its group
 // whose rho_saddle is below the particle density; it is computed per particle
 // after the waves.
+#include <cooperative_groups.h>
 #include <cub/cub.cuh>
 #include <cfloat>
 #include <climits>
@@ -58,6 +59,10 @@ constexpr int kBigGroup = 96;   // groups larger than this are summed by a warp
 constexpr int kRowWarp = 8;     // saddle-row prefixes longer than this are linked by a warp
 constexpr int kMaxBigRows = 512;
 constexpr long long kMaxTaskLevels = 4000000LL;  // cap on one task's threshold levels (error, never a hang)
+// A wide task runs on a thread-block cluster of this many CTAs: the leader
+// runs the task, the followers take slices of its position-parallel phases.
+constexpr int kClusterCtas = 4;
+constexpr int32_t kPhUnion = 1, kPhFind = 2, kPhTerms = 3, kPhExit = 4;
 constexpr int kProfPhases = 16;  // phase cycle counters per task (structural 0..7, 12; statistics 8..11)
 
 struct Task {
@@ -281,7 +286,102 @@ struct SharedTask {
   // how many, and the bits of their largest peak density (0: none)
   int32_t npruned;
   unsigned long long pruned_max_bits;
+  // cluster phases of a wide task: the phase the leader hands its followers,
+  // whether the union-find array is the leader's shared memory, and each
+  // follower's smallest next event of a union phase
+  int32_t phase, plocal;
+  double ev_part[kClusterCtas];
 };
+
+namespace cg = cooperative_groups;
+
+// CTAs of the launch's cluster (1 outside a cluster launch)
+__device__ __forceinline__ int cluster_ctas() { return (int)cg::this_cluster().num_blocks(); }
+
+// The leader hands phase `code` to its followers: a cluster-wide barrier that
+// every thread of every CTA of the cluster takes; the phase ends with a second
+// one (cg::this_cluster().sync()) once each CTA has done its slice.
+__device__ __forceinline__ void lead_phase(SharedTask& T, int32_t code, bool local) {
+  if (threadIdx.x == 0) { T.phase = code; T.plocal = local ? 1 : 0; }
+  cg::this_cluster().sync();
+}
+
+// ---- position-parallel phases of a structural pass, over the positions
+// [a, b) that fall to cluster-wide thread gt (stride gs): one block runs them
+// with gt = threadIdx.x, gs = NT; a wide task's cluster splits them over its
+// CTAs (see tree_wave_kernel).  par is the union-find array (entries relative
+// to poff), in the leader CTA's shared memory or in global memory.
+//
+// Union over saddle edges above rhot (a prefix of each row, rows sorted by
+// decreasing saddle).  Each undirected edge is linked once, from the row of
+// its smaller group id; rows with more than kRowWarp such edges go to the
+// block's list s_big (count *nbig) for union_long_rows.  The next event is the
+// smallest peak density or saddle still above rhot (the last edge of each
+// prefix): the block's minimum lands in *ev_min.
+template <int NT>
+__device__ void union_short_rows(const TreeArgs& A, int32_t a, int32_t b, int32_t poff, double rhot, int32_t* par,
+                                 int32_t* s_big, int32_t* nbig, double* ev_min, int32_t gt, int32_t gs) {
+  double ev = DBL_MAX;
+  for (int32_t i = a + gt; i < b; i += gs) {
+    const int32_t g = A.GL[i];
+    const double dg = A.densg[g];
+    if (!(dg > rhot)) continue;
+    ev = fmin(ev, dg);
+    const int32_t e0 = A.soff[g - 1];
+    const int32_t c = A.ecur[g];
+    const int32_t ne = edges_above_at(A, g, e0, c, c > 0 ? A.srho[e0 + c - 1] : 0.0, rhot);
+    if (ne == 0) continue;
+    ev = fmin(ev, A.srho[e0 + ne - 1]);
+    if (ne > kRowWarp) {
+      const int32_t slot = atomicAdd(nbig, 1);
+      if (slot < kMaxBigRows) { s_big[slot] = i; continue; }
+    }
+    for (int32_t e = e0; e < e0 + ne; ++e) {
+      const int32_t h = A.sisad[e];
+      const int32_t j = A.pos_of[h];
+      if (j < a || j >= b) { set_err(A, 11, g); continue; }  // f90:1229-1233
+      if (h > g) uf_union(par, i - poff, j - poff);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) ev = fmin(ev, __shfl_xor_sync(0xffffffffu, ev, o));
+  if ((threadIdx.x & 31) == 0 && ev < DBL_MAX) atomic_min_pos(ev_min, ev);
+}
+
+// the block's long rows (s_big), a warp each
+template <int NT>
+__device__ void union_long_rows(const TreeArgs& A, int32_t a, int32_t b, int32_t poff, int32_t* par,
+                                const int32_t* s_big, int32_t nbig) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  nbig = min(nbig, kMaxBigRows);
+  for (int32_t bi = tid >> 5; bi < nbig; bi += NT / 32) {
+    const int32_t i = s_big[bi];
+    const int32_t g = A.GL[i];
+    const int32_t e0 = A.soff[g - 1], e1 = e0 + A.ecur[g];
+    for (int32_t e = e0 + lane; e < e1; e += 32) {
+      const int32_t h = A.sisad[e];
+      const int32_t j = A.pos_of[h];
+      if (j < a || j >= b) { set_err(A, 11, g); continue; }
+      if (h > g) uf_union(par, i - poff, j - poff);
+    }
+  }
+}
+
+// roots of the surviving positions, component sizes by root in cnt; dropped
+// groups get -1
+__device__ __forceinline__ void find_roots(const TreeArgs& A, int32_t a, int32_t b, int32_t poff, double rhot,
+                                           int32_t* par, int32_t gt, int32_t gs) {
+  for (int32_t i = a + gt; i < b; i += gs) {
+    const int32_t g = A.GL[i];
+    if (A.densg[g] > rhot) {
+      const int32_t r = uf_find(par, i - poff);
+      par[i - poff] = r;
+      atomicAdd(&A.cnt[r + poff], 1);
+    } else {
+      par[i - poff] = -1;
+    }
+  }
+}
 
 template <int NT, class SortT, class ScanT, class MaxScanT>
 __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT::TempStorage& sort_tmp,
@@ -309,65 +409,22 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   }
   __syncthreads();
   mark(0);
-  // union over saddle edges above rhot (a prefix of each row, rows sorted by
-  // decreasing saddle).  Each undirected edge is linked once, from the row of
-  // its smaller group id; rows with more than kRowWarp such edges are linked
-  // by a whole warp afterwards.  The next event is the smallest peak density
-  // or saddle still above rhot (the last edge of each prefix).
-  double ev = DBL_MAX;
-  for (int32_t i = a + tid; i < b; i += NT) {
-    const int32_t g = A.GL[i];
-    const double dg = A.densg[g];
-    if (!(dg > rhot)) continue;
-    ev = fmin(ev, dg);
-    const int32_t e0 = A.soff[g - 1];
-    const int32_t c = A.ecur[g];
-    const int32_t ne = edges_above_at(A, g, e0, c, c > 0 ? A.srho[e0 + c - 1] : 0.0, rhot);
-    if (ne == 0) continue;
-    ev = fmin(ev, A.srho[e0 + ne - 1]);
-    if (ne > kRowWarp) {
-      const int32_t slot = atomicAdd(&T.nbig, 1);
-      if (slot < kMaxBigRows) { s_big[slot] = i; continue; }
-    }
-    for (int32_t e = e0; e < e0 + ne; ++e) {
-      const int32_t h = A.sisad[e];
-      const int32_t j = A.pos_of[h];
-      if (j < a || j >= b) { set_err(A, 11, g); continue; }  // f90:1229-1233
-      if (h > g) uf_union(par, i - poff, j - poff);
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) ev = fmin(ev, __shfl_xor_sync(0xffffffffu, ev, o));
-  if ((tid & 31) == 0 && ev < DBL_MAX) atomic_min_pos(&T.next_event, ev);
+  const int K = NT >= 1024 ? cluster_ctas() : 1;
+  if (K > 1) lead_phase(T, kPhUnion, local);
+  union_short_rows<NT>(A, a, b, poff, rhot, par, s_big, &T.nbig, &T.next_event, tid, K * NT);
   __syncthreads();
   mark(12);
-  {
-    const int lane = tid & 31;
-    const int32_t nbig = min(T.nbig, kMaxBigRows);
-    for (int32_t bi = tid >> 5; bi < nbig; bi += NT / 32) {
-      const int32_t i = s_big[bi];
-      const int32_t g = A.GL[i];
-      const int32_t e0 = A.soff[g - 1], e1 = e0 + A.ecur[g];
-      for (int32_t e = e0 + lane; e < e1; e += 32) {
-        const int32_t h = A.sisad[e];
-        const int32_t j = A.pos_of[h];
-        if (j < a || j >= b) { set_err(A, 11, g); continue; }
-        if (h > g) uf_union(par, i - poff, j - poff);
-      }
-    }
+  union_long_rows<NT>(A, a, b, poff, par, s_big, T.nbig);
+  if (K > 1) {
+    cg::this_cluster().sync();  // the followers' unions and next events are in
+    if (tid == 0)
+      for (int r = 1; r < K; ++r) T.next_event = fmin(T.next_event, T.ev_part[r]);
   }
   __syncthreads();
   mark(1);
-  for (int32_t i = a + tid; i < b; i += NT) {
-    int32_t g = A.GL[i];
-    if (A.densg[g] > rhot) {
-      const int32_t r = uf_find(par, i - poff);
-      par[i - poff] = r;
-      atomicAdd(&A.cnt[r + poff], 1);
-    } else {
-      par[i - poff] = -1;
-    }
-  }
+  if (K > 1) lead_phase(T, kPhFind, local);
+  find_roots(A, a, b, poff, rhot, par, tid, K * NT);
+  if (K > 1) cg::this_cluster().sync();
   __syncthreads();
   mark(2);
   // exclusive scan of component sizes over root positions -> component offsets (in cnt)
@@ -736,7 +793,13 @@ __device__ void approx_stats(const TreeArgs& A, SharedTask& T, long long* ph, in
   }
   __syncthreads();
   mark(8);
-  for (int32_t i = a + tid; i < b; i += NT) position_terms(A, i, rhot, A.cs + 12 * (size_t)(a + A.compidx[i]) + 9);
+  {
+    const int K = NT >= 1024 ? cluster_ctas() : 1;
+    if (K > 1) lead_phase(T, kPhTerms, false);
+    for (int32_t i = a + tid; i < b; i += K * NT)
+      position_terms(A, i, rhot, A.cs + 12 * (size_t)(a + A.compidx[i]) + 9);
+    if (K > 1) cg::this_cluster().sync();
+  }
   __syncthreads();
   mark(9);
   for (int32_t k = tid; k < ncomp; k += NT) {
@@ -1154,6 +1217,49 @@ __device__ void prune_low_components(const TreeArgs& A, SharedTask& T, typename 
   __syncthreads();
 }
 
+// A follower CTA of a wide task's cluster: it waits for the leader's phases
+// and runs its slice of each (positions a + rank * NT + tid, stride K * NT),
+// reading the leader's task state and, when the task fits, its union-find
+// array through distributed shared memory.  Each phase is a pair of cluster
+// barriers, the pair the leader takes around its own slice; kPhExit ends the
+// loop, and one last barrier tells the leader that its shared memory is read
+// no more.
+template <int NT>
+__device__ void follow_phases(const TreeArgs& A, SharedTask& T, int32_t* s_big, int32_t* s_par) {
+  cg::cluster_group cl = cg::this_cluster();
+  const int K = (int)cl.num_blocks();
+  const int rank = (int)cl.block_rank();
+  const int tid = threadIdx.x;
+  SharedTask* LT = cl.map_shared_rank(&T, 0);
+  int32_t* lpar = cl.map_shared_rank(s_par, 0);
+  const int32_t gt = rank * NT + tid, gs = K * NT;
+  for (;;) {
+    cl.sync();  // a phase starts
+    const int32_t code = LT->phase;
+    if (code == kPhExit) break;
+    const int32_t a = LT->a, b = LT->b;
+    const double rhot = LT->rhot;
+    const bool local = LT->plocal != 0;
+    int32_t* par = local ? lpar : A.par;
+    const int32_t poff = local ? a : 0;
+    if (code == kPhUnion) {
+      if (tid == 0) { T.nbig = 0; T.next_event = DBL_MAX; }
+      __syncthreads();
+      union_short_rows<NT>(A, a, b, poff, rhot, par, s_big, &T.nbig, &T.next_event, gt, gs);
+      __syncthreads();
+      union_long_rows<NT>(A, a, b, poff, par, s_big, T.nbig);
+      if (tid == 0) LT->ev_part[rank] = T.next_event;
+    } else if (code == kPhFind) {
+      find_roots(A, a, b, poff, rhot, par, gt, gs);
+    } else if (code == kPhTerms) {
+      for (int32_t i = a + gt; i < b; i += gs)
+        position_terms(A, i, rhot, A.cs + 12 * (size_t)(a + A.compidx[i]) + 9);
+    }
+    cl.sync();  // the phase ends
+  }
+  cl.sync();
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeArgs A, const Task* __restrict__ tasks) {
   using SortT = cub::BlockRadixSort<int32_t, NT, ipt_for(NT), int32_t>;
@@ -1171,7 +1277,16 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
   __shared__ long long s_clk[6];  // structural, approx, exact cycles; levels; structural passes; max ncomp
   __shared__ long long s_ph[kProfPhases];  // cycles per phase of the structural passes and statistics
   const int tid = threadIdx.x;
-  if (tid == 0) T.cont = tasks[blockIdx.x];
+  // wide tasks: CTA 0 of each cluster leads, the others serve its phases
+  int K = 1;
+  if (NT >= 1024) {
+    K = cluster_ctas();
+    if (cg::this_cluster().block_rank() != 0) {
+      follow_phases<NT>(A, T, s_big, s_par);
+      return;
+    }
+  }
+  if (tid == 0) T.cont = tasks[blockIdx.x / K];
   // A block runs its task and then, when the task branches, one of the new
   // children itself (the one with the most groups) instead of leaving it to
   // the next wave: the longest chains of the tree no longer wait at every
@@ -1379,6 +1494,11 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
   const bool more = T.has_cont != 0;
   __syncthreads();  // thread 0 rewrites T for the next task
   if (!more) break;
+  }
+  if (K > 1) {  // release the followers, then wait until they no longer read T
+    if (tid == 0) T.phase = kPhExit;
+    cg::this_cluster().sync();
+    cg::this_cluster().sync();
   }
 }
 
@@ -1910,6 +2030,30 @@ int stage_nodes(Engine& E) {
     AHOP_CUDA_TRY(cudaEventCreateWithFlags(&E.ev_fork, cudaEventDisableTiming));
     AHOP_CUDA_TRY(cudaEventCreateWithFlags(&E.ev_join, cudaEventDisableTiming));
   }
+  if (E.tree_cluster_for != E.tree_cluster_req) {
+    // wide tasks on clusters of kClusterCtas CTAs when the device can hold one
+    // at the largest shared-memory size; else one CTA per wide task
+    int ncl = 0;
+    if (E.tree_cluster_req > 1) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(kClusterCtas);
+      cfg.blockDim = dim3(kNTBig);
+      cfg.dynamicSmemBytes = wave_dyn_smem(kNTBig, par_cap(kNTBig));
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = kClusterCtas;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      if (cudaOccupancyMaxActiveClusters(&ncl, tree_wave_kernel<kNTBig>, &cfg) != cudaSuccess) {
+        cudaGetLastError();  // not supported here: no clusters
+        ncl = 0;
+      }
+    }
+    E.tree_cluster = ncl > 0 ? kClusterCtas : 1;
+    E.tree_cluster_for = E.tree_cluster_req;
+  }
   for (int wave = 0; nsmall + nbig > 0; ++wave) {
     if (wave > 100000) { set_error("structure tree: too many waves"); return AHOP_ELIMIT; }
     A.next = tasks[cur ^ 1];
@@ -1954,7 +2098,25 @@ int stage_nodes(Engine& E) {
       // union-find parents sized to the launch's largest task: the rest of the
       // shared-memory carveout stays L1
       A.par_cap_big = std::min(par_cap(kNTBig), std::max(max_big, 1));
-      tree_wave_kernel<kNTBig><<<nbig, kNTBig, wave_dyn_smem(kNTBig, A.par_cap_big), E.stream2>>>(A, list_b);
+      if (E.tree_cluster > 1) {
+        // a cluster per wide task: CTA 0 runs the task, the others take slices
+        // of its position-parallel phases (tree_wave_kernel, follow_phases)
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)nbig * (unsigned)E.tree_cluster);
+        cfg.blockDim = dim3(kNTBig);
+        cfg.dynamicSmemBytes = wave_dyn_smem(kNTBig, A.par_cap_big);
+        cfg.stream = E.stream2;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)E.tree_cluster;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        AHOP_CUDA_TRY(cudaLaunchKernelEx(&cfg, tree_wave_kernel<kNTBig>, A, (const Task*)list_b));
+      } else {
+        tree_wave_kernel<kNTBig><<<nbig, kNTBig, wave_dyn_smem(kNTBig, A.par_cap_big), E.stream2>>>(A, list_b);
+      }
       AHOP_CUDA_TRY(cudaGetLastError());
       if (prof) AHOP_CUDA_TRY(cudaEventRecord(E.wave_ev[3], E.stream2));
       AHOP_CUDA_TRY(cudaEventRecord(E.ev_join, E.stream2));

@@ -171,6 +171,13 @@ int ahop_debug_wave_profile(float* out, int32_t maxwaves);
 /* Tuning: structure-tree tasks of more than `groups` groups run in
  * 1024-thread blocks on a second stream (default 512). */
 int ahop_debug_set_big_task(int32_t groups);
+/* Tuning: CTAs per wide structure-tree task: 4 (default; a thread-block
+ * cluster whose leader runs the task and whose other CTAs take slices of its
+ * union, root-finding and group-term passes, used when the device can hold
+ * such a cluster) or 1 (one CTA per task).  get returns the size the last
+ * compute used (1 before any). */
+int ahop_debug_set_tree_cluster(int32_t ctas);
+int ahop_debug_get_tree_cluster(void);
 int ahop_debug_task_profile(int64_t* out, int32_t maxrows);
 /* Ask compute to keep the first k neighbours per particle (default nhop). */
 int ahop_debug_set_store_neighbours(int32_t k);
