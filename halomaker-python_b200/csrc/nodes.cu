@@ -62,7 +62,7 @@ constexpr long long kMaxTaskLevels = 4000000LL;  // cap on one task's threshold 
 // A wide task runs on a thread-block cluster of this many CTAs: the leader
 // runs the task, the followers take slices of its position-parallel phases.
 constexpr int kClusterCtas = 4;
-constexpr int32_t kPhUnion = 1, kPhFind = 2, kPhTerms = 3, kPhExit = 4;
+constexpr int32_t kPhUnion = 1, kPhFind = 2, kPhTerms = 3, kPhExit = 4, kPhDecide = 5;
 constexpr int kProfPhases = 16;  // phase cycle counters per task (structural 0..7, 12; statistics 8..11)
 
 struct Task {
@@ -291,6 +291,7 @@ struct SharedTask {
   // follower's smallest next event of a union phase
   int32_t phase, plocal;
   double ev_part[kClusterCtas];
+  int32_t fold_n;  // large components whose partial sums a decide phase folds
 };
 
 namespace cg = cooperative_groups;
@@ -717,12 +718,12 @@ struct CompSums {
 };
 
 template <int NT>
-__device__ void component_decide_block(const TreeArgs& A, int32_t c0, int32_t c1, double rhot, double* C,
+__device__ CompSums block_partial_sums(const TreeArgs& A, int32_t c0, int32_t c1, int32_t gt, int32_t gs,
                                        CompSums* red) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   CompSums s{0, 0, kFalse, -1.0, 0, 0, 0, 0, 0, 0};
 #pragma unroll 4
-  for (int32_t i = c0 + tid; i < c1; i += NT) {
+  for (int32_t i = c0 + gt; i < c1; i += gs) {
     const double* G = A.gs + 8 * (size_t)i;
     const int32_t ng = A.gn[i];
     s.nl += ng;
@@ -754,17 +755,67 @@ __device__ void component_decide_block(const TreeArgs& A, int32_t c0, int32_t c1
   fold(s);
   if (lane == 0) red[warp] = s;
   __syncthreads();
+  CompSums w{0, 0, kFalse, -1.0, 0, 0, 0, 0, 0, 0};
   if (warp == 0) {
-    CompSums w = (lane < NT / 32) ? red[lane] : CompSums{0, 0, kFalse, -1.0, 0, 0, 0, 0, 0, 0};
+    if (lane < NT / 32) w = red[lane];
     fold(w);
-    if (lane == 0) decide_from_sums(A, rhot, w.nl, w.nmax, w.dmax, w.S, w.M, w.Sx, w.Sy, w.Sz, w.Q, w.triB, C);
   }
-  __syncthreads();  // red is reused by the next component
+  __syncthreads();  // red is reused by the next call
+  return w;
+}
+
+// two partial sums folded (any order: the test's bounds do not depend on it)
+__device__ __forceinline__ CompSums add_sums(CompSums x, const CompSums& y) {
+  x.nl += y.nl;
+  x.nmax = max(x.nmax, y.nmax);
+  x.dmax = fmax(x.dmax, y.dmax);
+  x.S += y.S;
+  x.M += y.M;
+  x.Sx += y.Sx;
+  x.Sy += y.Sy;
+  x.Sz += y.Sz;
+  x.Q += y.Q;
+  x.triB = tri_or(x.triB, y.triB);
+  return x;
+}
+
+template <int NT>
+__device__ void component_decide_block(const TreeArgs& A, int32_t c0, int32_t c1, double rhot, double* C,
+                                       CompSums* red) {
+  const CompSums w = block_partial_sums<NT>(A, c0, c1, threadIdx.x, NT, red);
+  if (threadIdx.x == 0) decide_from_sums(A, rhot, w.nl, w.nmax, w.dmax, w.S, w.M, w.Sx, w.Sy, w.Sz, w.Q, w.triB, C);
 }
 
 // components of more groups than this are summed by the whole block
 __host__ __device__ constexpr int block_comp_for(int nt) { return nt >= 1024 ? 512 : 1024; }
 constexpr int kMaxBlockComps = 32;
+// large components a cluster's decide phase takes at once (their per-CTA
+// partial sums sit after the block fold's scratch, over the reorder keys)
+constexpr int kFoldBatch = 8;
+static_assert((kNTBig / 32 + kFoldBatch * kClusterCtas) * (int)sizeof(CompSums) <= kNTBig * 2 * 4,
+              "cluster partial sums must fit the reorder keys");
+
+// The decide phase of a wide task's cluster: warp w of CTA rank decides the
+// mid-sized components k = rank * NT / 32 + w (stride K * NT / 32); then for
+// each of the nbc large components listed in bc the CTA's partial sums over
+// its slice of rows go to parts[j * kClusterCtas + rank] (the leader's shared
+// memory), which the leader folds and decides.
+template <int NT>
+__device__ void decide_slice(const TreeArgs& A, int32_t a, int32_t b, int32_t ncomp, double rhot, int rank, int K,
+                             const int32_t* bc, int32_t nbc, CompSums* red, CompSums* parts) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int32_t k = rank * (NT / 32) + warp; k < ncomp; k += K * (NT / 32)) {
+    const int32_t c0 = A.cstart[a + k], c1 = k + 1 < ncomp ? A.cstart[a + k + 1] : b;
+    if (c1 - c0 > kSmallComp && c1 - c0 <= block_comp_for(NT))
+      component_decide(A, c0, c1, rhot, A.cs + 12 * (size_t)(a + k), lane);
+  }
+  for (int32_t j = 0; j < nbc; ++j) {
+    const int32_t k = bc[j];
+    const int32_t c0 = A.cstart[a + k], c1 = k + 1 < ncomp ? A.cstart[a + k + 1] : b;
+    const CompSums p = block_partial_sums<NT>(A, c0, c1, rank * NT + tid, K * NT, red);
+    if (tid == 0) parts[j * kClusterCtas + rank] = p;
+  }
+}
 
 // Approximate statistics of every component of the task: anchors, then the
 // groups' terms position-parallel over the whole block, then a thread per
@@ -816,6 +867,24 @@ __device__ void approx_stats(const TreeArgs& A, SharedTask& T, long long* ph, in
   // more large components than the list holds: warps take all of them
   const int32_t nbc = s_nbc;
   const bool by_block = nbc <= kMaxBlockComps;
+  const int K = NT >= 1024 ? cluster_ctas() : 1;
+  if (K > 1 && by_block && nbc <= kFoldBatch) {
+    CompSums* s_parts = s_red + NT / 32;
+    if (tid == 0) T.fold_n = nbc;
+    lead_phase(T, kPhDecide, false);
+    decide_slice<NT>(A, a, b, ncomp, rhot, 0, K, s_bc, nbc, s_red, s_parts);
+    cg::this_cluster().sync();  // every CTA's decisions and partial sums are in
+    if (tid == 0)
+      for (int32_t j = 0; j < nbc; ++j) {
+        CompSums w = s_parts[j * kClusterCtas];
+        for (int r = 1; r < K; ++r) w = add_sums(w, s_parts[j * kClusterCtas + r]);
+        decide_from_sums(A, rhot, w.nl, w.nmax, w.dmax, w.S, w.M, w.Sx, w.Sy, w.Sz, w.Q, w.triB,
+                         A.cs + 12 * (size_t)(a + s_bc[j]));
+      }
+    __syncthreads();
+    mark(11);
+    return;
+  }
   for (int32_t k = warp; k < ncomp; k += NT / 32) {
     const int32_t c0 = A.cstart[a + k], c1 = comp_end(A, T, k);
     if (c1 - c0 > kSmallComp && !(by_block && c1 - c0 > block_comp_for(NT)))
@@ -1225,7 +1294,7 @@ __device__ void prune_low_components(const TreeArgs& A, SharedTask& T, typename 
 // loop, and one last barrier tells the leader that its shared memory is read
 // no more.
 template <int NT>
-__device__ void follow_phases(const TreeArgs& A, SharedTask& T, int32_t* s_big, int32_t* s_par) {
+__device__ void follow_phases(const TreeArgs& A, SharedTask& T, int32_t* s_big, int32_t* s_par, CompSums* s_red) {
   cg::cluster_group cl = cg::this_cluster();
   const int K = (int)cl.num_blocks();
   const int rank = (int)cl.block_rank();
@@ -1254,6 +1323,9 @@ __device__ void follow_phases(const TreeArgs& A, SharedTask& T, int32_t* s_big, 
     } else if (code == kPhTerms) {
       for (int32_t i = a + gt; i < b; i += gs)
         position_terms(A, i, rhot, A.cs + 12 * (size_t)(a + A.compidx[i]) + 9);
+    } else if (code == kPhDecide) {
+      decide_slice<NT>(A, a, b, LT->ncomp, rhot, rank, K, cl.map_shared_rank(s_big, 0), LT->fold_n, s_red,
+                       cl.map_shared_rank(s_red + NT / 32, 0));
     }
     cl.sync();  // the phase ends
   }
@@ -1282,7 +1354,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
   if (NT >= 1024) {
     K = cluster_ctas();
     if (cg::this_cluster().block_rank() != 0) {
-      follow_phases<NT>(A, T, s_big, s_par);
+      follow_phases<NT>(A, T, s_big, s_par, reinterpret_cast<CompSums*>(s_terms));
       return;
     }
   }
