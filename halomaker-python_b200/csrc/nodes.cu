@@ -62,7 +62,8 @@ constexpr long long kMaxTaskLevels = 4000000LL;  // cap on one task's threshold 
 // A wide task runs on a thread-block cluster of this many CTAs: the leader
 // runs the task, the followers take slices of its position-parallel phases.
 constexpr int kClusterCtas = 4;
-constexpr int32_t kPhUnion = 1, kPhFind = 2, kPhTerms = 3, kPhExit = 4, kPhDecide = 5;
+constexpr int32_t kPhUnion = 1, kPhFind = 2, kPhTerms = 3, kPhExit = 4, kPhDecide = 5, kPhReorder = 6;
+constexpr int32_t kClusterReorderChunks = 8;  // reorders of at least this many chunks use the cluster
 constexpr int kProfPhases = 16;  // phase cycle counters per task (structural 0..7, 12; statistics 8..11)
 
 struct Task {
@@ -115,6 +116,8 @@ struct TreeArgs {
   int32_t big_task;
   int32_t* nnext_big;
   int32_t* max_big;       // largest task pushed to next_big (bounds every task a wide launch runs)
+  int32_t* rcnt;          // [kClusterCtas][ng+1] roots counted per CTA in a cluster reorder, by position
+  int32_t* rrun;          // [kClusterCtas][ng+1] running ranks per CTA in a cluster reorder, by position
   int32_t par_cap_big;    // union-find parents in shared memory for wide tasks of at most this many groups
   // a slot of next / next_big is readable once its flag is set; ntaken /
   // ntaken_big count the slots that blocks of the current wave took over
@@ -384,6 +387,109 @@ __device__ __forceinline__ void find_roots(const TreeArgs& A, int32_t a, int32_t
   }
 }
 
+// Stable reorder by root of positions [c_begin, c_end) (whole chunks of
+// NT * IPT positions from a, or the task's end) into GL2: inside a chunk a
+// stable block radix sort groups equal roots; a run's rank is its offset from
+// the run head (block max-scan of head indices); run[] carries each root's
+// rank across the chunks (entry r - a for root position r).
+template <int NT, class SortT, class MaxScanT>
+__device__ void reorder_chunks(const TreeArgs& A, int32_t a, int32_t b, int32_t poff, const int32_t* par,
+                               int32_t* run, int32_t c_begin, int32_t c_end,
+                               typename SortT::TempStorage& sort_tmp,
+                               typename MaxScanT::TempStorage& maxscan_tmp, int32_t* s_keys) {
+  constexpr int IPT = ipt_for(NT);
+  const int tid = threadIdx.x;
+  const int32_t sent = b - a;  // key of dropped groups, above every root offset
+  const int kbits = 32 - __clz(sent);
+  for (int32_t c0 = c_begin; c0 < c_end; c0 += (NT * IPT)) {
+    int32_t keys[IPT], vals[IPT];
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+      int32_t i = c0 + tid * IPT + k;
+      int32_t r = (i < c_end) ? par[i - poff] : -1;
+      keys[k] = (r >= 0) ? (r + poff - a) : sent;
+      vals[k] = i;
+    }
+    SortT(sort_tmp).Sort(keys, vals, 0, kbits);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) s_keys[tid * IPT + k] = keys[k];
+    __syncthreads();
+    int32_t headq[IPT];
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+      int q = tid * IPT + k;
+      headq[k] = (q == 0 || s_keys[q - 1] != keys[k]) ? q : 0;
+    }
+    MaxScanT(maxscan_tmp).InclusiveScan(headq, headq, cub::Max());
+    bool tail[IPT];
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+      int q = tid * IPT + k;
+      tail[k] = (q == (NT * IPT) - 1) || (s_keys[q + 1] != keys[k]);
+      if (keys[k] == sent) continue;
+      int32_t np = a + A.cnt[keys[k] + a] + run[keys[k]] + (q - headq[k]);
+      if (np < a || np >= b) { set_err(A, 17, np); continue; }
+      A.GL2[np] = A.GL[vals[k]];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+      int q = tid * IPT + k;
+      if (tail[k] && keys[k] != sent) run[keys[k]] += q - headq[k] + 1;
+    }
+    __syncthreads();
+  }
+}
+
+// chunk range [ch0, ch1) of the cluster's CTA `rank` (of K) over positions [a, b)
+template <int NT>
+__device__ __forceinline__ void reorder_range_of(int32_t a, int32_t b, int rank, int K, int32_t& p0, int32_t& p1) {
+  constexpr int32_t CH = NT * ipt_for(NT);
+  const int32_t nch = (b - a + CH - 1) / CH, per = (nch + K - 1) / K;
+  const int32_t ch0 = min(nch, rank * per), ch1 = min(nch, ch0 + per);
+  p0 = a + ch0 * CH;
+  p1 = min(b, a + ch1 * CH);
+}
+
+// a cluster reorder, step 1: CTA rank counts the roots of its chunk range in
+// its own row of A.rcnt, at the root's absolute position (the positions of
+// tasks that run at the same time on other clusters are disjoint)
+template <int NT>
+__device__ void reorder_count(const TreeArgs& A, int32_t a, int32_t b, int32_t poff, const int32_t* par, int rank,
+                              int K) {
+  const int tid = threadIdx.x;
+  int32_t* cnt = A.rcnt + (size_t)rank * (A.ngroups + 1) + a;  // entry r - a
+  for (int32_t j = tid; j < b - a; j += NT) cnt[j] = 0;
+  __syncthreads();
+  int32_t p0, p1;
+  reorder_range_of<NT>(a, b, rank, K, p0, p1);
+  for (int32_t i = p0 + tid; i < p1; i += NT) {
+    const int32_t r = par[i - poff];
+    if (r >= 0) atomicAdd(&cnt[r + poff - a], 1);
+  }
+}
+
+// step 2 (after every CTA's count): ranks start after the counts of the
+// ranges before this one, then the range is reordered
+template <int NT, class SortT, class MaxScanT>
+__device__ void reorder_range(const TreeArgs& A, int32_t a, int32_t b, int32_t poff, const int32_t* par, int rank,
+                              int K, typename SortT::TempStorage& sort_tmp,
+                              typename MaxScanT::TempStorage& maxscan_tmp, int32_t* s_keys) {
+  const int tid = threadIdx.x;
+  const size_t G = (size_t)A.ngroups + 1;
+  int32_t* run = A.rrun + (size_t)rank * G + a;  // entry r - a
+  for (int32_t j = tid; j < b - a; j += NT) {
+    int32_t v = 0;
+    for (int r = 0; r < rank; ++r) v += A.rcnt[(size_t)r * G + a + j];
+    run[j] = v;
+  }
+  __syncthreads();
+  int32_t p0, p1;
+  reorder_range_of<NT>(a, b, rank, K, p0, p1);
+  reorder_chunks<NT, SortT, MaxScanT>(A, a, b, poff, par, run, p0, p1, sort_tmp, maxscan_tmp, s_keys);
+}
+
 template <int NT, class SortT, class ScanT, class MaxScanT>
 __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT::TempStorage& sort_tmp,
                                 typename ScanT::TempStorage& scan_tmp, typename MaxScanT::TempStorage& maxscan_tmp,
@@ -445,47 +551,18 @@ __device__ void structural_pass(const TreeArgs& A, SharedTask& T, typename SortT
   // stable reorder by root, chunk by chunk: inside a chunk a stable block
   // radix sort groups equal roots; a run's rank is its offset from the run
   // head (block max-scan of head indices); run[] carries ranks across chunks
-  const int32_t sent = b - a;  // key of dropped groups, above every root offset
-  const int kbits = 32 - __clz(sent);
-  for (int32_t c0 = a; c0 < b; c0 += (NT * IPT)) {
-    int32_t keys[IPT], vals[IPT];
-#pragma unroll
-    for (int k = 0; k < IPT; ++k) {
-      int32_t i = c0 + tid * IPT + k;
-      int32_t r = (i < b) ? par[i - poff] : -1;
-      keys[k] = (r >= 0) ? (r + poff - a) : sent;
-      vals[k] = i;
-    }
-    SortT(sort_tmp).Sort(keys, vals, 0, kbits);
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < IPT; ++k) s_keys[tid * IPT + k] = keys[k];
-    __syncthreads();
-    int32_t headq[IPT];
-#pragma unroll
-    for (int k = 0; k < IPT; ++k) {
-      int q = tid * IPT + k;
-      headq[k] = (q == 0 || s_keys[q - 1] != keys[k]) ? q : 0;
-    }
-    MaxScanT(maxscan_tmp).InclusiveScan(headq, headq, cub::Max());
-    bool tail[IPT];
-#pragma unroll
-    for (int k = 0; k < IPT; ++k) {
-      int q = tid * IPT + k;
-      tail[k] = (q == (NT * IPT) - 1) || (s_keys[q + 1] != keys[k]);
-      if (keys[k] == sent) continue;
-      int32_t r = keys[k] + a;
-      int32_t np = a + A.cnt[r] + A.run[r] + (q - headq[k]);
-      if (np < a || np >= b) { set_err(A, 17, np); continue; }
-      A.GL2[np] = A.GL[vals[k]];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < IPT; ++k) {
-      int q = tid * IPT + k;
-      if (tail[k] && keys[k] != sent) A.run[keys[k] + a] += q - headq[k] + 1;
-    }
-    __syncthreads();
+  if (K > 1 && b - a > (kClusterReorderChunks - 1) * NT * IPT) {
+    // the cluster's CTAs take contiguous ranges of chunks: each counts the
+    // roots of its range, then starts its ranks after the counts of the
+    // ranges before it (worth its three barriers and the rank set-up only
+    // for long tasks)
+    lead_phase(T, kPhReorder, local);
+    reorder_count<NT>(A, a, b, poff, par, 0, K);
+    cg::this_cluster().sync();
+    reorder_range<NT, SortT, MaxScanT>(A, a, b, poff, par, 0, K, sort_tmp, maxscan_tmp, s_keys);
+    cg::this_cluster().sync();
+  } else {
+    reorder_chunks<NT, SortT, MaxScanT>(A, a, b, poff, par, A.run + a, a, b, sort_tmp, maxscan_tmp, s_keys);
   }
   mark(4);
   // copy back, positions, component starts
@@ -1293,8 +1370,10 @@ __device__ void prune_low_components(const TreeArgs& A, SharedTask& T, typename 
 // barriers, the pair the leader takes around its own slice; kPhExit ends the
 // loop, and one last barrier tells the leader that its shared memory is read
 // no more.
-template <int NT>
-__device__ void follow_phases(const TreeArgs& A, SharedTask& T, int32_t* s_big, int32_t* s_par, CompSums* s_red) {
+template <int NT, class SortT, class MaxScanT>
+__device__ void follow_phases(const TreeArgs& A, SharedTask& T, int32_t* s_big, int32_t* s_par, CompSums* s_red,
+                              int32_t* s_keys, typename SortT::TempStorage& sort_tmp,
+                              typename MaxScanT::TempStorage& maxscan_tmp) {
   cg::cluster_group cl = cg::this_cluster();
   const int K = (int)cl.num_blocks();
   const int rank = (int)cl.block_rank();
@@ -1323,6 +1402,10 @@ __device__ void follow_phases(const TreeArgs& A, SharedTask& T, int32_t* s_big, 
     } else if (code == kPhTerms) {
       for (int32_t i = a + gt; i < b; i += gs)
         position_terms(A, i, rhot, A.cs + 12 * (size_t)(a + A.compidx[i]) + 9);
+    } else if (code == kPhReorder) {
+      reorder_count<NT>(A, a, b, poff, par, rank, K);
+      cl.sync();  // every CTA's count is in (the leader takes this barrier too)
+      reorder_range<NT, SortT, MaxScanT>(A, a, b, poff, par, rank, K, sort_tmp, maxscan_tmp, s_keys);
     } else if (code == kPhDecide) {
       decide_slice<NT>(A, a, b, LT->ncomp, rhot, rank, K, cl.map_shared_rank(s_big, 0), LT->fold_n, s_red,
                        cl.map_shared_rank(s_red + NT / 32, 0));
@@ -1354,7 +1437,8 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 4) tree_wave_kernel(TreeA
   if (NT >= 1024) {
     K = cluster_ctas();
     if (cg::this_cluster().block_rank() != 0) {
-      follow_phases<NT>(A, T, s_big, s_par, reinterpret_cast<CompSums*>(s_terms));
+      follow_phases<NT, SortT, MaxScanT>(A, T, s_big, s_par, reinterpret_cast<CompSums*>(s_terms), s_keys, sort_tmp,
+                                         maxscan_tmp);
       return;
     }
   }
@@ -1920,7 +2004,7 @@ int stage_nodes(Engine& E) {
   const size_t bytes_i = G * 4;
   // every sub-array starts on a 256-byte boundary: size the buffer with the rounding
   auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
-  const size_t need = r256(bytes_i) * 12 + r256(G * 8 * 8) + r256(G * 12 * 8) +
+  const size_t need = r256(bytes_i) * 12 + r256(bytes_i * kClusterCtas) * 2 + r256(G * 8 * 8) + r256(G * 12 * 8) +
                       r256((size_t)(nnodesmax + 1) * sizeof(Task)) * 4 + r256((size_t)(nnodesmax + 1) * 4) * 4;
   AHOP_CUDA_TRY(E.d_tree_scratch.ensure(need));
   char* p = static_cast<char*>(E.d_tree_scratch.p);
@@ -1938,6 +2022,8 @@ int stage_nodes(Engine& E) {
   A.deepnode = reinterpret_cast<int32_t*>(take(bytes_i));
   A.gcur = reinterpret_cast<int32_t*>(take(bytes_i));
   A.ecur = reinterpret_cast<int32_t*>(take(bytes_i));
+  A.rcnt = reinterpret_cast<int32_t*>(take(bytes_i * kClusterCtas));
+  A.rrun = reinterpret_cast<int32_t*>(take(bytes_i * kClusterCtas));
   A.gs = reinterpret_cast<double*>(take(G * 8 * 8));
   A.cs = reinterpret_cast<double*>(take(G * 12 * 8));
   A.big_task = E.big_task;
