@@ -1834,6 +1834,50 @@ __global__ void gather_member_rho(const int32_t* __restrict__ gmem, const double
   if (i < m) rho[i] = dens[gmem[i]];
 }
 
+// Members by decreasing density inside each group with one radix sort of all
+// members: key = group (ascending: the groups' member ranges stay where they
+// are), then the density rounded down to float, decreasing (rounding is
+// monotone, and non-negative floats order like their bits).  Members whose
+// keys are equal (densities within a float step) are then put in exact order
+// by member_fix_runs_kernel.  Exactly equal densities may end in any order:
+// counts above a threshold and the bounded running sums do not depend on it.
+__global__ void member_rho_keys_kernel(const int32_t* __restrict__ gmem, const int32_t* __restrict__ group,
+                                       const double* __restrict__ dens, int64_t m,
+                                       unsigned long long* __restrict__ key) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int32_t s = gmem[i];
+  key[i] = ((unsigned long long)(uint32_t)group[s] << 32) |
+           (unsigned long long)(0xffffffffu - __float_as_uint(__double2float_rd(dens[s])));
+}
+
+constexpr int kMaxKeyRun = 64;  // longer runs of equal keys (contrived inputs): the segmented sort instead
+
+// a thread per run of equal keys (of at most kMaxKeyRun members): insertion
+// sort by exact density, decreasing; a longer run raises *flag
+__global__ void member_fix_runs_kernel(const unsigned long long* __restrict__ key, int64_t m, int32_t* __restrict__ mem,
+                                       double* __restrict__ rho, int32_t* __restrict__ flag) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i + 1 >= m || key[i + 1] != key[i] || (i > 0 && key[i - 1] == key[i])) return;
+  int64_t e = i + 2;
+  while (e < m && key[e] == key[i]) {
+    if (e - i >= kMaxKeyRun) { atomicExch(flag, 1); return; }
+    ++e;
+  }
+  for (int64_t j = i + 1; j < e; ++j) {
+    const double r = rho[j];
+    const int32_t v = mem[j];
+    int64_t k = j;
+    while (k > i && rho[k - 1] < r) {
+      rho[k] = rho[k - 1];
+      mem[k] = mem[k - 1];
+      --k;
+    }
+    rho[k] = r;
+    mem[k] = v;
+  }
+}
+
 // running sums per group (one warp per group) in decreasing-density order
 __global__ void prefix_moments_kernel(const int32_t* __restrict__ goff, int32_t ng,
                                       const int32_t* __restrict__ mem_rho_order, const double* __restrict__ rdesc,
@@ -1969,20 +2013,54 @@ int stage_nodes(Engine& E) {
   double* rho_idx = E.d_gmem_rho.as<double>();        // densities in particle-index order
   double* rdesc = E.d_gmem_rho.as<double>() + nact;   // sorted decreasing
   int32_t* mem_rho = reinterpret_cast<int32_t*>(E.d_sad_val2.p);
-  E.launches++;
-  gather_member_rho<<<(unsigned)((nact + T - 1) / T), T, 0, st>>>(E.d_gmem.as<int32_t>(), E.d_dens.as<double>(),
-                                                                  nact, rho_idx);
-  AHOP_CUDA_TRY(cudaGetLastError());
-  size_t tmp = 0;
-  cub::DeviceSegmentedSort::SortPairsDescending(nullptr, tmp, rho_idx, rdesc, E.d_gmem.as<int32_t>(), mem_rho,
-                                                (int)nact, ng, E.d_goff.as<int32_t>() + 1,
-                                                E.d_goff.as<int32_t>() + 2, st);
-  AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
-  E.cub_calls++;
-  AHOP_CUDA_TRY(cub::DeviceSegmentedSort::SortPairsDescending(E.d_cub.p, tmp, rho_idx, rdesc,
-                                                              E.d_gmem.as<int32_t>(), mem_rho, (int)nact, ng,
-                                                              E.d_goff.as<int32_t>() + 1,
-                                                              E.d_goff.as<int32_t>() + 2, st));
+  bool sorted = false;
+  if (nact > 0) {
+    // one radix sort of (group, density rounded to float), then exact order
+    // inside runs of equal keys (member_rho_keys_kernel)
+    AHOP_CUDA_TRY(E.d_key.ensure((size_t)nact * 8));
+    AHOP_CUDA_TRY(E.d_key2.ensure((size_t)nact * 8));
+    unsigned long long* k0 = E.d_key.as<unsigned long long>();
+    unsigned long long* k1 = E.d_key2.as<unsigned long long>();
+    const unsigned gm = (unsigned)((nact + T - 1) / T);
+    E.launches++;
+    member_rho_keys_kernel<<<gm, T, 0, st>>>(E.d_gmem.as<int32_t>(), E.d_group.as<int32_t>(), E.d_dens.as<double>(),
+                                             nact, k0);
+    AHOP_CUDA_TRY(cudaGetLastError());
+    int end_bit = 32;
+    while (end_bit < 64 && (1LL << (end_bit - 32)) <= (int64_t)ng) ++end_bit;
+    size_t tmp = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, k0, k1, E.d_gmem.as<int32_t>(), mem_rho, (int)nact, 0, end_bit, st);
+    AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
+    E.cub_calls++;
+    AHOP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(E.d_cub.p, tmp, k0, k1, E.d_gmem.as<int32_t>(), mem_rho,
+                                                  (int)nact, 0, end_bit, st));
+    E.launches += 2;
+    gather_member_rho<<<gm, T, 0, st>>>(mem_rho, E.d_dens.as<double>(), nact, rdesc);
+    int32_t* fl = reinterpret_cast<int32_t*>(k0);  // the unsorted keys are no longer needed
+    AHOP_CUDA_TRY(cudaMemsetAsync(fl, 0, 4, st));
+    member_fix_runs_kernel<<<gm, T, 0, st>>>(k1, nact, mem_rho, rdesc, fl);
+    AHOP_CUDA_TRY(cudaGetLastError());
+    int32_t* hf = reinterpret_cast<int32_t*>(E.h_scalars);
+    AHOP_CUDA_TRY(cudaMemcpyAsync(hf, fl, 4, cudaMemcpyDeviceToHost, st));
+    AHOP_CUDA_TRY(cudaStreamSynchronize(st));
+    sorted = hf[0] == 0;
+  }
+  if (!sorted && nact > 0) {  // a run of more than kMaxKeyRun equal keys: sort the groups' members exactly
+    E.launches++;
+    gather_member_rho<<<(unsigned)((nact + T - 1) / T), T, 0, st>>>(E.d_gmem.as<int32_t>(), E.d_dens.as<double>(),
+                                                                    nact, rho_idx);
+    AHOP_CUDA_TRY(cudaGetLastError());
+    size_t tmp = 0;
+    cub::DeviceSegmentedSort::SortPairsDescending(nullptr, tmp, rho_idx, rdesc, E.d_gmem.as<int32_t>(), mem_rho,
+                                                  (int)nact, ng, E.d_goff.as<int32_t>() + 1,
+                                                  E.d_goff.as<int32_t>() + 2, st);
+    AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
+    E.cub_calls++;
+    AHOP_CUDA_TRY(cub::DeviceSegmentedSort::SortPairsDescending(E.d_cub.p, tmp, rho_idx, rdesc,
+                                                                E.d_gmem.as<int32_t>(), mem_rho, (int)nact, ng,
+                                                                E.d_goff.as<int32_t>() + 1,
+                                                                E.d_goff.as<int32_t>() + 2, st));
+  }
   {
     int64_t threads = (int64_t)ng * 32;
     E.launches++;
@@ -2386,7 +2464,7 @@ int stage_nodes(Engine& E) {
     E.launches++;
     iota_kernel<<<(unsigned)((nn + T - 1) / T), T, 0, st>>>(new_to_old, nn, 1);
     AHOP_CUDA_TRY(cudaGetLastError());
-    tmp = 0;
+    size_t tmp = 0;
     NodeLess less{A.node};
     cub::DeviceMergeSort::SortKeys(nullptr, tmp, new_to_old, nn, less, st);
     AHOP_CUDA_TRY(E.d_cub.ensure(tmp));
