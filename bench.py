@@ -605,7 +605,8 @@ def main():
                  "leaf_visits_per_query": ts[10] / n, "insertions_per_query": ts[11] / n, "overflow_leaves": ts[12],
                  "ideal_visits_per_query": ts[18] / n, "chunks_per_query": ts[26] / n,
                  "ballot_hits_per_query": ts[27] / n,
-                 "union_visits_per_query_leaf": ts[28] / max(1, ts[29])}
+                 "union_visits_per_query_leaf": ts[28] / max(1, ts[29]),
+                 "overflow_cycle_share": ts[19] / max(1, ts[19] + ts[20])}
     ph = [float(ts[21 + k]) for k in range(5)]
     if sum(ph) > 0:
         knn_stats["cycle_share"] = {k: v / sum(ph) for k, v in zip(
