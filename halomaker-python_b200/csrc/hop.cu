@@ -73,15 +73,16 @@ __global__ void group_kernel(const int32_t* __restrict__ root, const int32_t* __
   if (r == (int32_t)s) { densg[g] = dens[s]; gpeak[g] = (int32_t)s; }
 }
 
-// sort key: (group ascending, particle index descending); inactive particles last
+// sort key: (group ascending, particle index descending); inactive particles
+// last.  The index takes ob bits (2^ob > n), the group the bits above.
 __global__ void member_keys_kernel(const int32_t* __restrict__ group, const int32_t* __restrict__ orig,
-                                   int64_t n, int32_t ngroups, unsigned long long* __restrict__ key,
+                                   int64_t n, int32_t ngroups, int ob, unsigned long long* __restrict__ key,
                                    int32_t* __restrict__ val) {
   int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (s >= n) return;
   int32_t g = group[s];
   unsigned long long gg = (unsigned long long)(g > 0 ? g : ngroups + 1);
-  key[s] = (gg << 32) | (unsigned long long)(0xffffffffu - (uint32_t)orig[s]);
+  key[s] = (gg << ob) | (((1ull << ob) - 1ull) - (unsigned long long)(uint32_t)orig[s]);
   val[s] = (int32_t)s;
 }
 
@@ -173,10 +174,11 @@ int stage_hop_groups(Engine& E) {
   AHOP_CUDA_TRY(E.d_idx2.ensure(n * 4));
   AHOP_CUDA_TRY(E.d_gmem.ensure(n * 4));
   E.launches++;
-  member_keys_kernel<<<grid, T, 0, st>>>(E.d_group.as<int32_t>(), E.d_orig.as<int32_t>(), n, ng,
+  const int ob = bits_for(n);  // 2^ob > n > every particle index
+  member_keys_kernel<<<grid, T, 0, st>>>(E.d_group.as<int32_t>(), E.d_orig.as<int32_t>(), n, ng, ob,
                                          E.d_key.as<unsigned long long>(), E.d_idx2.as<int32_t>());
   AHOP_CUDA_TRY(cudaGetLastError());
-  int end_bit = 32 + bits_for((int64_t)ng + 1);
+  int end_bit = ob + bits_for((int64_t)ng + 2);
   if (end_bit > 64) end_bit = 64;
   tmp = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, tmp, E.d_key.as<unsigned long long>(),

@@ -607,6 +607,49 @@ constexpr int kMaxCandSpill = 4096;  // ... in the warp's global spill buffer (e
 static_assert((kMaxCand & (kMaxCand - 1)) == 0 && (kMaxCandSpill & (kMaxCandSpill - 1)) == 0,
               "candidate capacities must be powers of two");
 
+// Ascending bitonic sort of the 32 * E keys at kb by one warp in registers:
+// lane l holds keys [l * E, l * E + E); strides below E are exchanges inside
+// a lane, larger ones shuffles with lane l ^ (stride / E).  The keys are
+// distinct (slot numbers in their low bits), so the order is the same as any
+// other sort's.
+template <int E>
+__device__ __forceinline__ void warp_sort_regs(unsigned* kb, int lane) {
+  constexpr int N = 32 * E;
+  unsigned v[E];
+#pragma unroll
+  for (int r = 0; r < E; ++r) v[r] = kb[lane * E + r];
+#pragma unroll
+  for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= E) {
+        const int lj = j / E, lk = k / E;
+        const bool keep_min = ((lane & lj) == 0) == ((lane & lk) == 0);
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+          const unsigned p = __shfl_xor_sync(0xffffffffu, v[r], lj);
+          v[r] = keep_min ? min(v[r], p) : max(v[r], p);
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+          if ((r & j) == 0) {
+            const bool asc = ((lane * E + r) & k) == 0;
+            const unsigned a = v[r], b = v[r | j];
+            const unsigned lo = min(a, b), hi = max(a, b);
+            v[r] = asc ? lo : hi;
+            v[r | j] = asc ? hi : lo;
+          }
+        }
+      }
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int r = 0; r < E; ++r) kb[lane * E + r] = v[r];
+  __syncwarp();
+}
+
 // One warp per query leaf (its 32 Morton-consecutive particles).
 //  A. every query sorts the 64 particles of its own and the adjacent leaf
 //     (the order is kept, 32 bytes per query); their nv-th distance bounds
@@ -727,12 +770,21 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) knn_leaf_kernel(KnnArg
       __syncwarp();
     }
     if (!overflow) {
-      // candidates nearest-first: warp bitonic sort of the keys in shared memory
+      // candidates nearest-first: warp bitonic sort of the keys, in
+      // registers up to kMaxCand keys, else in the spill buffer
       int N = 32;
       while (N < ncand) N <<= 1;
       for (int i = ncand + lane; i < N; i += 32) kb[i] = 0xffffffffu;
       __syncwarp();
-      for (int k = 2; k <= N; k <<= 1) {
+      switch (N) {
+        case 32: warp_sort_regs<1>(kb, lane); break;
+        case 64: warp_sort_regs<2>(kb, lane); break;
+        case 128: warp_sort_regs<4>(kb, lane); break;
+        case 256: warp_sort_regs<8>(kb, lane); break;
+        case 512: warp_sort_regs<16>(kb, lane); break;
+        default: break;
+      }
+      for (int k = 2; k <= (N > kMaxCand ? N : 1); k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
           for (int t = lane; t < (N >> 1); t += 32) {
             const int i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
