@@ -234,12 +234,16 @@ int ahop_compute_adaptahop(const double* pos_in, const double* mass_in, int64_t 
     AHOP_CUDA_TRY(cudaEventCreateWithFlags(&E.ev_copied, cudaEventDisableTiming));
   }
   if (!E.ev_mass) AHOP_CUDA_TRY(cudaEventCreateWithFlags(&E.ev_mass, cudaEventDisableTiming));
+  if (!E.ev_posup) AHOP_CUDA_TRY(cudaEventCreateWithFlags(&E.ev_posup, cudaEventDisableTiming));
   AHOP_CUDA_TRY(cudaEventRecord(E.ev[0], st));
   // positions first on the compute stream (the Morton keys and the sort need
-  // only them); the masses go up on the copy stream meanwhile and are waited
-  // for just before the sorted gather
-  AHOP_CUDA_TRY(cudaStreamWaitEvent(E.stream_copy, E.ev[0], 0));
+  // only them); the masses follow on the copy stream once the positions are
+  // in (two uploads at once would share the link and delay the positions),
+  // overlapping the Morton sort, and are waited for just before the sorted
+  // gather
   AHOP_CUDA_TRY(cudaMemcpyAsync(E.d_pos_in.p, pos_in, npart * 24, cudaMemcpyHostToDevice, st));
+  AHOP_CUDA_TRY(cudaEventRecord(E.ev_posup, st));
+  AHOP_CUDA_TRY(cudaStreamWaitEvent(E.stream_copy, E.ev_posup, 0));
   AHOP_CUDA_TRY(cudaMemcpyAsync(E.d_mass_in.p, mass_in, npart * 8, cudaMemcpyHostToDevice, E.stream_copy));
   AHOP_CUDA_TRY(cudaEventRecord(E.ev_mass, E.stream_copy));
   E.mass_pending = true;

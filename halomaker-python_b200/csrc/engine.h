@@ -90,6 +90,7 @@ struct Engine {
   cudaStream_t stream_copy = nullptr;   // host path: density copy-out during the later stages
   cudaEvent_t ev_dens = nullptr, ev_copied = nullptr;
   cudaEvent_t ev_mass = nullptr;        // host path: masses uploaded on the copy stream
+  cudaEvent_t ev_posup = nullptr;       // host path: positions uploaded (the masses follow)
   bool mass_pending = false;            // ... and not yet waited for by the compute stream
   cudaEvent_t wave_ev[4] = {};          // per-wave timing (task profile only)
   float wave_prof[4 * 64] = {};         // per wave: small tasks, ms, large tasks, ms
