@@ -401,6 +401,12 @@ int ahop_debug_set_tree_cluster(int32_t ctas) {
 
 int ahop_debug_get_tree_cluster(void) { return engine().tree_cluster; }
 
+int ahop_debug_set_tree_par_cap(int32_t groups) {
+  if (groups < 0) { set_error("tree union-find cap must be >= 0"); return AHOP_EINVAL; }
+  engine().tree_par_cap = groups;
+  return AHOP_OK;
+}
+
 int ahop_debug_set_big_task(int32_t groups) {
   if (groups < 1) { set_error("big-task threshold must be positive"); return AHOP_EINVAL; }
   engine().big_task = groups;

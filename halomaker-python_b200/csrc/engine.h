@@ -87,6 +87,7 @@ struct Engine {
   int tree_cluster = 1;           // CTAs per wide structure-tree task in use (1: no clusters)
   int tree_cluster_req = 4;       // CTAs asked for (debug API: 4 or 1)
   int tree_cluster_for = 0;       // the request tree_cluster was chosen for (0: none yet)
+  int tree_par_cap = 0;           // cap on the wide tasks' shared union-find array (0: none; debug API)
   cudaStream_t stream_copy = nullptr;   // host path: density copy-out during the later stages
   cudaEvent_t ev_dens = nullptr, ev_copied = nullptr;
   cudaEvent_t ev_mass = nullptr;        // host path: masses uploaded on the copy stream

@@ -2334,6 +2334,7 @@ int stage_nodes(Engine& E) {
       // union-find parents sized to the launch's largest task: the rest of the
       // shared-memory carveout stays L1
       A.par_cap_big = std::min(par_cap(kNTBig), std::max(max_big, 1));
+      if (E.tree_par_cap > 0) A.par_cap_big = std::min(A.par_cap_big, E.tree_par_cap);  // larger tasks: global array
       if (E.tree_cluster > 1) {
         // a cluster per wide task: CTA 0 runs the task, the others take slices
         // of its position-parallel phases (tree_wave_kernel, follow_phases)

@@ -178,6 +178,10 @@ int ahop_debug_set_big_task(int32_t groups);
  * compute used (1 before any). */
 int ahop_debug_set_tree_cluster(int32_t ctas);
 int ahop_debug_get_tree_cluster(void);
+/* Testing: wide tasks of more than `groups` groups keep their union-find
+ * parents in global memory instead of shared memory (0: no cap, the default;
+ * the shared array then holds up to 32,768 groups). */
+int ahop_debug_set_tree_par_cap(int32_t groups);
 int ahop_debug_task_profile(int64_t* out, int32_t maxrows);
 /* Ask compute to keep the first k neighbours per particle (default nhop). */
 int ahop_debug_set_store_neighbours(int32_t k);

@@ -51,3 +51,25 @@ def test_cluster_and_single_cta_trees_are_identical():
     for key in ("density", "liste_parts", "integer_table", "real_table"):
         assert np.array_equal(one[key], four[key]), key
         assert np.array_equal(four[key], again[key]), key
+
+
+def test_wide_tasks_with_global_union_find_are_identical():
+    """Wide tasks larger than the shared union-find array keep their parents in
+    global memory (followers then union there too); capping the array forces
+    that path on a small box."""
+    from ahop_b200 import _lib as L, finder, synthetic
+    lib = L.lib()
+    lib.ahop_debug_set_tree_par_cap.argtypes = [C.c_int32]
+    ps = synthetic.clustered_box(1_048_576, 1_200, seed=11, nmax=150_000)
+    finder.configure(ps.n)
+    ref = finder.run(ps.pos, ps.mass)
+    try:
+        L.check(lib.ahop_debug_set_tree_par_cap(600), "set_tree_par_cap")
+        four, _ = _run(lib, finder, ps, 4)
+        one, _ = _run(lib, finder, ps, 1)
+    finally:
+        lib.ahop_debug_set_tree_par_cap(0)
+        lib.ahop_debug_set_tree_cluster(4)
+    for key in ("density", "liste_parts", "integer_table", "real_table"):
+        assert np.array_equal(ref[key], four[key]), key
+        assert np.array_equal(ref[key], one[key]), key
