@@ -1204,11 +1204,28 @@ __global__ void root_terms_kernel(const TreeArgs A, double rhot) {
 }
 
 // a warp per colour: approximate sums and the three-state test
+// (colours of more than kRootBig groups are left to root_decide_big_kernel)
+constexpr int32_t kRootBig = 2048;
 __global__ void root_decide_kernel(const TreeArgs A, int32_t ncomp, double rhot) {
   const int32_t k = (int32_t)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
   if (k >= ncomp) return;
   const int32_t c1 = (k + 1 < ncomp) ? A.cstart[k + 1] : A.ngroups;
+  if (c1 - A.cstart[k] > kRootBig) return;
   component_decide(A, A.cstart[k], c1, rhot, A.cs + 12 * (size_t)k, threadIdx.x & 31);
+}
+
+// a block per colour of more than kRootBig groups (blocks stride over the
+// colours): the block folds the sums (the test's bounds hold for any order)
+__global__ void __launch_bounds__(kNT) root_decide_big_kernel(const TreeArgs A, int32_t ncomp, double rhot) {
+  __shared__ CompSums red[kNT / 32];
+  for (int32_t k = blockIdx.x; k < ncomp; k += gridDim.x) {
+    const int32_t c0 = A.cstart[k], c1 = (k + 1 < ncomp) ? A.cstart[k + 1] : A.ngroups;
+    if (c1 - c0 <= kRootBig) continue;  // the same for every thread of the block
+    const CompSums w = block_partial_sums<kNT>(A, c0, c1, threadIdx.x, kNT, red);
+    if (threadIdx.x == 0)
+      decide_from_sums(A, rhot, w.nl, w.nmax, w.dmax, w.S, w.M, w.Sx, w.Sy, w.Sz, w.Q, w.triB,
+                       A.cs + 12 * (size_t)k);
+  }
 }
 
 // one block per undecided colour: exact sums and the significance test
@@ -2201,10 +2218,11 @@ int stage_nodes(Engine& E) {
     AHOP_CUDA_TRY(cudaMemcpyAsync(h + 4, A.run + ng, 4, cudaMemcpyDeviceToHost, st));
     AHOP_CUDA_TRY(cudaStreamSynchronize(st));
     const int32_t ncomp = h[4];
-    E.launches += 4;
+    E.launches += 5;
     root_anchor_kernel<<<(unsigned)((ncomp + T - 1) / T), T, 0, st>>>(A, ncomp);
     root_terms_kernel<<<gb, T, 0, st>>>(A, rhot);
     root_decide_kernel<<<(unsigned)(((int64_t)ncomp * 32 + T - 1) / T), T, 0, st>>>(A, ncomp, rhot);
+    root_decide_big_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(ncomp, 296)), kNT, 0, st>>>(A, ncomp, rhot);
     root_colour_kernel<<<ncomp, kNT, 0, st>>>(A, ncomp, rhot);
     E.launches++;
     root_okflag_kernel<<<(unsigned)((ncomp + 1 + T - 1) / T), T, 0, st>>>(A, ncomp, A.cnt);
