@@ -1791,14 +1791,26 @@ __global__ void __launch_bounds__(256) node_fold_kernel(const TreeArgs A, int32_
   double acc = 0.0;
   int32_t ml = 0;
   const int32_t p0 = nstart[N], p1 = nend[N];
-  for (int32_t base = p0; base < p1; base += 32) {
-    const int32_t p = base + lane;
-    if (p < p1) {
-      const double* G = ps + 8 * (size_t)p;
+  // the next chunk's pair sums are loaded into registers while the current
+  // chunk is folded (the folds are sequential: their order is the reference's)
+  double nx[7];
+  if (p0 + lane < p1) {
+    const double* G = ps + 8 * (size_t)(p0 + lane);
 #pragma unroll
-      for (int c = 0; c < 7; ++c) st[wib][lane * 7 + c] = G[c];
+    for (int c = 0; c < 7; ++c) nx[c] = G[c];
+  }
+  for (int32_t base = p0; base < p1; base += 32) {
+    if (base + lane < p1) {
+#pragma unroll
+      for (int c = 0; c < 7; ++c) st[wib][lane * 7 + c] = nx[c];
     }
     __syncwarp();
+    const int32_t pn = base + 32 + lane;
+    if (pn < p1) {
+      const double* G = ps + 8 * (size_t)pn;
+#pragma unroll
+      for (int c = 0; c < 7; ++c) nx[c] = G[c];
+    }
     const int cnt = min(32, p1 - base);
     if (lane < 6) {
 #pragma unroll 8
